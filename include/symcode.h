@@ -1,0 +1,144 @@
+/*
+ * symcode.h -- C ABI of the B200 (sm_100a) pseudo-spectral Navier-Stokes hot
+ * path of SymmetryCode.jl.
+ *
+ * Every entry point replaces one call of the reference's Julia solver/closure
+ * API (cited per function as file:line of the reference project) and is what
+ * a Julia `ccall` shim binds (see symmetrycode.jl_b200/julia/SymCodeB200.jl).
+ *
+ * Conventions (identical to the reference's arrays):
+ *  - A spectral scalar field is a contiguous array of interleaved complex
+ *    numbers (re, im) of the plan's precision, shape (n/2+1, n[, n]) in
+ *    column-major order (x fastest, x is the halved RFFT axis): the element
+ *    with integer wavenumber index (ix, iy, iz) (0-based) is at linear index
+ *    ix + (n/2+1) * (iy + n * iz).  `Complex{Float32/Float64}` CuArrays have
+ *    exactly this layout.
+ *  - A vector field is passed as an array of D device pointers (x, y[, z]);
+ *    a symmetric tensor field as 3 (2D) or 6 (3D) pointers in the order
+ *    xx, yy[, zz], xy[, yz, zx]; a velocity-gradient field as D*D pointers in
+ *    the order xx, yx, zx, xy, yy, zy, xz, yz, zz (G_ab = d u_a / d x_b).
+ *  - A physical scalar field is a real array of shape (n, n[, n]), x fastest.
+ *  - Normalisation: u_hat = F[u] / n^D (src/solver.jl:204-215).
+ *  - All pointers are device pointers unless stated otherwise; `stream` is a
+ *    cudaStream_t (NULL = legacy default stream).  Calls are stream-ordered and
+ *    asynchronous unless documented as synchronous.
+ *  - Every call returns an sc_status; on error sc_last_error_string() (per
+ *    thread) describes it.  No exception crosses the ABI.
+ *  - A plan is not thread-safe: use one plan per stream/thread.
+ */
+#ifndef SYMCODE_H
+#define SYMCODE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SC_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define SC_API __attribute__((visibility("default")))
+#else
+#define SC_API
+#endif
+
+typedef struct sc_plan sc_plan;
+
+typedef enum sc_dtype { SC_FLOAT32 = 0, SC_FLOAT64 = 1 } sc_dtype;
+
+typedef enum sc_status {
+  SC_OK = 0,
+  SC_ERR_INVALID = 1,      /* bad argument (null pointer, D not 2/3, ...) */
+  SC_ERR_SIZE = 2,         /* n odd or not 2^a 3^b 5^c in the supported set */
+  SC_ERR_CUDA = 3,         /* CUDA runtime error */
+  SC_ERR_OOM = 4,          /* device allocation failed */
+  SC_ERR_DIVERGED = 5,     /* blow-up guard tripped (energy > limit or non-finite) */
+  SC_ERR_UNSUPPORTED = 6   /* valid request outside what this build implements */
+} sc_status;
+
+/* Linear band forcing of the RK4 stepper: f_hat = A u_hat on 1 <= |k|^2 < 9
+ * (shells 1 and 2, the shells the reference clamps in maintain_shell_energy!,
+ * src/solver.jl:1146-1152, src/data.jl:49,65) with A = eps / (2 E_band)
+ * recomputed from every stage input in FP64, so energy enters at rate eps. */
+typedef struct sc_forcing {
+  int enabled;
+  double eps;
+} sc_forcing;
+
+/* ---- library ------------------------------------------------------------ */
+SC_API int sc_abi_version(void);
+SC_API const char* sc_last_error_string(void);
+/* 1 if n is a grid size this build has FFT kernels for (even, 2^a 3^b 5^c). */
+SC_API int sc_fft_size_supported(int n);
+
+/* ---- plan: Grid{D}(; l, n) + getcache(grid) ------------------------------
+ * Replaces `Grid{D}(; l, n, backend)` (src/solver.jl:131-151) together with
+ * `getcache(grid)` (src/solver.jl:956-965) and the cuFFT plan of `getplan`
+ * (src/solver.jl:432).  Allocates all scratch on the current device; no
+ * allocation happens in any later call except the first sc_to_phys/sc_to_spec
+ * (full-spectrum scratch) and the first sc_rk4_steps/sc_wray3_step (graph). */
+SC_API int sc_plan_create(sc_plan** plan, int D, int n, double l, int dtype, size_t* workspace_bytes);
+SC_API int sc_plan_destroy(sc_plan* plan);
+SC_API int sc_plan_info(const sc_plan* plan, int* D, int* n, int* dtype, int* kcut);
+
+/* ---- FFT wrappers --------------------------------------------------------
+ * to_phys! (src/solver.jl:210-211): phys = c2r(spec) * n^D (unnormalised
+ * inverse).  Unlike the reference's c2r the input is preserved.  Imaginary
+ * parts of the kx = 0 and kx = n/2 planes that break Hermitian symmetry are
+ * treated as the c2r transform does (only the real part of the row DC and
+ * Nyquist bins is used). */
+SC_API int sc_to_phys(sc_plan* plan, const void* spec, void* phys, void* stream);
+/* to_spec! (src/solver.jl:214-215): spec = r2c(phys) / n^D. */
+SC_API int sc_to_spec(sc_plan* plan, const void* phys, void* spec, void* stream);
+
+/* ---- spectral point kernels (in place, full layout) ---------------------- */
+/* twothirds! (src/solver.jl:371-389) on `ncomp` scalar fields. */
+SC_API int sc_twothirds(sc_plan* plan, void* const* fields, int ncomp, void* stream);
+/* project! (src/solver.jl:350-368). */
+SC_API int sc_project(sc_plan* plan, void* const* u_hat, void* stream);
+
+/* ---- Navier-Stokes right-hand side ----------------------------------------
+ * convectiondiffusion!(du, u, grid, cache; visc) (src/solver.jl:949-953):
+ * du_i = -i k_j (F[(P u_i)(P u_j)]/n^D - visc i (k_j u_i + k_i u_j)), P the
+ * 2/3 rule.  Output: du on the retained modes (|k_i| <= n/3, k != 0), zero
+ * elsewhere -- i.e. twothirds!(du) of the reference's du, which is all that
+ * ever reaches the retained modes of the state. */
+SC_API int sc_rhs(sc_plan* plan, const void* const* u_hat, void* const* du_hat, double visc, void* stream);
+
+/* ---- time steppers (state in full layout, advanced in place) -------------
+ * wray3!(convectiondiffusion!, u, dt, grid, cache; visc) (src/solver.jl:968-1012):
+ * one low-storage Wray RK3 step, projecting after every stage.  The state is
+ * kept on the 2/3 cube (modes outside it are set to zero); its retained modes
+ * follow the reference's exactly. */
+SC_API int sc_wray3_step(sc_plan* plan, void* const* u_hat, double dt, double visc, void* stream);
+/* New (no reference counterpart): `nsteps` classical RK4 steps,
+ * u_{n+1} = P(u_n + dt/6 (k1 + 2 k2 + 2 k3 + k4)), k_s = P(rhs(u_s)) + forcing,
+ * with the optional linear band forcing.  Same state convention as
+ * sc_wray3_step.  One RK4 step is captured in a CUDA graph and replayed. */
+SC_API int sc_rk4_steps(sc_plan* plan, void* const* u_hat, double dt, double visc, int nsteps,
+                 const sc_forcing* forcing, void* stream);
+
+/* ---- device-resident state (compact 2/3 cube held by the plan) ----------- */
+/* Gather the retained modes of u_hat into the plan's state. */
+SC_API int sc_state_load(sc_plan* plan, const void* const* u_hat, void* stream);
+/* Scatter the plan's state back to the full layout (zeros outside the 2/3 cube). */
+SC_API int sc_state_store(sc_plan* plan, void* const* u_hat, void* stream);
+/* sc_rk4_steps on the plan's state, without the load/store. */
+SC_API int sc_state_rk4(sc_plan* plan, double dt, double visc, int nsteps, const sc_forcing* forcing, void* stream);
+/* energy(u) (src/solver.jl:643-646) of the plan's state, FP64, synchronous. */
+SC_API int sc_state_energy(sc_plan* plan, double* energy, void* stream);
+/* Number of kernels one sc_state_rk4 step launches (for launch accounting). */
+SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
+
+/* ---- diagnostics (FP64 on the device; synchronous, result to host) ------- */
+/* energy(u) (src/solver.jl:643-646): 1/2 sum_i getenergy(u_i). */
+SC_API int sc_energy(sc_plan* plan, const void* const* u_hat, double* energy, void* stream);
+/* get_dissipation! (src/solver.jl:808-811): visc sum k^2 |u|^2 (RFFT double count). */
+SC_API int sc_dissipation(sc_plan* plan, const void* const* u_hat, double visc, double* diss, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SYMCODE_H */

@@ -1,0 +1,621 @@
+// C ABI of the B200 pseudo-spectral Navier-Stokes path (declared in include/symcode.h).
+//
+// The plan object stands in for the reference's `Grid` + `getcache` pair
+// (src/solver.jl:131-151, 956-965): it owns the twiddle table, the pencil
+// scratch of the five-sweep pipeline and the compact 2/3-cube state buffers of
+// the steppers.  The caller owns the fields it passes in.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sc_fft.cuh"
+#include "sc_internal.h"
+#include "symcode.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define SC_CU(call)                                                                      \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) return fail(SC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SC_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return SC_OK;
+}
+
+}  // namespace
+
+struct sc_plan {
+  int D = 0, n = 0, dtype = 0, dev = 0;
+  double l = 0;
+  int kc = 0, K1 = 0, K2 = 0;
+  size_t csz = 0;   // compact modes per component
+  size_t fsz = 0;   // full-layout modes per component
+  size_t esz = 0;   // bytes per complex
+  size_t ws = 0;
+  void* tw = nullptr;
+  void* U[3] = {}, *ACC[3] = {}, *S[3] = {};
+  void* sig[6] = {};
+  void* be[6] = {};
+  void* cc[3] = {};
+  void* dd[6] = {};
+  double* dscal = nullptr;  // [0] forcing A, [1] reduction accumulator
+  void* fa = nullptr, *fb = nullptr;  // full-spectrum scratch (lazy)
+  std::vector<void*> allocs;
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t g_rk4 = nullptr;
+  double k_rk4[4] = {0, 0, 0, 0};
+  cudaGraphExec_t g_wray = nullptr;
+  double k_wray[2] = {0, 0};
+};
+
+namespace {
+
+int plan_alloc(sc_plan* p, void** out, size_t bytes) {
+  void* ptr = nullptr;
+  cudaError_t e = cudaMalloc(&ptr, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SC_ERR_OOM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  p->allocs.push_back(ptr);
+  p->ws += bytes;
+  *out = ptr;
+  return SC_OK;
+}
+
+void plan_free(sc_plan* p) {
+  if (p->g_rk4) cudaGraphExecDestroy(p->g_rk4);
+  if (p->g_wray) cudaGraphExecDestroy(p->g_wray);
+  for (void* a : p->allocs) cudaFree(a);
+  p->allocs.clear();
+  if (p->cap) cudaStreamDestroy(p->cap);
+}
+
+template <typename R>
+int upload_twiddles(sc_plan* p) {
+  using C = typename sc::V2<R>::T;
+  std::vector<C> h(p->n);
+  for (int m = 0; m < p->n; ++m) {
+    // exp(-2 pi i m / n) from long double, reduced to the first half-turn for accuracy
+    const long double pi = 3.141592653589793238462643383279502884L;
+    const long double th = 2.0L * pi * (long double)m / (long double)p->n;
+    h[m].x = (R)cosl(th);
+    h[m].y = (R)(-sinl(th));
+  }
+  SC_CU(cudaMemcpy(p->tw, h.data(), sizeof(C) * p->n, cudaMemcpyHostToDevice));
+  return SC_OK;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------------------
+// the five-sweep product pipeline: compact u -> compact F[u_i u_j]/n^D in p->sig
+// ---------------------------------------------------------------------------
+template <typename R>
+int products(sc_plan* p, void* const* u, cudaStream_t st) {
+  const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+  sc::ColArgs a{};
+  if (p->D == 3) {
+    for (int c = 0; c < 3; ++c) { a.in[c] = u[c]; a.out[c] = p->be[c]; }
+    a.ncomp = 3; a.K1 = K1; a.ncols = K2;
+    a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
+    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
+    sc::ColArgs b{};
+    for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
+    b.ncomp = 3; b.K1 = K1; b.ncols = n;
+    b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
+    b.kpos = kc + 1; b.kneg = kc;
+    sc::launch_col_inv<R>(n, b, p->tw, st);
+    sc::XArgs x{};
+    for (int c = 0; c < 3; ++c) x.in[c] = p->cc[c];
+    for (int c = 0; c < 6; ++c) x.out[c] = p->dd[c];
+    x.D = 3; x.K1in = K1; x.K1out = K1; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
+    sc::launch_xsweep_ns<R>(n, x, p->tw, st);
+    sc::ColArgs f{};
+    for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
+    f.ncomp = 6; f.K1 = K1; f.ncols = n;
+    f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = (long long)K1 * K2; f.out_es = K1;
+    f.kpos = kc + 1; f.kneg = kc;
+    sc::launch_col_fwd<R>(n, f, p->tw, st);
+    sc::ColArgs g{};
+    for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = p->sig[c]; }
+    g.ncomp = 6; g.K1 = K1; g.ncols = K2;
+    g.in_cs = K1; g.in_es = (long long)K1 * K2; g.out_cs = K1; g.out_es = (long long)K1 * K2;
+    g.kpos = kc + 1; g.kneg = kc;
+    sc::launch_col_fwd<R>(n, g, p->tw, st);
+  } else {
+    for (int c = 0; c < 2; ++c) { a.in[c] = u[c]; a.out[c] = p->cc[c]; }
+    a.ncomp = 2; a.K1 = K1; a.ncols = 1;
+    a.in_cs = 0; a.in_es = K1; a.out_cs = 0; a.out_es = K1;
+    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
+    sc::XArgs x{};
+    for (int c = 0; c < 2; ++c) x.in[c] = p->cc[c];
+    for (int c = 0; c < 3; ++c) x.out[c] = p->dd[c];
+    x.D = 2; x.K1in = K1; x.K1out = K1; x.nrows = n; x.scale = 1.0 / ((double)n * n);
+    sc::launch_xsweep_ns<R>(n, x, p->tw, st);
+    sc::ColArgs f{};
+    for (int c = 0; c < 3; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->sig[c]; }
+    f.ncomp = 3; f.K1 = K1; f.ncols = 1;
+    f.in_cs = 0; f.in_es = K1; f.out_cs = 0; f.out_es = K1;
+    f.kpos = kc + 1; f.kneg = kc;
+    sc::launch_col_fwd<R>(n, f, p->tw, st);
+  }
+  return check_launch("product pipeline");
+}
+
+template <typename R>
+sc::EpiArgs epi_base(sc_plan* p, void* const* us, double visc) {
+  sc::EpiArgs e{};
+  for (int c = 0; c < 6; ++c) e.sig[c] = p->sig[c];
+  for (int c = 0; c < p->D; ++c) e.us[c] = us[c];
+  e.D = p->D; e.K1 = p->K1; e.K2 = p->K2; e.kc = p->kc;
+  e.kfac = 2.0 * M_PI / p->l;
+  e.visc = visc;
+  return e;
+}
+
+template <typename R>
+int rk4_step(sc_plan* p, double dt, double visc, const sc_forcing* frc, cudaStream_t st) {
+  const bool forced = frc != nullptr && frc->enabled;
+  for (int s = 0; s < 4; ++s) {
+    void* const* us = s == 0 ? p->U : p->S;
+    if (forced) sc::launch_band_forcing<R>(us, p->D, p->K1, p->K2, p->kc, frc->eps, p->dscal, st);
+    int rc = products<R>(p, us, st);
+    if (rc) return rc;
+    sc::EpiArgs e = epi_base<R>(p, us, visc);
+    e.proj_k = 1;
+    e.forcing = forced ? p->dscal : nullptr;
+    static const double wa[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+    static const double cbv[3] = {0.5, 0.5, 1.0};
+    for (int c = 0; c < p->D; ++c) {
+      e.base_a[c] = s == 0 ? p->U[c] : p->ACC[c];
+      e.out_a[c] = s == 3 ? p->U[c] : p->ACC[c];
+      if (s < 3) { e.base_b[c] = p->U[c]; e.out_b[c] = p->S[c]; }
+    }
+    e.ca = wa[s] * dt;
+    e.has_b = s < 3;
+    e.cb = s < 3 ? cbv[s] * dt : 0.0;
+    sc::launch_epilogue<R>(e, st);
+  }
+  return check_launch("rk4 step");
+}
+
+template <typename R>
+int wray3_step(sc_plan* p, double dt, double visc, cudaStream_t st) {
+  static const double a[3] = {8.0 / 15, 5.0 / 12, 3.0 / 4};
+  static const double b[2] = {1.0 / 4, 0.0};
+  for (int s = 0; s < 3; ++s) {
+    int rc = products<R>(p, p->U, st);
+    if (rc) return rc;
+    sc::EpiArgs e = epi_base<R>(p, p->U, visc);
+    e.proj_a = 1;
+    for (int c = 0; c < p->D; ++c) {
+      e.base_a[c] = s == 0 ? p->U[c] : p->S[c];
+      e.out_a[c] = p->U[c];
+      e.base_b[c] = s == 0 ? p->U[c] : p->S[c];
+      e.out_b[c] = p->S[c];
+    }
+    e.ca = a[s] * dt;
+    e.has_b = (s < 2 && (s == 0 || b[s] != 0.0)) ? 1 : 0;
+    e.cb = s < 2 ? b[s] * dt : 0.0;
+    sc::launch_epilogue<R>(e, st);
+  }
+  return check_launch("wray3 step");
+}
+
+template <typename R>
+int pack_state(sc_plan* p, const void* const* u, void* const* dst, cudaStream_t st) {
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) { a.src[c] = u[c]; a.dst[c] = dst[c]; }
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  sc::launch_pack<R>(a, st);
+  return check_launch("pack");
+}
+
+template <typename R>
+int unpack_state(sc_plan* p, void* const* src, void* const* u, cudaStream_t st) {
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) { a.src[c] = src[c]; a.dst[c] = u[c]; }
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  sc::launch_unpack<R>(a, st);
+  return check_launch("unpack");
+}
+
+int check_ptrs(const void* const* u, int k) {
+  if (!u) return fail(SC_ERR_INVALID, "null field array");
+  for (int c = 0; c < k; ++c)
+    if (!u[c]) return fail(SC_ERR_INVALID, "null component pointer %d", c);
+  return SC_OK;
+}
+
+int ensure_device(sc_plan* p) {
+  int cur = -1;
+  SC_CU(cudaGetDevice(&cur));
+  if (cur != p->dev) SC_CU(cudaSetDevice(p->dev));
+  return SC_OK;
+}
+
+template <typename R>
+int run_rk4_graph(sc_plan* p, double dt, double visc, int nsteps, const sc_forcing* frc, cudaStream_t st) {
+  const double key[4] = {dt, visc, (frc && frc->enabled) ? 1.0 : 0.0, (frc && frc->enabled) ? frc->eps : 0.0};
+  if (!p->g_rk4 || std::memcmp(key, p->k_rk4, sizeof(key)) != 0) {
+    if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
+    cudaGraph_t g;
+    SC_CU(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    int rc = rk4_step<R>(p, dt, visc, frc, p->cap);
+    cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(SC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&p->g_rk4, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { p->g_rk4 = nullptr; return fail(SC_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    std::memcpy(p->k_rk4, key, sizeof(key));
+  }
+  for (int i = 0; i < nsteps; ++i) SC_CU(cudaGraphLaunch(p->g_rk4, st));
+  return SC_OK;
+}
+
+template <typename R>
+int run_wray_graph(sc_plan* p, double dt, double visc, cudaStream_t st) {
+  const double key[2] = {dt, visc};
+  if (!p->g_wray || std::memcmp(key, p->k_wray, sizeof(key)) != 0) {
+    if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
+    cudaGraph_t g;
+    SC_CU(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
+    int rc = wray3_step<R>(p, dt, visc, p->cap);
+    cudaError_t e = cudaStreamEndCapture(p->cap, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(SC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&p->g_wray, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { p->g_wray = nullptr; return fail(SC_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    std::memcpy(p->k_wray, key, sizeof(key));
+  }
+  SC_CU(cudaGraphLaunch(p->g_wray, st));
+  return SC_OK;
+}
+
+template <typename R>
+int ensure_full_scratch(sc_plan* p) {
+  if (p->fa) return SC_OK;
+  const size_t bytes = p->fsz * p->esz;
+  int rc = plan_alloc(p, &p->fa, bytes);
+  if (rc) return rc;
+  return plan_alloc(p, &p->fb, bytes);
+}
+
+template <typename R>
+int to_phys_impl(sc_plan* p, const void* spec, void* phys, cudaStream_t st) {
+  int rc = ensure_full_scratch<R>(p);
+  if (rc) return rc;
+  const int n = p->n, Kf = n / 2 + 1;
+  const void* cur = spec;
+  if (p->D == 3) {
+    sc::ColArgs a{};
+    a.in[0] = spec; a.out[0] = p->fa; a.ncomp = 1; a.K1 = Kf; a.ncols = n;
+    a.in_cs = Kf; a.in_es = (long long)Kf * n; a.out_cs = Kf; a.out_es = (long long)Kf * n;
+    a.kpos = n / 2; a.kneg = n / 2;
+    sc::launch_col_inv<R>(n, a, p->tw, st);
+    sc::ColArgs b{};
+    b.in[0] = p->fa; b.out[0] = p->fb; b.ncomp = 1; b.K1 = Kf; b.ncols = n;
+    b.in_cs = (long long)Kf * n; b.in_es = Kf; b.out_cs = (long long)Kf * n; b.out_es = Kf;
+    b.kpos = n / 2; b.kneg = n / 2;
+    sc::launch_col_inv<R>(n, b, p->tw, st);
+    cur = p->fb;
+  } else {
+    sc::ColArgs b{};
+    b.in[0] = spec; b.out[0] = p->fb; b.ncomp = 1; b.K1 = Kf; b.ncols = 1;
+    b.in_cs = 0; b.in_es = Kf; b.out_cs = 0; b.out_es = Kf;
+    b.kpos = n / 2; b.kneg = n / 2;
+    sc::launch_col_inv<R>(n, b, p->tw, st);
+    cur = p->fb;
+  }
+  sc::XPlainArgs x{};
+  x.in[0] = cur; x.out[0] = phys; x.ncomp = 1; x.K1 = Kf;
+  x.nrows = p->D == 3 ? (long long)n * n : n;
+  x.scale = 1.0;
+  sc::launch_x_c2r<R>(n, x, p->tw, st);
+  return check_launch("to_phys");
+}
+
+template <typename R>
+int to_spec_impl(sc_plan* p, const void* phys, void* spec, cudaStream_t st) {
+  int rc = ensure_full_scratch<R>(p);
+  if (rc) return rc;
+  const int n = p->n, Kf = n / 2 + 1;
+  sc::XPlainArgs x{};
+  x.in[0] = phys; x.out[0] = p->D == 3 ? p->fa : p->fb; x.ncomp = 1; x.K1 = Kf;
+  x.nrows = p->D == 3 ? (long long)n * n : n;
+  x.scale = 1.0 / std::pow((double)n, p->D);
+  sc::launch_x_r2c<R>(n, x, p->tw, st);
+  if (p->D == 3) {
+    sc::ColArgs a{};
+    a.in[0] = p->fa; a.out[0] = p->fb; a.ncomp = 1; a.K1 = Kf; a.ncols = n;
+    a.in_cs = (long long)Kf * n; a.in_es = Kf; a.out_cs = (long long)Kf * n; a.out_es = Kf;
+    a.kpos = n / 2; a.kneg = n / 2;
+    sc::launch_col_fwd<R>(n, a, p->tw, st);
+    sc::ColArgs b{};
+    b.in[0] = p->fb; b.out[0] = spec; b.ncomp = 1; b.K1 = Kf; b.ncols = n;
+    b.in_cs = Kf; b.in_es = (long long)Kf * n; b.out_cs = Kf; b.out_es = (long long)Kf * n;
+    b.kpos = n / 2; b.kneg = n / 2;
+    sc::launch_col_fwd<R>(n, b, p->tw, st);
+  } else {
+    sc::ColArgs b{};
+    b.in[0] = p->fb; b.out[0] = spec; b.ncomp = 1; b.K1 = Kf; b.ncols = 1;
+    b.in_cs = 0; b.in_es = Kf; b.out_cs = 0; b.out_es = Kf;
+    b.kpos = n / 2; b.kneg = n / 2;
+    sc::launch_col_fwd<R>(n, b, p->tw, st);
+  }
+  return check_launch("to_spec");
+}
+
+template <typename R>
+int energy_impl(sc_plan* p, const void* const* u, int compact, int weight_k2, double* out, cudaStream_t st) {
+  SC_CU(cudaMemsetAsync(p->dscal + 1, 0, sizeof(double), st));
+  const int K1 = compact ? p->K1 : p->n / 2 + 1;
+  const int K2 = compact ? p->K2 : p->n;
+  sc::launch_spectral_energy<R>(u, p->D, p->D, p->n, K1, K2, compact, p->kc, 2.0 * M_PI / p->l, weight_k2,
+                                p->dscal + 1, st);
+  int rc = check_launch("energy");
+  if (rc) return rc;
+  double h = 0;
+  SC_CU(cudaMemcpyAsync(&h, p->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SC_CU(cudaStreamSynchronize(st));
+  *out = h;
+  return SC_OK;
+}
+
+#define SC_DTYPE_DISPATCH(p, FN, ...) \
+  ((p)->dtype == SC_FLOAT64 ? FN<double>(__VA_ARGS__) : FN<float>(__VA_ARGS__))
+
+}  // namespace
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+extern "C" {
+
+int sc_abi_version(void) { return SC_ABI_VERSION; }
+const char* sc_last_error_string(void) { return g_err.c_str(); }
+int sc_fft_size_supported(int n) { return sc::fft_size_supported(n) ? 1 : 0; }
+
+int sc_plan_create(sc_plan** out, int D, int n, double l, int dtype, size_t* workspace_bytes) {
+  if (!out) return fail(SC_ERR_INVALID, "plan output pointer is null");
+  *out = nullptr;
+  if (D != 2 && D != 3) return fail(SC_ERR_INVALID, "D must be 2 or 3 (got %d)", D);
+  if (n % 2 != 0) return fail(SC_ERR_SIZE, "Only even number of grid points supported (n=%d)", n);
+  if (!sc::fft_size_supported(n)) return fail(SC_ERR_SIZE, "n=%d is not a supported 2^a 3^b 5^c size", n);
+  if (!(l > 0)) return fail(SC_ERR_INVALID, "domain length must be positive");
+  if (dtype != SC_FLOAT32 && dtype != SC_FLOAT64) return fail(SC_ERR_INVALID, "dtype must be 0 (f32) or 1 (f64)");
+  sc_plan* p = new sc_plan();
+  p->D = D; p->n = n; p->l = l; p->dtype = dtype;
+  SC_CU(cudaGetDevice(&p->dev));
+  p->kc = n / 3; p->K1 = p->kc + 1; p->K2 = 2 * p->kc + 1;
+  p->esz = dtype == SC_FLOAT64 ? 16 : 8;
+  p->csz = (size_t)p->K1 * p->K2 * (D == 3 ? p->K2 : 1);
+  p->fsz = (size_t)(n / 2 + 1) * n * (D == 3 ? n : 1);
+  const size_t plane = (size_t)p->K1 * n * (D == 3 ? n : 1);  // (kx, y[, z])
+  const size_t mid = (size_t)p->K1 * p->K2 * n;                // (kx, ky, z)
+  int rc = SC_OK;
+  bool ok = (dtype == SC_FLOAT64) ? sc::init_kernels<double>(n) : sc::init_kernels<float>(n);
+  if (!ok) { rc = fail(SC_ERR_CUDA, "kernel attribute setup failed for n=%d", n); goto bad; }
+  if ((rc = plan_alloc(p, &p->tw, (size_t)n * p->esz))) goto bad;
+  for (int c = 0; c < D; ++c) {
+    if ((rc = plan_alloc(p, &p->U[c], p->csz * p->esz))) goto bad;
+    if ((rc = plan_alloc(p, &p->ACC[c], p->csz * p->esz))) goto bad;
+    if ((rc = plan_alloc(p, &p->S[c], p->csz * p->esz))) goto bad;
+  }
+  for (int c = 0; c < (D == 3 ? 6 : 3); ++c) {
+    if ((rc = plan_alloc(p, &p->sig[c], p->csz * p->esz))) goto bad;
+    if ((rc = plan_alloc(p, &p->dd[c], plane * p->esz))) goto bad;
+    if (D == 3 && (rc = plan_alloc(p, &p->be[c], mid * p->esz))) goto bad;
+  }
+  for (int c = 0; c < D; ++c)
+    if ((rc = plan_alloc(p, &p->cc[c], plane * p->esz))) goto bad;
+  if ((rc = plan_alloc(p, (void**)&p->dscal, 16 * sizeof(double)))) goto bad;
+  if (cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    rc = fail(SC_ERR_CUDA, "stream creation failed");
+    goto bad;
+  }
+  rc = dtype == SC_FLOAT64 ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
+  if (rc) goto bad;
+  if (cudaMemset(p->dscal, 0, 16 * sizeof(double)) != cudaSuccess) { rc = fail(SC_ERR_CUDA, "memset"); goto bad; }
+  if (workspace_bytes) *workspace_bytes = p->ws;
+  *out = p;
+  return SC_OK;
+bad:
+  plan_free(p);
+  delete p;
+  return rc;
+}
+
+int sc_plan_destroy(sc_plan* p) {
+  if (!p) return SC_OK;
+  ensure_device(p);
+  plan_free(p);
+  delete p;
+  return SC_OK;
+}
+
+int sc_plan_info(const sc_plan* p, int* D, int* n, int* dtype, int* kcut) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (D) *D = p->D;
+  if (n) *n = p->n;
+  if (dtype) *dtype = p->dtype;
+  if (kcut) *kcut = p->kc;
+  return SC_OK;
+}
+
+int sc_to_phys(sc_plan* p, const void* spec, void* phys, void* stream) {
+  if (!p || !spec || !phys) return fail(SC_ERR_INVALID, "null argument");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, to_phys_impl, p, spec, phys, as_stream(stream));
+}
+
+int sc_to_spec(sc_plan* p, const void* phys, void* spec, void* stream) {
+  if (!p || !spec || !phys) return fail(SC_ERR_INVALID, "null argument");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, to_spec_impl, p, phys, spec, as_stream(stream));
+}
+
+int sc_rhs(sc_plan* p, const void* const* u, void* const* du, double visc, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = check_ptrs((const void* const*)du, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  auto body = [&](auto tag) -> int {
+    using R = decltype(tag);
+    int r = pack_state<R>(p, u, p->S, st);
+    if (r) return r;
+    r = products<R>(p, p->S, st);
+    if (r) return r;
+    sc::EpiArgs e = epi_base<R>(p, p->S, visc);
+    for (int c = 0; c < p->D; ++c) { e.base_a[c] = nullptr; e.out_a[c] = p->ACC[c]; }
+    e.ca = 1.0;
+    sc::launch_epilogue<R>(e, st);
+    r = check_launch("rhs epilogue");
+    if (r) return r;
+    return unpack_state<R>(p, p->ACC, du, st);
+  };
+  return p->dtype == SC_FLOAT64 ? body(double()) : body(float());
+}
+
+int sc_state_load(sc_plan* p, const void* const* u, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, pack_state, p, u, p->U, as_stream(stream));
+}
+
+int sc_state_store(sc_plan* p, void* const* u, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  int rc = check_ptrs((const void* const*)u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, unpack_state, p, p->U, u, as_stream(stream));
+}
+
+int sc_state_rk4(sc_plan* p, double dt, double visc, int nsteps, const sc_forcing* frc, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (nsteps < 0) return fail(SC_ERR_INVALID, "nsteps must be >= 0");
+  if (frc && frc->enabled && !(frc->eps >= 0)) return fail(SC_ERR_INVALID, "forcing eps must be >= 0");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  if (nsteps == 0) return SC_OK;
+  return SC_DTYPE_DISPATCH(p, run_rk4_graph, p, dt, visc, nsteps, frc, as_stream(stream));
+}
+
+int sc_state_rk4_launches_per_step(const sc_plan* p, int forced) {
+  if (!p) return 0;
+  // per stage: [band forcing] + 5 sweeps (3D) or 3 sweeps (2D) + epilogue
+  return 4 * ((forced ? 1 : 0) + (p->D == 3 ? 5 : 3) + 1);
+}
+
+int sc_rk4_steps(sc_plan* p, void* const* u, double dt, double visc, int nsteps, const sc_forcing* frc,
+                 void* stream) {
+  int rc = sc_state_load(p, (const void* const*)u, stream);
+  if (rc) return rc;
+  rc = sc_state_rk4(p, dt, visc, nsteps, frc, stream);
+  if (rc) return rc;
+  return sc_state_store(p, u, stream);
+}
+
+int sc_wray3_step(sc_plan* p, void* const* u, double dt, double visc, void* stream) {
+  int rc = sc_state_load(p, (const void* const*)u, stream);
+  if (rc) return rc;
+  rc = SC_DTYPE_DISPATCH(p, run_wray_graph, p, dt, visc, as_stream(stream));
+  if (rc) return rc;
+  return sc_state_store(p, u, stream);
+}
+
+int sc_state_energy(sc_plan* p, double* e, void* stream) {
+  if (!p || !e) return fail(SC_ERR_INVALID, "null argument");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  double s = 0;
+  rc = SC_DTYPE_DISPATCH(p, energy_impl, p, (const void* const*)p->U, 1, 0, &s, as_stream(stream));
+  if (rc) return rc;
+  *e = 0.5 * s;
+  return SC_OK;
+}
+
+int sc_energy(sc_plan* p, const void* const* u, double* e, void* stream) {
+  if (!p || !e) return fail(SC_ERR_INVALID, "null argument");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  double s = 0;
+  rc = SC_DTYPE_DISPATCH(p, energy_impl, p, u, 0, 0, &s, as_stream(stream));
+  if (rc) return rc;
+  *e = 0.5 * s;
+  return SC_OK;
+}
+
+int sc_dissipation(sc_plan* p, const void* const* u, double visc, double* d, void* stream) {
+  if (!p || !d) return fail(SC_ERR_INVALID, "null argument");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  double s = 0;
+  rc = SC_DTYPE_DISPATCH(p, energy_impl, p, u, 0, 1, &s, as_stream(stream));
+  if (rc) return rc;
+  *d = visc * s;
+  return SC_OK;
+}
+
+int sc_twothirds(sc_plan* p, void* const* f, int ncomp, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (ncomp < 1 || ncomp > sc::kMaxComp) return fail(SC_ERR_INVALID, "ncomp must be 1..%d", sc::kMaxComp);
+  int rc = check_ptrs((const void* const*)f, ncomp);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  sc::PackArgs a{};
+  for (int c = 0; c < ncomp; ++c) a.dst[c] = f[c];
+  a.ncomp = ncomp; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  if (p->dtype == SC_FLOAT64) sc::launch_twothirds_full<double>(a, as_stream(stream));
+  else sc::launch_twothirds_full<float>(a, as_stream(stream));
+  return check_launch("twothirds");
+}
+
+int sc_project(sc_plan* p, void* const* u, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  int rc = check_ptrs((const void* const*)u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) a.dst[c] = u[c];
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  if (p->dtype == SC_FLOAT64) sc::launch_project_full<double>(a, 2.0 * M_PI / p->l, as_stream(stream));
+  else sc::launch_project_full<float>(a, 2.0 * M_PI / p->l, as_stream(stream));
+  return check_launch("project");
+}
+
+}  // extern "C"

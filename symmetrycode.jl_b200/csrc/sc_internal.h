@@ -1,0 +1,106 @@
+// Internal launch interface between the C ABI (sc_api.cu) and the kernels (sc_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace sc {
+
+constexpr int kMaxComp = 12;
+
+// A batched 1D transform along a strided axis ("column sweep").  Element
+// (kx, c, e) of component q lives at in[q][kx + c*in_cs + e*in_es]; NPEN
+// consecutive kx form one tile.  Along the transform axis only the compact
+// index set {0..kpos-1} U {N-kneg..N-1} of FFT indices is stored (at compact
+// positions 0..kpos+kneg-1): it is zero-padded on input (inverse) or pruned on
+// output (forward).
+struct ColArgs {
+  const void* in[kMaxComp];
+  void* out[kMaxComp];
+  int ncomp;
+  int K1;     // number of kx (tile axis extent)
+  int ncols;  // number of columns c
+  long long in_cs, in_es, out_cs, out_es;
+  int kpos, kneg;     // compact mapping of the transform axis
+  int zero_origin;    // inverse only: treat (kx, c, e) = (0, 0, 0) as zero (k = 0 mode)
+  // optional derivative outputs (inverse only): out[ncomp + j] = transform of
+  // (i * kfac * k_e) * in[deriv_src[j]] where k_e is the signed wavenumber of
+  // compact position e; ndrv = 0 disables
+  int ndrv;
+  int drv_src[kMaxComp];
+  double kfac;
+};
+
+// The x sweep of the Navier-Stokes right-hand side: per row (y[, z]) read the
+// D velocity components' kx row (kx = 0..K1in-1), c2r to physical space,
+// form the symmetric products u_i u_j scaled by `scale`, r2c and store the
+// first K1out kx of each product row.
+struct XArgs {
+  const void* in[3];
+  void* out[6];
+  int D;
+  int K1in, K1out;
+  long long nrows;
+  double scale;
+};
+
+// Plain batched c2r / r2c along x for `ncomp` rows-of-fields (FFT API).
+struct XPlainArgs {
+  const void* in[kMaxComp];
+  void* out[kMaxComp];
+  int ncomp;
+  int K1;          // spectral row extent (kx = 0..K1-1)
+  long long nrows;
+  double scale;    // applied to the output
+};
+
+// Pointwise spectral epilogue over the compact 2/3 cube (see k_epilogue).
+struct EpiArgs {
+  const void* sig[6];   // compact product spectra F[u_i u_j]/n^D, pair order of `pairs`
+  const void* us[3];    // stage input (viscous term, forcing)
+  const void* base_a[3];
+  void* out_a[3];
+  const void* base_b[3];
+  void* out_b[3];
+  int D;
+  int K1, K2, kc;       // compact extents, kc = n/3
+  double kfac;          // 2 pi / l
+  double visc;
+  double ca, cb;        // out_a = P?(base_a + ca*k), out_b = base_b + cb*k
+  int proj_k;           // project the derivative k (RK4)
+  int proj_a;           // project out_a (Wray3)
+  int has_b;
+  const double* forcing;  // device scalar A (nullptr: no forcing)
+};
+
+struct PackArgs {
+  const void* src[kMaxComp];
+  void* dst[kMaxComp];
+  int ncomp;
+  int D, n;
+  int kc;  // compact half-width
+};
+
+template <typename R> bool launch_col_inv(int N, const ColArgs& a, const void* tw, cudaStream_t st);
+template <typename R> bool launch_col_fwd(int N, const ColArgs& a, const void* tw, cudaStream_t st);
+template <typename R> bool launch_xsweep_ns(int N, const XArgs& a, const void* tw, cudaStream_t st);
+template <typename R> bool launch_x_c2r(int N, const XPlainArgs& a, const void* tw, cudaStream_t st);
+template <typename R> bool launch_x_r2c(int N, const XPlainArgs& a, const void* tw, cudaStream_t st);
+template <typename R> void launch_epilogue(const EpiArgs& a, cudaStream_t st);
+template <typename R> void launch_pack(const PackArgs& a, cudaStream_t st);
+template <typename R> void launch_unpack(const PackArgs& a, cudaStream_t st);
+// forcing coefficient A = eps / (2 E_band) of the compact state u into *A
+template <typename R> void launch_band_forcing(const void* const* u, int D, int K1, int K2, int kc,
+                                               double eps, double* A, cudaStream_t st);
+// FP64 sum over a spectral array of w(kx) * |u|^2 (w = 1 at kx = 0 and kx = n/2, else 2),
+// optionally times nu*k^2; accumulated (atomically) into *out.
+template <typename R> void launch_spectral_energy(const void* const* u, int ncomp, int D, int n,
+                                                  int K1, int K2, int compact, int kc,
+                                                  double kfac, int weight_k2, double* out,
+                                                  cudaStream_t st);
+bool fft_size_supported(int n);
+template <typename R> bool init_kernels(int N);
+template <typename R> void launch_twothirds_full(const PackArgs& a, cudaStream_t st);  // in place on a.dst
+template <typename R> void launch_project_full(const PackArgs& a, double kfac, cudaStream_t st);
+
+}  // namespace sc

@@ -1,0 +1,249 @@
+"""Host-side mirror of SymmetryCode.jl's solver API over the B200 C ABI.
+
+Each function here has the name of the reference function it replaces (an
+in-place Julia ``f!`` becomes ``f_``), the same argument meaning and the same
+array layout, and runs the hand-written sm_100a kernels of ``libsymcode.so``
+through ctypes.  torch provides device memory and streams only.
+
+Field layout: a spectral scalar field of a ``Grid`` is a contiguous complex
+torch tensor of shape ``(n, n/2+1)`` (2D) or ``(n, n, n/2+1)`` (3D) -- in
+memory the reference's column-major ``(n/2+1, n[, n])`` array; vector fields
+are lists ``[x, y(, z)]``, symmetric tensors ``[xx, yy(, zz), xy(, yz, zx)]``.
+"""
+
+from __future__ import annotations
+
+import ctypes as ct
+import math
+
+import torch
+
+from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
+                   ptr_array, sc_forcing)
+
+__all__ = [
+    "Grid", "SymcodeError", "scalarfield", "vectorfield", "tensorfield", "spacescalarfield",
+    "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
+    "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions",
+]
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ct.c_void_p(stream.cuda_stream)
+
+
+class Grid:
+    """``Grid{D}(; l, n)`` + ``getcache(grid)`` (src/solver.jl:131-151, 956-965).
+
+    Creates the device plan (twiddles and all pencil scratch) on ``device``.
+    ``dtype`` is the real precision of the fields (torch.float32 / float64).
+    """
+
+    def __init__(self, D, n, l=2 * math.pi, dtype=torch.float64, device="cuda"):
+        if n % 2 != 0:
+            raise AssertionError("Only even number of grid points supported.")
+        if D not in (2, 3):
+            raise ValueError("D must be 2 or 3")
+        if not torch.cuda.is_available():
+            raise RuntimeError("symcode needs a CUDA device (sm_100a); none is available")
+        self.D, self.n, self.l = D, n, float(l)
+        self.dtype = dtype
+        self.cdtype = torch.complex64 if dtype == torch.float32 else torch.complex128
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        L = lib()
+        plan = ct.c_void_p()
+        ws = ct.c_size_t()
+        with torch.cuda.device(self.device):
+            check(L.sc_plan_create(ct.byref(plan), D, n, self.l,
+                                   SC_FLOAT32 if dtype == torch.float32 else SC_FLOAT64, ct.byref(ws)))
+        self._plan = plan
+        self.workspace_bytes = ws.value
+
+    # reference accessors (src/solver.jl:155-202)
+    @property
+    def tensordim(self):
+        return 3 if self.D == 2 else 6
+
+    @property
+    def spacing(self):
+        return self.l / self.n
+
+    @property
+    def volume(self):
+        return (self.l / self.n) ** self.D
+
+    @property
+    def ndrange(self):
+        return (self.n // 2 + 1,) + (self.n,) * (self.D - 1)
+
+    @property
+    def space_ndrange(self):
+        return (self.n,) * self.D
+
+    @property
+    def spec_shape(self):
+        return tuple(reversed(self.ndrange))
+
+    @property
+    def phys_shape(self):
+        return (self.n,) * self.D
+
+    @property
+    def plan(self):
+        return self._plan
+
+    def close(self):
+        if getattr(self, "_plan", None):
+            with torch.cuda.device(self.device):
+                lib().sc_plan_destroy(self._plan)
+            self._plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- helpers ---------------------------------------------------------
+    def _check_spec(self, t):
+        if t.dtype != self.cdtype or tuple(t.shape) != self.spec_shape or not t.is_contiguous() or t.device != self.device:
+            raise ValueError(f"expected contiguous {self.cdtype} tensor of shape {self.spec_shape} on {self.device}, "
+                             f"got {t.dtype} {tuple(t.shape)} on {t.device}")
+        return t.data_ptr()
+
+    def _check_phys(self, t):
+        if t.dtype != self.dtype or tuple(t.shape) != self.phys_shape or not t.is_contiguous() or t.device != self.device:
+            raise ValueError(f"expected contiguous {self.dtype} tensor of shape {self.phys_shape} on {self.device}")
+        return t.data_ptr()
+
+
+# --------------------------------------------------------------------------
+# field allocators (src/solver.jl:245-300)
+# --------------------------------------------------------------------------
+
+def scalarfield(g: Grid):
+    return torch.zeros(g.spec_shape, dtype=g.cdtype, device=g.device)
+
+
+def vectorfield(g: Grid):
+    return [scalarfield(g) for _ in range(g.D)]
+
+
+def tensorfield(g: Grid):
+    return [scalarfield(g) for _ in range(g.tensordim)]
+
+
+def spacescalarfield(g: Grid):
+    return torch.zeros(g.phys_shape, dtype=g.dtype, device=g.device)
+
+
+def spacevectorfield(g: Grid):
+    return [spacescalarfield(g) for _ in range(g.D)]
+
+
+# --------------------------------------------------------------------------
+# solver calls
+# --------------------------------------------------------------------------
+
+def to_phys_(phys, spec, g: Grid, stream=None):
+    """``to_phys!(phys, spec, plan, g)`` (src/solver.jl:210-211); ``spec`` is preserved."""
+    check(lib().sc_to_phys(g.plan, ct.c_void_p(g._check_spec(spec)), ct.c_void_p(g._check_phys(phys)),
+                           _stream_ptr(stream)))
+    return phys
+
+
+def to_spec_(spec, phys, g: Grid, stream=None):
+    """``to_spec!(spec, phys, plan, g)`` (src/solver.jl:214-215)."""
+    check(lib().sc_to_spec(g.plan, ct.c_void_p(g._check_phys(phys)), ct.c_void_p(g._check_spec(spec)),
+                           _stream_ptr(stream)))
+    return spec
+
+
+def twothirds_(fields, g: Grid, stream=None):
+    """``apply!(twothirds!, g, (u, g))`` on one or several scalar fields (src/solver.jl:371-389)."""
+    if isinstance(fields, torch.Tensor):
+        fields = [fields]
+    pp, _keep = ptr_array([g._check_spec(f) for f in fields])
+    check(lib().sc_twothirds(g.plan, pp, len(fields), _stream_ptr(stream)))
+    return fields
+
+
+def project_(u, g: Grid, stream=None):
+    """``apply!(project!, g, (u, g))`` (src/solver.jl:350-368)."""
+    pp, _keep = ptr_array([g._check_spec(c) for c in u])
+    check(lib().sc_project(g.plan, pp, _stream_ptr(stream)))
+    return u
+
+
+def convectiondiffusion_(du, u, g: Grid, visc, stream=None):
+    """``convectiondiffusion!(du, u, grid, cache; visc)`` (src/solver.jl:949-953).
+
+    ``du`` receives the right-hand side on the modes the 2/3 rule keeps
+    (``twothirds!`` of the reference's ``du``), zero elsewhere.
+    """
+    pu, _k1 = ptr_array([g._check_spec(c) for c in u])
+    pd, _k2 = ptr_array([g._check_spec(c) for c in du])
+    check(lib().sc_rhs(g.plan, pu, pd, float(visc), _stream_ptr(stream)))
+    return du
+
+
+def wray3_(u, dt, g: Grid, visc, stream=None):
+    """``wray3!(convectiondiffusion!, u, Δt, grid, cache; visc)`` (src/solver.jl:968-1012)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    check(lib().sc_wray3_step(g.plan, pu, float(dt), float(visc), _stream_ptr(stream)))
+    return u
+
+
+def rk4_(u, dt, g: Grid, visc, nsteps=1, eps=None, stream=None):
+    """``nsteps`` RK4 steps with optional linear band forcing at injection rate ``eps`` (new)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    f = sc_forcing(1 if eps is not None else 0, float(eps) if eps is not None else 0.0)
+    check(lib().sc_rk4_steps(g.plan, pu, float(dt), float(visc), int(nsteps), ct.byref(f), _stream_ptr(stream)))
+    return u
+
+
+def energy(u, g: Grid, stream=None):
+    """``energy(u)`` (src/solver.jl:643-646), accumulated in FP64 on the device."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    out = ct.c_double()
+    check(lib().sc_energy(g.plan, pu, ct.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+def get_dissipation(u, visc, g: Grid, stream=None):
+    """``get_dissipation!`` (src/solver.jl:808-811), FP64 on the device."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    out = ct.c_double()
+    check(lib().sc_dissipation(g.plan, pu, float(visc), ct.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+class State:
+    """Device-resident compact state of a plan (sc_state_* entry points)."""
+
+    def __init__(self, g: Grid):
+        self.g = g
+
+    def load(self, u, stream=None):
+        pu, _k = ptr_array([self.g._check_spec(c) for c in u])
+        check(lib().sc_state_load(self.g.plan, pu, _stream_ptr(stream)))
+
+    def store(self, u, stream=None):
+        pu, _k = ptr_array([self.g._check_spec(c) for c in u])
+        check(lib().sc_state_store(self.g.plan, pu, _stream_ptr(stream)))
+
+    def rk4(self, dt, visc, nsteps=1, eps=None, stream=None):
+        f = sc_forcing(1 if eps is not None else 0, float(eps) if eps is not None else 0.0)
+        check(lib().sc_state_rk4(self.g.plan, float(dt), float(visc), int(nsteps), ct.byref(f), _stream_ptr(stream)))
+
+    def energy(self, stream=None):
+        out = ct.c_double()
+        check(lib().sc_state_energy(self.g.plan, ct.byref(out), _stream_ptr(stream)))
+        return out.value
+
+    def launches_per_step(self, forced):
+        return lib().sc_state_rk4_launches_per_step(self.g.plan, 1 if forced else 0)
