@@ -1,0 +1,385 @@
+"""Benchmark: 810^3 FP32 forced DNS, RK4 steps/s on one B200 (per GPU replica).
+
+Workload (the 810^3 DNS configuration): grid 810^3 on [0, 2pi)^3, FP32 bulk,
+nu = 6e-4, dt = 2e-3, classical RK4 with linear band forcing eps = 0.1 on
+1 <= |k|^2 < 9, 2/3 dealiasing; seeded synthetic initial field (numpy PCG64
+seed 2, spectrum E(k) ~ k^4 exp(-2 (k/4)^2), solenoidal, unit energy).  A
+"step" is one RK4 step (4 right-hand sides) of the whole field.  The state
+(3 x 634 MB compact spectra) and every sweep's operands exceed L2 (126 MB), so
+no L2 flush is needed between steps.
+
+value   : steps/s with the state resident in HBM (device-timed, CUDA events on
+          the launching stream, max over ranks; ranks run independent replicas).
+e2e     : the same metric through the public C ABI with host buffers: pinned
+          host -> device copy of the full-layout field, sc_state_load, K calls
+          of sc_state_rk4 (1 step) each followed by the per-step energy read to
+          the host (the reference's blow-up guard reads energy every step,
+          src/les.jl:224-237), sc_state_store and the device -> host copy.
+roofline: dominant kernel of one right-hand side, algorithmic bytes per launch
+          / its CUDA-event time, against MEASURED_PEAKS.json hbm_gbs.
+
+`--impl reference` times the reference path's CPU restatement (the FP64 numpy /
+scipy.fft oracle, all host threads) on a bounded sample and reports it scaled
+to the same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "symmetrycode.jl_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "810³ DNS RK4 steps/s (err vs FP64); batched LES+adjoint steps/s vs plain"
+UNIT = "steps/s"
+N_GRID = 810
+NU, DT, EPS, KPEAK, SEED = 6e-4, 2e-3, 0.1, 4.0, 2
+WORKLOAD = (f"{N_GRID}^3 forced DNS, RK4, FP32 (nu={NU}, dt={DT}, linear band forcing eps={EPS} "
+            f"on 1<=|k|^2<9, k_p={KPEAK:g}, seed {SEED})")
+
+
+def algorithmic_bytes(n, esize):
+    """Compulsory HBM bytes of one right-hand side of the 5-sweep pruned pipeline.
+
+    k = n//3, kx = k+1, kt = 2k+1; a = kx kt kt e, b = kx kt n e, c = kx n n e.
+    Returns per-kernel bytes (z-inv, y-inv, x, y-fwd, z-fwd+epilogue) and the total.
+    """
+    k = n // 3
+    kx, kt = k + 1, 2 * k + 1
+    a = kx * kt * kt * esize
+    b = kx * kt * n * esize
+    c = kx * n * n * esize
+    per = {
+        "z_inverse": 3 * (a + b),
+        "y_inverse": 3 * (b + c),
+        "x_sweep": 3 * c + 6 * c,
+        "y_forward": 6 * (c + b),
+        "z_forward_epilogue": 6 * b + 12 * a,
+    }
+    return per, sum(per.values())
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    def __init__(self, path):
+        self.path = path
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self, gpu_index):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.proc is None or not os.path.exists(self.path):
+            return out
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                if int(parts[0]) != gpu_index:
+                    continue
+                sms.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if sms:
+            sms.sort()
+            out["sm_mhz"] = sms[len(sms) // 2]
+            out["sm_max_mhz"] = mx
+            out["reasons"] = sorted(reasons)
+        return out
+
+
+def init_dist():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def initial_compact(n, seed):
+    """Seeded compact FP64 initial field (same generator and bytes as the parity tests)."""
+    import oracle as O
+    return O.random_field_compact(3, n, seed, kpeak=KPEAK, totalenergy=1.0)
+
+
+def to_full(uc, n, dtype):
+    import numpy as np
+    import torch
+    import oracle as O
+    g = O.Grid(3, n)
+    cd = np.complex64 if dtype == torch.float32 else np.complex128
+    return [torch.from_numpy(O.unpack_retained(c.astype(cd), g)) for c in uc]
+
+
+def cpu_sample_steps(n, nsteps=1):
+    """Time `nsteps` forced RK4 steps of the FP64 oracle at n^3 on all host threads."""
+    import oracle as O
+    g = O.Grid(3, n)
+    u = O.random_field(g, seed=SEED, kpeak=KPEAK)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        u = O.rk4_step(u, DT, g, NU, EPS)
+    return (time.perf_counter() - t0) / nsteps
+
+
+def scale_to_810(sec_per_step, n):
+    """FFT-dominated cost ~ N log N with N = n^3: seconds per 810^3 step."""
+    f = (N_GRID ** 3 * math.log2(N_GRID ** 3)) / (n ** 3 * math.log2(n ** 3))
+    return sec_per_step * f
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    # largest sample grid whose W + K steps fit in about three minutes
+    t128 = cpu_sample_steps(128, 1)
+    sample_n = 128
+    for cand in (192, 256):
+        est = t128 * (cand / 128) ** 3 * math.log2(cand ** 3) / math.log2(128 ** 3)
+        if est * (args.steps + args.warmup) <= 180:
+            sample_n = cand
+    for _ in range(args.warmup):
+        cpu_sample_steps(sample_n, 1)
+    times = [cpu_sample_steps(sample_n, 1) for _ in range(args.steps)]
+    sps = 1.0 / scale_to_810(sum(times) / len(times), sample_n)
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": sps, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": N_GRID},
+        "cpu_baseline": {"value": sps, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} forced RK4 step(s) of the FP64 numpy/scipy.fft (pocketfft, "
+                                   f"{cores} threads) restatement of the reference at {sample_n}^3, scaled to "
+                                   f"810^3 by N log N (Julia/FFTW reference unavailable: no Julia toolchain)"},
+        "e2e": {"value": sps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    import symcode as S
+
+    ws, rank, local = init_dist()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n = args.n
+    g = S.Grid(3, n, 2 * math.pi, dtype=torch.float32, device=dev)
+    st = S.State(g)
+    uc = initial_compact(n, SEED + rank)
+    host = to_full(uc, n, torch.float32)
+    u = [c.to(dev) for c in host]
+    st.load(u)
+    stream = torch.cuda.current_stream()
+    forced = True
+    launches_per_step = st.launches_per_step(forced)
+
+    # FP32 vs FP64 error of one RK4 step (relative L2 on the state)
+    err = None
+    if not args.skip_fp64 and rank == 0:
+        g64 = S.Grid(3, n, 2 * math.pi, dtype=torch.float64, device=dev)
+        u64 = [c.to(dev) for c in to_full(uc, n, torch.float64)]
+        S.rk4_(u64, DT, g64, NU, nsteps=1, eps=EPS)
+        u32 = [c.clone() for c in u]
+        S.rk4_(u32, DT, g, NU, nsteps=1, eps=EPS)
+        num = sum(float((a.to(torch.complex128) - b).abs().pow(2).sum()) for a, b in zip(u32, u64))
+        den = sum(float(b.abs().pow(2).sum()) for b in u64)
+        err = math.sqrt(num / den)
+        del u64, u32
+        g64.close()
+        torch.cuda.empty_cache()
+
+    # warm-up
+    for _ in range(args.warmup):
+        st.rk4(DT, NU, 1, EPS)
+    torch.cuda.synchronize()
+
+    # timed region: K steps, state resident
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                            f"clocks_rank{rank}.csv")
+    with ClockSampler(clk_path) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            st.rk4(DT, NU, 1, EPS)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, ws)
+    value = ws * args.steps / (ms / 1e3)
+    energy_after = st.energy()
+    if not math.isfinite(energy_after):
+        raise RuntimeError("state diverged during the benchmark")
+
+    # live per-kernel profile (CUDA events around each kernel of one RHS)
+    prof = st.profile_rhs(NU, reps=3)
+    names = ["z_inverse", "y_inverse", "x_sweep", "y_forward", "z_forward", "epilogue"]
+    kms = dict(zip(names, prof))
+    per, b_rhs = algorithmic_bytes(n, 8)
+    # this build splits the last sweep: z_forward reads 6b, writes 6a; the
+    # epilogue reads the 6a products plus the RK4 state (12a)
+    k = n // 3
+    a = (k + 1) * (2 * k + 1) ** 2 * 8
+    b = (k + 1) * (2 * k + 1) * n * 8
+    alg = {"z_inverse": per["z_inverse"], "y_inverse": per["y_inverse"], "x_sweep": per["x_sweep"],
+           "y_forward": per["y_forward"], "z_forward": 6 * b + 6 * a, "epilogue": 6 * a + 12 * a}
+    dom = max(kms, key=lambda kk: kms[kk])
+    hbm, src = peaks()
+    achieved = alg[dom] / (kms[dom] / 1e3) / 1e9
+    step_bytes = 4 * b_rhs
+    step_gbs = step_bytes * (value / ws) / 1e9
+
+    # e2e through the public C ABI with host buffers
+    pinned = [c.pin_memory() for c in host]
+    out_host = [torch.empty_like(c).pin_memory() for c in host]
+    dev_u = [torch.empty_like(c, device=dev) for c in host]
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for c, h in zip(dev_u, pinned):
+        c.copy_(h, non_blocking=True)
+    st.load(dev_u)
+    for _ in range(args.steps):
+        st.rk4(DT, NU, 1, EPS)
+        e = st.energy()  # synchronous D2H of the FP64 energy
+        if not (e < 1e5):
+            raise RuntimeError("blow-up guard tripped")
+    st.store(dev_u)
+    for c, h in zip(dev_u, out_host):
+        h.copy_(c, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    state_bytes = sum(c.numel() * c.element_size() for c in host)
+    e2e = {"value": ws * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": state_bytes / args.steps + 8}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.skip_cpu:
+        sec = cpu_sample_steps(args.cpu_sample_n, 1)
+        v = 1.0 / scale_to_810(sec, args.cpu_sample_n)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"1 forced RK4 step of the FP64 numpy/scipy.fft restatement at {args.cpu_sample_n}^3 "
+                         f"({sec:.2f} s on {os.cpu_count()} threads), scaled to 810^3 by N log N"}
+
+    if rank == 0:
+        clocks = clk.summary(local)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": n, "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                       "l2": "inputs larger than L2 (5.7 GB compact state; every sweep streams >1 GB)",
+                       "err_vs_fp64_one_step": err},
+            "grid_points_per_s": value * n ** 3,
+            "step_hbm": {"algorithmic_bytes_per_step": step_bytes, "achieved_gbs": step_gbs,
+                         "frac": step_gbs / hbm},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "kernel_ms": kms, "kernel_algorithmic_bytes": alg},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_GRID)
+    ap.add_argument("--cpu-sample-n", type=int, default=256)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-fp64", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

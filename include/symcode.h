@@ -128,6 +128,12 @@ SC_API int sc_state_store(sc_plan* plan, void* const* u_hat, void* stream);
 SC_API int sc_state_rk4(sc_plan* plan, double dt, double visc, int nsteps, const sc_forcing* forcing, void* stream);
 /* energy(u) (src/solver.jl:643-646) of the plan's state, FP64, synchronous. */
 SC_API int sc_state_energy(sc_plan* plan, double* energy, void* stream);
+/* Profiling hook: run the right-hand side of the plan's state `reps` times
+ * with CUDA events between its kernels and return the mean time (ms) of each
+ * kernel in launch order -- 3D: z-inverse, y-inverse, x sweep, y-forward,
+ * z-forward, epilogue; 2D: y-inverse, x sweep, y-forward, epilogue.
+ * `ms` must hold 8 doubles.  Synchronous. */
+SC_API int sc_state_profile_rhs(sc_plan* plan, double visc, int reps, double* ms, int* nkernels, void* stream);
 /* Number of kernels one sc_state_rk4 step launches (for launch accounting). */
 SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
 

@@ -112,9 +112,13 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // ---------------------------------------------------------------------------
 // the five-sweep product pipeline: compact u -> compact F[u_i u_j]/n^D in p->sig
 // ---------------------------------------------------------------------------
+// `ev` (optional): events recorded after each launch, ev[0] before the first.
 template <typename R>
-int products(sc_plan* p, void* const* u, cudaStream_t st) {
+int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+  int iev = 0;
+  auto mark = [&]() { if (ev) cudaEventRecord(ev[iev++], st); };
+  mark();
   sc::ColArgs a{};
   if (p->D == 3) {
     for (int c = 0; c < 3; ++c) { a.in[c] = u[c]; a.out[c] = p->be[c]; }
@@ -122,46 +126,54 @@ int products(sc_plan* p, void* const* u, cudaStream_t st) {
     a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
     a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
     if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
+    mark();
     sc::ColArgs b{};
     for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
     b.ncomp = 3; b.K1 = K1; b.ncols = n;
     b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
     b.kpos = kc + 1; b.kneg = kc;
     sc::launch_col_inv<R>(n, b, p->tw, st);
+    mark();
     sc::XArgs x{};
     for (int c = 0; c < 3; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 6; ++c) x.out[c] = p->dd[c];
     x.D = 3; x.K1in = K1; x.K1out = K1; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
+    mark();
     sc::ColArgs f{};
     for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
     f.ncomp = 6; f.K1 = K1; f.ncols = n;
     f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = (long long)K1 * K2; f.out_es = K1;
     f.kpos = kc + 1; f.kneg = kc;
     sc::launch_col_fwd<R>(n, f, p->tw, st);
+    mark();
     sc::ColArgs g{};
     for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = p->sig[c]; }
     g.ncomp = 6; g.K1 = K1; g.ncols = K2;
     g.in_cs = K1; g.in_es = (long long)K1 * K2; g.out_cs = K1; g.out_es = (long long)K1 * K2;
     g.kpos = kc + 1; g.kneg = kc;
     sc::launch_col_fwd<R>(n, g, p->tw, st);
+    mark();
   } else {
     for (int c = 0; c < 2; ++c) { a.in[c] = u[c]; a.out[c] = p->cc[c]; }
     a.ncomp = 2; a.K1 = K1; a.ncols = 1;
     a.in_cs = 0; a.in_es = K1; a.out_cs = 0; a.out_es = K1;
     a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
     if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
+    mark();
     sc::XArgs x{};
     for (int c = 0; c < 2; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 3; ++c) x.out[c] = p->dd[c];
     x.D = 2; x.K1in = K1; x.K1out = K1; x.nrows = n; x.scale = 1.0 / ((double)n * n);
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
+    mark();
     sc::ColArgs f{};
     for (int c = 0; c < 3; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->sig[c]; }
     f.ncomp = 3; f.K1 = K1; f.ncols = 1;
     f.in_cs = 0; f.in_es = K1; f.out_cs = 0; f.out_es = K1;
     f.kpos = kc + 1; f.kneg = kc;
     sc::launch_col_fwd<R>(n, f, p->tw, st);
+    mark();
   }
   return check_launch("product pipeline");
 }
@@ -554,6 +566,40 @@ int sc_wray3_step(sc_plan* p, void* const* u, double dt, double visc, void* stre
   rc = SC_DTYPE_DISPATCH(p, run_wray_graph, p, dt, visc, as_stream(stream));
   if (rc) return rc;
   return sc_state_store(p, u, stream);
+}
+
+int sc_state_profile_rhs(sc_plan* p, double visc, int reps, double* ms, int* nkernels, void* stream) {
+  if (!p || !ms || !nkernels || reps < 1) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const int nk = (p->D == 3 ? 5 : 3) + 1;
+  cudaEvent_t ev[8];
+  for (int i = 0; i <= nk; ++i) SC_CU(cudaEventCreate(&ev[i]));
+  for (int i = 0; i < nk; ++i) ms[i] = 0;
+  auto body = [&](auto tag) -> int {
+    using R = decltype(tag);
+    for (int r = 0; r < reps; ++r) {
+      int q = products<R>(p, p->U, st, ev);
+      if (q) return q;
+      sc::EpiArgs e = epi_base<R>(p, p->U, visc);
+      for (int c = 0; c < p->D; ++c) { e.base_a[c] = nullptr; e.out_a[c] = p->ACC[c]; }
+      e.ca = 1.0;
+      sc::launch_epilogue<R>(e, st);
+      cudaEventRecord(ev[nk], st);
+      SC_CU(cudaEventSynchronize(ev[nk]));
+      for (int i = 0; i < nk; ++i) {
+        float t = 0;
+        SC_CU(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+        ms[i] += t / reps;
+      }
+    }
+    return check_launch("profile");
+  };
+  rc = p->dtype == SC_FLOAT64 ? body(double()) : body(float());
+  for (int i = 0; i <= nk; ++i) cudaEventDestroy(ev[i]);
+  *nkernels = nk;
+  return rc;
 }
 
 int sc_state_energy(sc_plan* p, double* e, void* stream) {

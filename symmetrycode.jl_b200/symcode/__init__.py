@@ -245,5 +245,12 @@ class State:
         check(lib().sc_state_energy(self.g.plan, ct.byref(out), _stream_ptr(stream)))
         return out.value
 
+    def profile_rhs(self, visc, reps=3, stream=None):
+        """Mean ms per kernel of one right-hand side (sc_state_profile_rhs)."""
+        ms = (ct.c_double * 8)()
+        nk = ct.c_int()
+        check(lib().sc_state_profile_rhs(self.g.plan, float(visc), int(reps), ms, ct.byref(nk), _stream_ptr(stream)))
+        return list(ms[: nk.value])
+
     def launches_per_step(self, forced):
         return lib().sc_state_rk4_launches_per_step(self.g.plan, 1 if forced else 0)
