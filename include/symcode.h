@@ -134,6 +134,14 @@ SC_API int sc_state_energy(sc_plan* plan, double* energy, void* stream);
  * z-forward, epilogue; 2D: y-inverse, x sweep, y-forward, epilogue.
  * `ms` must hold 8 doubles.  Synchronous. */
 SC_API int sc_state_profile_rhs(sc_plan* plan, double visc, int reps, double* ms, int* nkernels, void* stream);
+/* Microbenchmark of one sweep kernel on zero-filled synthetic buffers of the
+ * right shape (allocated and freed inside; legacy default stream):
+ * kernel 0 = y-inverse sweep (3 comps) over `count` z planes, 1 = y-forward
+ * sweep (6 comps) over `count` z planes, 2 = the 3D x sweep with products over
+ * `count` rows.  Returns the mean ms per launch over `reps` launches and the
+ * algorithmic bytes of one launch.  Synchronous; used by the profiles and the
+ * tile autotuning, not by the solver. */
+SC_API int sc_microbench(int kernel, int n, int dtype, long long count, int reps, double* ms, double* bytes);
 /* Number of kernels one sc_state_rk4 step launches (for launch accounting). */
 SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
 

@@ -602,6 +602,88 @@ int sc_state_profile_rhs(sc_plan* p, double visc, int reps, double* ms, int* nke
   return rc;
 }
 
+}  // extern "C"
+
+namespace {
+template <typename R>
+int microbench_impl(int kernel, int n, long long count, int reps, double* ms, double* bytes) {
+  const int kc = n / 3, K1 = kc + 1, K2 = 2 * kc + 1;
+  const size_t esz = sizeof(typename sc::V2<R>::T);
+  std::vector<void*> bufs;
+  auto alloc = [&](size_t elems) -> void* {
+    void* ptr = nullptr;
+    if (cudaMalloc(&ptr, elems * esz) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    cudaMemset(ptr, 0, elems * esz);
+    bufs.push_back(ptr);
+    return ptr;
+  };
+  auto cleanup = [&]() { for (void* b : bufs) cudaFree(b); };
+  void* tw = alloc(n);
+  if (!tw) { cleanup(); return fail(SC_ERR_OOM, "microbench allocation failed"); }
+  {  // real twiddles so the arithmetic matches the solver's
+    std::vector<typename sc::V2<R>::T> h(n);
+    for (int m = 0; m < n; ++m) {
+      const long double th = 2.0L * 3.141592653589793238462643383279502884L * m / n;
+      h[m].x = (R)cosl(th); h[m].y = (R)(-sinl(th));
+    }
+    cudaMemcpy(tw, h.data(), n * esz, cudaMemcpyHostToDevice);
+  }
+  if (!(esz == 8 ? sc::init_kernels<float>(n) : sc::init_kernels<double>(n))) { cleanup(); return fail(SC_ERR_SIZE, "n"); }
+  sc::ColArgs ca{};
+  sc::XArgs xa{};
+  double b = 0;
+  const int nin = kernel == 1 ? 6 : 3, nout = kernel == 0 ? 3 : 6;
+  if (kernel == 0 || kernel == 1) {  // y-inverse / y-forward geometry over `count` z planes
+    const size_t small = (size_t)K1 * K2 * count, big = (size_t)K1 * n * count;
+    for (int c = 0; c < nin; ++c) ca.in[c] = alloc(kernel == 0 ? small : big);
+    for (int c = 0; c < nout; ++c) ca.out[c] = alloc(kernel == 0 ? big : small);
+    ca.ncomp = nout; ca.K1 = K1; ca.ncols = (int)count; ca.kpos = kc + 1; ca.kneg = kc;
+    if (kernel == 0) { ca.in_cs = (long long)K1 * K2; ca.in_es = K1; ca.out_cs = (long long)K1 * n; ca.out_es = K1; }
+    else { ca.in_cs = (long long)K1 * n; ca.in_es = K1; ca.out_cs = (long long)K1 * K2; ca.out_es = K1; }
+    b = (double)nin * esz * (kernel == 0 ? small : big) + (double)nout * esz * (kernel == 0 ? big : small);
+  } else if (kernel == 2) {  // 3D x sweep over `count` rows
+    for (int c = 0; c < 3; ++c) xa.in[c] = alloc((size_t)K1 * count);
+    for (int c = 0; c < 6; ++c) xa.out[c] = alloc((size_t)K1 * count);
+    xa.D = 3; xa.K1in = K1; xa.K1out = K1; xa.nrows = count; xa.scale = 1.0 / ((double)n * n * n);
+    b = 9.0 * K1 * count * esz;
+  } else {
+    cleanup();
+    return fail(SC_ERR_INVALID, "unknown microbench kernel %d", kernel);
+  }
+  for (void* q : bufs) if (!q) { cleanup(); return fail(SC_ERR_OOM, "microbench allocation failed"); }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0); cudaEventCreate(&e1);
+  auto launch = [&]() {
+    if (kernel == 0) sc::launch_col_inv<R>(n, ca, tw, 0);
+    else if (kernel == 1) sc::launch_col_fwd<R>(n, ca, tw, 0);
+    else sc::launch_xsweep_ns<R>(n, xa, tw, 0);
+  };
+  launch();
+  cudaEventRecord(e0, 0);
+  for (int r = 0; r < reps; ++r) launch();
+  cudaEventRecord(e1, 0);
+  cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0); cudaEventDestroy(e1);
+  int rc = check_launch("microbench");
+  cleanup();
+  if (rc) return rc;
+  *ms = t / reps;
+  *bytes = b;
+  return SC_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sc_microbench(int kernel, int n, int dtype, long long count, int reps, double* ms, double* bytes) {
+  if (!ms || !bytes || reps < 1 || count < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (!sc::fft_size_supported(n)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
+  return dtype == SC_FLOAT64 ? microbench_impl<double>(kernel, n, count, reps, ms, bytes)
+                             : microbench_impl<float>(kernel, n, count, reps, ms, bytes);
+}
+
 int sc_state_energy(sc_plan* p, double* e, void* stream) {
   if (!p || !e) return fail(SC_ERR_INVALID, "null argument");
   int rc = ensure_device(p);

@@ -69,26 +69,43 @@ k_col_inv(const ColArgs a, const typename V2<R>::T* __restrict__ tw) {
   const C* __restrict__ in = static_cast<const C*>(a.in[src]);
   C* __restrict__ out = static_cast<C*>(a.out[q]);
   const int Kc = a.kpos + a.kneg;
-  for (int idx = threadIdx.x; idx < T * N; idx += NT) {
+  // all loads of the tile are issued before the first shared-memory store so
+  // that each thread keeps LPT requests in flight
+  constexpr int LPT = (T * N + NT - 1) / NT;
+  C v[LPT];
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
     const int t = idx % T, e = idx / T;
     const int kx = kx0 + t;
-    C v = mk<C>(R(0), R(0));
+    v[i] = mk<C>(R(0), R(0));
     const int p = compact_pos(e, N, a.kpos, a.kneg);
-    if (kx < a.K1 && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
-      v = in[kx + (long long)c * a.in_cs + (long long)p * a.in_es];
+    if ((T * N % NT == 0 || idx < T * N) && kx < a.K1 && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0))
+      v[i] = in[kx + (long long)c * a.in_cs + (long long)p * a.in_es];
+  }
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
+    if (T * N % NT == 0 || idx < T * N) {
+      const int t = idx % T, e = idx / T;
+      C w = v[i];
       if (drv) {  // multiply by i k_e
+        const int p = compact_pos(e, N, a.kpos, a.kneg);
         const R kk = R(a.kfac * double(p < a.kpos ? p : p - Kc));
-        v = mk<C>(-kk * v.y, kk * v.x);
+        w = mk<C>(-kk * w.y, kk * w.x);
       }
+      s[e * T + t] = w;
     }
-    s[e * T + t] = v;
   }
   __syncthreads();
   tile_fft<C, N, T, NT, true, true>(s, tw);
-  for (int idx = threadIdx.x; idx < T * N; idx += NT) {
+#pragma unroll 4
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
     const int t = idx % T, e = idx / T;
     const int kx = kx0 + t;
-    if (kx < a.K1) out[kx + (long long)c * a.out_cs + (long long)e * a.out_es] = s[e * T + t];
+    if ((T * N % NT == 0 || idx < T * N) && kx < a.K1)
+      out[kx + (long long)c * a.out_cs + (long long)e * a.out_es] = s[e * T + t];
   }
 }
 
@@ -103,20 +120,31 @@ k_col_fwd(const ColArgs a, const typename V2<R>::T* __restrict__ tw) {
   const int c = blockIdx.y;
   const C* __restrict__ in = static_cast<const C*>(a.in[blockIdx.z]);
   C* __restrict__ out = static_cast<C*>(a.out[blockIdx.z]);
-  for (int idx = threadIdx.x; idx < T * N; idx += NT) {
+  constexpr int LPT = (T * N + NT - 1) / NT;
+  C v[LPT];
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
     const int t = idx % T, e = idx / T;
     const int kx = kx0 + t;
-    C v = mk<C>(R(0), R(0));
-    if (kx < a.K1) v = in[kx + (long long)c * a.in_cs + (long long)e * a.in_es];
-    s[e * T + t] = v;
+    v[i] = mk<C>(R(0), R(0));
+    if ((T * N % NT == 0 || idx < T * N) && kx < a.K1) v[i] = in[kx + (long long)c * a.in_cs + (long long)e * a.in_es];
+  }
+#pragma unroll
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
+    if (T * N % NT == 0 || idx < T * N) s[(idx / T) * T + idx % T] = v[i];
   }
   __syncthreads();
   tile_fft<C, N, T, NT, false, true>(s, tw);
-  for (int idx = threadIdx.x; idx < T * N; idx += NT) {
+#pragma unroll 4
+  for (int i = 0; i < LPT; ++i) {
+    const int idx = threadIdx.x + i * NT;
     const int t = idx % T, e = idx / T;
     const int kx = kx0 + t;
     const int p = compact_pos(e, N, a.kpos, a.kneg);
-    if (kx < a.K1 && p >= 0) out[kx + (long long)c * a.out_cs + (long long)p * a.out_es] = s[e * T + t];
+    if ((T * N % NT == 0 || idx < T * N) && kx < a.K1 && p >= 0)
+      out[kx + (long long)c * a.out_cs + (long long)p * a.out_es] = s[e * T + t];
   }
 }
 
@@ -160,17 +188,30 @@ k_xsweep_ns(const XArgs a, const typename V2<R>::T* __restrict__ tw) {
   const C* in0 = static_cast<const C*>(a.in[0]);
   const C* in1 = static_cast<const C*>(a.in[1]);
   const C* in2 = D == 3 ? static_cast<const C*>(a.in[2]) : nullptr;
-  for (int idx = threadIdx.x; idx < TR * N; idx += NT) {
-    const int t = idx / N, f = idx % N;
-    const long long row = row0 + t;
-    C z1 = mk<C>(R(0), R(0)), z2 = mk<C>(R(0), R(0));
-    if (row < a.nrows) {
-      const long long off = row * a.K1in;
-      z1 = pack_pair(hext<C, N>(in0 + off, a.K1in, f), hext<C, N>(in1 + off, a.K1in, f));
-      if (D == 3) z2 = hext<C, N>(in2 + off, a.K1in, f);
+  {
+    constexpr int LPT = (TR * N + NT - 1) / NT;
+    C z1[LPT], z2[LPT];
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      const int t = idx / N, f = idx % N;
+      const long long row = row0 + t;
+      z1[i] = mk<C>(R(0), R(0));
+      z2[i] = mk<C>(R(0), R(0));
+      if ((TR * N % NT == 0 || idx < TR * N) && row < a.nrows) {
+        const long long off = row * a.K1in;
+        z1[i] = pack_pair(hext<C, N>(in0 + off, a.K1in, f), hext<C, N>(in1 + off, a.K1in, f));
+        if (D == 3) z2[i] = hext<C, N>(in2 + off, a.K1in, f);
+      }
     }
-    s0[t * N + f] = z1;
-    if (D == 3) s1[t * N + f] = z2;
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      if (TR * N % NT == 0 || idx < TR * N) {
+        s0[idx] = z1[i];
+        if (D == 3) s1[idx] = z2[i];
+      }
+    }
   }
   __syncthreads();
   // inverse transforms: TR pencils (2D) or 2*TR pencils (3D, buffers 0 and 1)
