@@ -1,0 +1,362 @@
+// Two-level register FFT sweeps for the FP32 solver sizes (sm_100a).
+//
+// A length-N transform is split N = N1 * N2 (810 = 27 * 30, 256 = 16 * 16,
+// 128 = 16 * 8, 64 = 8 * 8):
+//   step 1  thread (pencil, n2) gathers x[N2 n1 + n2], n1 = 0..N1-1, straight
+//           from global memory into registers, runs a radix-N1 DFT in
+//           registers, multiplies by exp(-+2 pi i n2 k1 / N) and writes one
+//           row of the shared exchange buffer;
+//   step 2  thread (pencil, k1) reads the N2 values of its column, runs a
+//           radix-N2 DFT in registers and stores X[k1 + N1 k2] straight to
+//           global memory (pruned to the retained modes on the forward side).
+// Each element crosses shared memory once (one store, one load) instead of
+// once per radix pass, and every thread keeps N1 independent global loads in
+// flight.  These kernels replace the Stockham-engine sweeps of sc_kernels.cu
+// for FP32 at the sizes of the DNS and LES configurations; the results are the
+// same transforms (tests compare both against the FP64 oracle).
+#include "sc_fft.cuh"
+#include "sc_internal.h"
+
+namespace sc {
+
+template <int N> struct Split;
+template <> struct Split<810> { static constexpr int N1 = 27, N2 = 30; };
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<128> { static constexpr int N1 = 16, N2 = 8; };
+template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+
+__device__ __forceinline__ int cpos(int f, int N, int kpos, int kneg) {
+  return f < kpos ? f : (f >= N - kneg ? f - N + kpos + kneg : -1);
+}
+
+// ---------------------------------------------------------------------------
+// column sweeps: tile of T consecutive kx, one column c, all N elements
+// ---------------------------------------------------------------------------
+template <int N, int T> struct Col2Cfg {
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  static constexpr int NJ = N1 > N2 ? N1 : N2;
+  static constexpr int NT = T * NJ;
+  static constexpr int SR = N2 * T + 8;  // exchange row stride (+8: half-bank shift between rows)
+  static constexpr size_t SMEM = size_t(N1) * SR * sizeof(float2);
+};
+
+template <int N, int T, bool INV>
+__global__ void __launch_bounds__(Col2Cfg<N, T>::NT)
+k_col2(const ColArgs a, const float2* __restrict__ tw) {
+  using C = float2;
+  using Cfg = Col2Cfg<N, T>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, SR = Cfg::SR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* ys = reinterpret_cast<C*>(smem_raw);
+  const int t = threadIdx.x % T, j = threadIdx.x / T;
+  const int kx = blockIdx.x * T + t;
+  const int c = blockIdx.y;
+  const int q = blockIdx.z;
+  const bool drv = q >= a.ncomp;
+  const C* __restrict__ in = static_cast<const C*>(a.in[drv ? a.drv_src[q - a.ncomp] : q]);
+  C* __restrict__ out = static_cast<C*>(a.out[q]);
+  const bool live = kx < a.K1;
+  const int Kc = a.kpos + a.kneg;
+  if (j < N2) {
+    C v[N1];
+    const C* base = in + kx + (long long)c * a.in_cs;
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int e = N2 * n1 + j;
+      v[n1] = mk<C>(0.f, 0.f);
+      if (INV) {
+        const int p = cpos(e, N, a.kpos, a.kneg);
+        if (live && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
+          v[n1] = __ldg(base + (long long)p * a.in_es);
+          if (drv) {
+            const float kk = float(a.kfac * double(p < a.kpos ? p : p - Kc));
+            v[n1] = mk<C>(-kk * v[n1].y, kk * v[n1].x);
+          }
+        }
+      } else if (live) {
+        v[n1] = __ldg(base + (long long)e * a.in_es);
+      }
+    }
+    DFT<N1, INV, C>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+      C w = __ldg(&tw[j * k1]);
+      if (INV) w.y = -w.y;
+      v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) ys[k1 * SR + j * T + t] = v[k1];
+  }
+  __syncthreads();
+  if (j < N1 && live) {
+    C w[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = ys[j * SR + n2 * T + t];
+    DFT<N2, INV, C>::run(w);
+    C* obase = out + kx + (long long)c * a.out_cs;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int e = j + N1 * k2;
+      if (INV) {
+        obase[(long long)e * a.out_es] = w[k2];
+      } else {
+        const int p = cpos(e, N, a.kpos, a.kneg);
+        if (p >= 0) obase[(long long)p * a.out_es] = w[k2];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x sweep with the Navier-Stokes products (rows are contiguous)
+// ---------------------------------------------------------------------------
+template <int N> struct X2Rows;
+template <> struct X2Rows<810> { static constexpr int TR = 2; };
+template <> struct X2Rows<256> { static constexpr int TR = 4; };
+template <> struct X2Rows<128> { static constexpr int TR = 8; };
+template <> struct X2Rows<64> { static constexpr int TR = 16; };
+
+template <int N, int D> struct X2Cfg {
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, N2P = N2 + 1;
+  static constexpr int TR = X2Rows<N>::TR;
+  static constexpr int K1M = N / 3 + 1;           // widest input row (2/3-truncated spectrum)
+  static constexpr int NPI = D == 3 ? 2 * TR : TR;   // inverse pencils
+  static constexpr int NPF = D == 3 ? 3 * TR : 2 * TR;  // forward pencils
+  static constexpr int NT = 192;
+  static constexpr size_t RIN = size_t(D) * TR * K1M * sizeof(float2);
+  static constexpr size_t UPH = size_t(D) * TR * N * sizeof(float);
+  static constexpr size_t ZB = size_t(NPF) * (2 * K1M - 1) * sizeof(float2);
+  static constexpr size_t A0 = (RIN + UPH) > ZB ? (RIN + UPH) : ZB;  // Rin+U, later aliased by Z
+  static constexpr size_t YB = size_t(NPF) * N1 * N2P * sizeof(float2);
+  static constexpr size_t SMEM = A0 + YB;
+};
+
+template <int N> __device__ __forceinline__ float2 hext2(const float2* row, int K1, int f) {
+  const int kmax = K1 - 1;
+  if (f == 0) return make_float2(row[0].x, 0.f);
+  if (f <= kmax) return row[f];
+  if (f >= N - kmax) { const float2 v = row[N - f]; return make_float2(v.x, -v.y); }
+  return make_float2(0.f, 0.f);
+}
+
+template <int N, int D>
+__global__ void __launch_bounds__(X2Cfg<N, D>::NT)
+k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
+  using C = float2;
+  using Cfg = X2Cfg<N, D>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, N2P = Cfg::N2P, TR = Cfg::TR, K1M = Cfg::K1M;
+  constexpr int NPI = Cfg::NPI, NPF = Cfg::NPF, NT = Cfg::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* rin = reinterpret_cast<C*>(smem_raw);                        // [D][TR][K1M]
+  float* uph = reinterpret_cast<float*>(smem_raw + Cfg::RIN);     // [D][TR][N]
+  C* zb = reinterpret_cast<C*>(smem_raw);                         // [NPF][2*K1M-1] (after F1)
+  C* yb = reinterpret_cast<C*>(smem_raw + Cfg::A0);               // [NPF][N1][N2P]
+  const long long row0 = (long long)blockIdx.x * TR;
+  const int K1 = a.K1in;
+  const int ko = a.K1out - 1;
+  constexpr int ZS = 2 * K1M - 1;
+
+  // L: stage the TR spectral rows of each component (contiguous in global memory)
+  {
+    constexpr int TOT = D * TR * K1M;
+    constexpr int LPT = (TOT + NT - 1) / NT;
+    C v[LPT];
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      v[i] = make_float2(0.f, 0.f);
+      const int cmp = idx / (TR * K1M), r = (idx / K1M) % TR, kx = idx % K1M;
+      if (idx < TOT && kx < K1 && row0 + r < a.nrows)
+        v[i] = __ldg(static_cast<const C*>(a.in[cmp]) + (row0 + r) * K1 + kx);
+    }
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      if (idx < TOT) rin[idx] = v[i];
+    }
+  }
+  __syncthreads();
+
+  // I1: inverse step 1 (pencil p: row p % TR; kind 0: u1 + i u2, kind 1: u3)
+  for (int it = threadIdx.x; it < NPI * N2; it += NT) {
+    const int p = it / N2, j = it % N2;
+    const int r = p % TR, kind = p / TR;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int f = N2 * n1 + j;
+      if (kind == 0) {
+        const C x1 = hext2<N>(rin + (0 * TR + r) * K1M, K1, f);
+        const C x2 = hext2<N>(rin + (1 * TR + r) * K1M, K1, f);
+        v[n1] = make_float2(x1.x - x2.y, x1.y + x2.x);
+      } else {
+        v[n1] = hext2<N>(rin + (2 * TR + r) * K1M, K1, f);
+      }
+    }
+    DFT<N1, true, C>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+      const C w = __ldg(&tw[j * k1]);
+      v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
+    }
+    C* yp = yb + p * N1 * N2P;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+  }
+  __syncthreads();
+
+  // I2: inverse step 2 -> physical velocities at x = i + N1 k2
+  for (int it = threadIdx.x; it < NPI * N1; it += NT) {
+    const int p = it / N1, i = it % N1;
+    const int r = p % TR, kind = p / TR;
+    C w[N2];
+    const C* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+    DFT<N2, true, C>::run(w);
+    if (kind == 0) {
+      float* u1 = uph + (0 * TR + r) * N;
+      float* u2 = uph + (1 * TR + r) * N;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) { u1[i + N1 * k2] = w[k2].x; u2[i + N1 * k2] = w[k2].y; }
+    } else {
+      float* u3 = uph + (2 * TR + r) * N;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) u3[i + N1 * k2] = w[k2].x;
+    }
+  }
+  __syncthreads();
+
+  // F1: products (scaled) and forward step 1
+  const float sc = float(a.scale);
+  for (int it = threadIdx.x; it < NPF * N2; it += NT) {
+    const int p = it / N2, j = it % N2;
+    const int r = p % TR, kind = p / TR;
+    const float* u1 = uph + (0 * TR + r) * N;
+    const float* u2 = uph + (1 * TR + r) * N;
+    const float* u3 = uph + ((D == 3 ? 2 : 0) * TR + r) * N;
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int x = N2 * n1 + j;
+      const float a1 = u1[x], a2 = u2[x];
+      if (D == 3) {
+        const float a3 = u3[x];
+        v[n1] = kind == 0 ? make_float2(a1 * a1 * sc, a2 * a2 * sc)
+              : kind == 1 ? make_float2(a3 * a3 * sc, a1 * a2 * sc)
+                          : make_float2(a2 * a3 * sc, a3 * a1 * sc);
+      } else {
+        v[n1] = kind == 0 ? make_float2(a1 * a1 * sc, a2 * a2 * sc) : make_float2(a1 * a2 * sc, 0.f);
+      }
+    }
+    DFT<N1, false, C>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(&tw[j * k1]));
+    C* yp = yb + p * N1 * N2P;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+  }
+  __syncthreads();
+
+  // F2: forward step 2, keep X[k] for k <= ko and k >= N - ko
+  for (int it = threadIdx.x; it < NPF * N1; it += NT) {
+    const int p = it / N1, i = it % N1;
+    C w[N2];
+    const C* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+    DFT<N2, false, C>::run(w);
+    C* zp = zb + p * ZS;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int k = i + N1 * k2;
+      if (k <= ko) zp[k] = w[k2];
+      else if (k >= N - ko) zp[ko + (N - k)] = w[k2];
+    }
+  }
+  __syncthreads();
+
+  // S: split the paired spectra and store the product rows
+  constexpr int NBF = NPF / TR;
+  const int K1o = a.K1out;
+  for (int it = threadIdx.x; it < TR * K1o; it += NT) {
+    const int r = it / K1o, kx = it % K1o;
+    const long long row = row0 + r;
+    if (row >= a.nrows) continue;
+#pragma unroll
+    for (int b = 0; b < NBF; ++b) {
+      const C* zp = zb + (b * TR + r) * ZS;
+      const C z = zp[kx], zc = zp[kx == 0 ? 0 : ko + kx];
+      const C xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+      const C xbv = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+      static_cast<C*>(a.out[2 * b])[row * K1o + kx] = xa;
+      if (2 * b + 1 < (D == 3 ? 6 : 3)) static_cast<C*>(a.out[2 * b + 1])[row * K1o + kx] = xbv;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+// ---------------------------------------------------------------------------
+template <typename F> static void set_smem2(F* f, size_t bytes) {
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
+
+template <int N> static void init_fast_n() {
+  constexpr int T = col_tile<N>();
+  set_smem2(k_col2<N, T, true>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
+  set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
+}
+
+bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64; }
+
+bool init_fast(int N) {
+  switch (N) {
+    case 810: init_fast_n<810>(); break;
+    case 256: init_fast_n<256>(); break;
+    case 128: init_fast_n<128>(); break;
+    case 64: init_fast_n<64>(); break;
+    default: return false;
+  }
+  return cudaGetLastError() == cudaSuccess;
+}
+
+template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
+  constexpr int T = col_tile<N>();
+  using Cfg = Col2Cfg<N, T>;
+  dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
+  k_col2<N, T, INV><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+}
+
+bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st) {
+  switch (N) {
+#define SC_C2(NN) \
+  case NN: if (inv) col2_n<NN, true>(a, tw, st); else col2_n<NN, false>(a, tw, st); return true;
+    SC_C2(810) SC_C2(256) SC_C2(128) SC_C2(64)
+#undef SC_C2
+    default: return false;
+  }
+}
+
+template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
+  const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
+  if (a.D == 3) k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  else k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+}
+
+bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st) {
+  if (a.K1in > N / 3 + 1 || a.K1out > a.K1in) return false;
+  switch (N) {
+    case 810: x2_n<810>(a, tw, st); return true;
+    case 256: x2_n<256>(a, tw, st); return true;
+    case 128: x2_n<128>(a, tw, st); return true;
+    case 64: x2_n<64>(a, tw, st); return true;
+    default: return false;
+  }
+}
+
+}  // namespace sc

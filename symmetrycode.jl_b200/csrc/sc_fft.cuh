@@ -43,30 +43,11 @@ template <bool INV, typename C> __device__ __forceinline__ C mul_mi(C a) {
   return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
 }
 
-// ---------------------------------------------------------------------------
 // exact twiddle constants exp(2 pi i j / R) for the composite radices
 // (correctly rounded doubles of cos/sin at these angles)
-// ---------------------------------------------------------------------------
-__host__ __device__ constexpr double tw_cos(int R, int j) {
-  constexpr double c6[6] = {1.0, 0.5, -0.5, -1.0, -0.5, 0.5};
-  constexpr double c8[8] = {1.0, 0.7071067811865476, 0.0, -0.7071067811865476, -1.0, -0.7071067811865476, 0.0, 0.7071067811865476};
-  constexpr double c9[9] = {1.0, 0.766044443118978, 0.17364817766693036, -0.5, -0.9396926207859084, -0.9396926207859084, -0.5, 0.17364817766693036, 0.766044443118978};
-  constexpr double c10[10] = {1.0, 0.8090169943749475, 0.30901699437494745, -0.30901699437494745, -0.8090169943749475, -1.0, -0.8090169943749475, -0.30901699437494745, 0.30901699437494745, 0.8090169943749475};
-  constexpr double c12[12] = {1.0, 0.8660254037844386, 0.5, 0.0, -0.5, -0.8660254037844386, -1.0, -0.8660254037844386, -0.5, 0.0, 0.5, 0.8660254037844386};
-  constexpr double c15[15] = {1.0, 0.9135454576426009, 0.6691306063588582, 0.30901699437494745, -0.10452846326765347, -0.5, -0.8090169943749475, -0.9781476007338057, -0.9781476007338057, -0.8090169943749475, -0.5, -0.10452846326765347, 0.30901699437494745, 0.6691306063588582, 0.9135454576426009};
-  constexpr double c16[16] = {1.0, 0.9238795325112867, 0.7071067811865476, 0.3826834323650898, 0.0, -0.3826834323650898, -0.7071067811865476, -0.9238795325112867, -1.0, -0.9238795325112867, -0.7071067811865476, -0.3826834323650898, 0.0, 0.3826834323650898, 0.7071067811865476, 0.9238795325112867};
-  return R == 6 ? c6[j] : R == 8 ? c8[j] : R == 9 ? c9[j] : R == 10 ? c10[j] : R == 12 ? c12[j] : R == 15 ? c15[j] : c16[j];
-}
-__host__ __device__ constexpr double tw_sin(int R, int j) {
-  constexpr double s6[6] = {0.0, 0.8660254037844386, 0.8660254037844386, 0.0, -0.8660254037844386, -0.8660254037844386};
-  constexpr double s8[8] = {0.0, 0.7071067811865476, 1.0, 0.7071067811865476, 0.0, -0.7071067811865476, -1.0, -0.7071067811865476};
-  constexpr double s9[9] = {0.0, 0.6427876096865394, 0.984807753012208, 0.8660254037844386, 0.3420201433256687, -0.3420201433256687, -0.8660254037844386, -0.984807753012208, -0.6427876096865394};
-  constexpr double s10[10] = {0.0, 0.5877852522924731, 0.9510565162951535, 0.9510565162951535, 0.5877852522924731, 0.0, -0.5877852522924731, -0.9510565162951535, -0.9510565162951535, -0.5877852522924731};
-  constexpr double s12[12] = {0.0, 0.5, 0.8660254037844386, 1.0, 0.8660254037844386, 0.5, 0.0, -0.5, -0.8660254037844386, -1.0, -0.8660254037844386, -0.5};
-  constexpr double s15[15] = {0.0, 0.4067366430758002, 0.7431448254773942, 0.9510565162951535, 0.9945218953682733, 0.8660254037844386, 0.5877852522924731, 0.20791169081775934, -0.20791169081775934, -0.5877852522924731, -0.8660254037844386, -0.9945218953682733, -0.9510565162951535, -0.7431448254773942, -0.4067366430758002};
-  constexpr double s16[16] = {0.0, 0.3826834323650898, 0.7071067811865476, 0.9238795325112867, 1.0, 0.9238795325112867, 0.7071067811865476, 0.3826834323650898, 0.0, -0.3826834323650898, -0.7071067811865476, -0.9238795325112867, -1.0, -0.9238795325112867, -0.7071067811865476, -0.3826834323650898};
-  return R == 6 ? s6[j] : R == 8 ? s8[j] : R == 9 ? s9[j] : R == 10 ? s10[j] : R == 12 ? s12[j] : R == 15 ? s15[j] : s16[j];
-}
+}  // namespace sc
+#include "sc_twiddles.h"
+namespace sc {
 
 // ---------------------------------------------------------------------------
 // radix-R DFTs in registers.  Forward: X_k = sum_m x_m exp(-2 pi i m k / R).
@@ -175,6 +156,16 @@ template <bool INV, typename C> struct DFT<10, INV, C> : DFTPQ<2, 5, INV, C> {};
 template <bool INV, typename C> struct DFT<12, INV, C> : DFTPQ<4, 3, INV, C> {};
 template <bool INV, typename C> struct DFT<15, INV, C> : DFTPQ<3, 5, INV, C> {};
 template <bool INV, typename C> struct DFT<16, INV, C> : DFTPQ<4, 4, INV, C> {};
+template <bool INV, typename C> struct DFT<18, INV, C> : DFTPQ<2, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<20, INV, C> : DFTPQ<4, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<24, INV, C> : DFTPQ<8, 3, INV, C> {};
+template <bool INV, typename C> struct DFT<25, INV, C> : DFTPQ<5, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<27, INV, C> : DFTPQ<3, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<30, INV, C> : DFTPQ<3, 10, INV, C> {};
+template <bool INV, typename C> struct DFT<32, INV, C> : DFTPQ<4, 8, INV, C> {};
+template <bool INV, typename C> struct DFT<36, INV, C> : DFTPQ<4, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<40, INV, C> : DFTPQ<8, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<45, INV, C> : DFTPQ<5, 9, INV, C> {};
 
 // ---------------------------------------------------------------------------
 // radix schedule for N = 2^a 3^b 5^c (compile time)

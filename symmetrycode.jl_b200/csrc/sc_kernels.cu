@@ -16,6 +16,9 @@
 #include "sc_fft.cuh"
 #include "sc_internal.h"
 
+#include <cstdlib>
+#include <cstring>
+
 namespace sc {
 
 // ---------------------------------------------------------------------------
@@ -632,6 +635,7 @@ template <typename R, int N> static bool init_n() {
 // Raise the dynamic shared-memory limits of every kernel of size N (once per
 // process and device, before any launch or stream capture).
 template <typename R> bool init_kernels(int N) {
+  if (sizeof(R) == 4 && fast_supported(N) && !init_fast(N)) return false;
   switch (N) {
 #define SC_CASE(NN) case NN: return init_n<R, NN>();
     SC_SIZES(SC_CASE)
@@ -640,7 +644,20 @@ template <typename R> bool init_kernels(int N) {
   }
 }
 
+bool fast_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SC_ENGINE");
+    return !(e && strcmp(e, "stockham") == 0);
+  }();
+  return on;
+}
+
+template <typename R> static bool use_fast(int N) {
+  return sizeof(R) == 4 && fast_enabled() && fast_supported(N);
+}
+
 template <typename R> bool launch_col_inv(int N, const ColArgs& a, const void* tw, cudaStream_t st) {
+  if (use_fast<R>(N)) return launch_col2(N, true, a, tw, st);
   switch (N) {
 #define SC_CASE(NN) case NN: return col_inv_n<R, NN>(a, tw, st);
     SC_SIZES(SC_CASE)
@@ -649,6 +666,7 @@ template <typename R> bool launch_col_inv(int N, const ColArgs& a, const void* t
   }
 }
 template <typename R> bool launch_col_fwd(int N, const ColArgs& a, const void* tw, cudaStream_t st) {
+  if (use_fast<R>(N)) return launch_col2(N, false, a, tw, st);
   switch (N) {
 #define SC_CASE(NN) case NN: return col_fwd_n<R, NN>(a, tw, st);
     SC_SIZES(SC_CASE)
@@ -657,6 +675,7 @@ template <typename R> bool launch_col_fwd(int N, const ColArgs& a, const void* t
   }
 }
 template <typename R> bool launch_xsweep_ns(int N, const XArgs& a, const void* tw, cudaStream_t st) {
+  if (use_fast<R>(N) && launch_xsweep2(N, a, tw, st)) return true;
   switch (N) {
 #define SC_CASE(NN) case NN: return xsweep_n<R, NN>(a, tw, st);
     SC_SIZES(SC_CASE)
