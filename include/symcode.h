@@ -145,6 +145,25 @@ SC_API int sc_microbench(int kernel, int n, int dtype, long long count, int reps
 /* Number of kernels one sc_state_rk4 step launches (for launch accounting). */
 SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
 
+/* ---- DNS -> LES filter ------------------------------------------------------
+ * sfs!(; tau, ubar, u, g_dns, g_les, Delta) (src/data.jl:625-642) for `ndelta`
+ * filter widths at once (the DNS products are computed once and shared):
+ *   ubar = twothirds(G_Delta cutoff(u)),
+ *   tau  = tracefree(twothirds(G_Delta cutoff(sigma_dns) - sigma_les(ubar))),
+ * cutoff! / gaussianfilter! as in src/filtering.jl:28-67.  `deltas[d]` is the
+ * physical width (Delta_factor * l / n_les in the reference, src/experiment.jl:164);
+ * deltas[d] <= 0 means no Gaussian (the reference's Delta = nothing).
+ * u_hat: DNS full layout (D pointers).  ubar_hat: ndelta*D LES full-layout
+ * fields (d-major); tau_hat: ndelta*(3|6) LES full-layout fields, pair order
+ * xx, yy[, zz], xy[, yz, zx].  The two plans must be distinct, same D, l,
+ * precision and device, n_les <= n_dns. */
+SC_API int sc_filter_sfs(sc_plan* dns, sc_plan* les, const void* const* u_hat, const double* deltas, int ndelta,
+                         void* const* ubar_hat, void* const* tau_hat, void* stream);
+/* filter_reynolds(ubar, g, visc, Delta) (src/solver.jl:768-774):
+ * Delta^2 sqrt(sum_ab getenergy(twothirds(d_b ubar_a))) / visc.  Synchronous. */
+SC_API int sc_filter_reynolds(sc_plan* les, const void* const* ubar_hat, double visc, double delta, double* re,
+                              void* stream);
+
 /* ---- diagnostics (FP64 on the device; synchronous, result to host) ------- */
 /* energy(u) (src/solver.jl:643-646): 1/2 sum_i getenergy(u_i). */
 SC_API int sc_energy(sc_plan* plan, const void* const* u_hat, double* energy, void* stream);

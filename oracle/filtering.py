@@ -13,7 +13,7 @@ import numpy as np
 from .spectral import (Grid, make_tracefree, nonlinearity, twothirds,
                        wavenumbers_full)
 
-__all__ = ["cutoff_index", "cutoff", "inverse_cutoff", "gaussianfilter", "sfs"]
+__all__ = ["cutoff_index", "cutoff", "inverse_cutoff", "gaussianfilter", "sfs", "filter_reynolds"]
 
 
 def cutoff_index(nbar, n, i0, is1):
@@ -82,3 +82,11 @@ def sfs(u, g_dns: Grid, g_les: Grid, delta):
     sbar2 = nonlinearity(ubar, g_les)
     tau = [twothirds(a - b, g_les) for a, b in zip(sbar1, sbar2)]
     return ubar, make_tracefree(tau, g_dns.D)
+
+
+def filter_reynolds(ubar, g: Grid, visc, delta):
+    """``filter_reynolds`` (src/solver.jl:768-774): Δ² √(Σ_ab getenergy(twothirds(i k_b ū_a))) / ν."""
+    from .spectral import getenergy, vectorgradient
+    A = vectorgradient(ubar, g)
+    a2 = sum(getenergy(twothirds(v, g)) for v in A.values())
+    return delta ** 2 * math.sqrt(a2) / visc

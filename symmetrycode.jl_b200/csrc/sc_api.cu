@@ -113,9 +113,15 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // the five-sweep product pipeline: compact u -> compact F[u_i u_j]/n^D in p->sig
 // ---------------------------------------------------------------------------
 // `ev` (optional): events recorded after each launch, ev[0] before the first.
+// Output: the product spectra on the compact cube of half-width `kout` <= kc
+// (x extent kout+1, y/z extent 2 kout+1) in `sig` (default: the plan's).
 template <typename R>
-int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = nullptr) {
+int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = nullptr, int kout = -1,
+             void* const* sig = nullptr) {
   const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+  if (kout < 0) kout = kc;
+  if (!sig) sig = p->sig;
+  const int K1o = kout + 1, K2o = 2 * kout + 1;
   int iev = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[iev++], st); };
   mark();
@@ -137,21 +143,21 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
     sc::XArgs x{};
     for (int c = 0; c < 3; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 6; ++c) x.out[c] = p->dd[c];
-    x.D = 3; x.K1in = K1; x.K1out = K1; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
+    x.D = 3; x.K1in = K1; x.K1out = K1o; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
     mark();
     sc::ColArgs f{};
     for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
-    f.ncomp = 6; f.K1 = K1; f.ncols = n;
-    f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = (long long)K1 * K2; f.out_es = K1;
-    f.kpos = kc + 1; f.kneg = kc;
+    f.ncomp = 6; f.K1 = K1o; f.ncols = n;
+    f.in_cs = (long long)K1o * n; f.in_es = K1o; f.out_cs = (long long)K1o * K2o; f.out_es = K1o;
+    f.kpos = kout + 1; f.kneg = kout;
     sc::launch_col_fwd<R>(n, f, p->tw, st);
     mark();
     sc::ColArgs g{};
-    for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = p->sig[c]; }
-    g.ncomp = 6; g.K1 = K1; g.ncols = K2;
-    g.in_cs = K1; g.in_es = (long long)K1 * K2; g.out_cs = K1; g.out_es = (long long)K1 * K2;
-    g.kpos = kc + 1; g.kneg = kc;
+    for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = sig[c]; }
+    g.ncomp = 6; g.K1 = K1o; g.ncols = K2o;
+    g.in_cs = K1o; g.in_es = (long long)K1o * K2o; g.out_cs = K1o; g.out_es = (long long)K1o * K2o;
+    g.kpos = kout + 1; g.kneg = kout;
     sc::launch_col_fwd<R>(n, g, p->tw, st);
     mark();
   } else {
@@ -164,14 +170,14 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
     sc::XArgs x{};
     for (int c = 0; c < 2; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 3; ++c) x.out[c] = p->dd[c];
-    x.D = 2; x.K1in = K1; x.K1out = K1; x.nrows = n; x.scale = 1.0 / ((double)n * n);
+    x.D = 2; x.K1in = K1; x.K1out = K1o; x.nrows = n; x.scale = 1.0 / ((double)n * n);
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
     mark();
     sc::ColArgs f{};
-    for (int c = 0; c < 3; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->sig[c]; }
-    f.ncomp = 3; f.K1 = K1; f.ncols = 1;
-    f.in_cs = 0; f.in_es = K1; f.out_cs = 0; f.out_es = K1;
-    f.kpos = kc + 1; f.kneg = kc;
+    for (int c = 0; c < 3; ++c) { f.in[c] = p->dd[c]; f.out[c] = sig[c]; }
+    f.ncomp = 3; f.K1 = K1o; f.ncols = 1;
+    f.in_cs = 0; f.in_es = K1o; f.out_cs = 0; f.out_es = K1o;
+    f.kpos = kout + 1; f.kneg = kout;
     sc::launch_col_fwd<R>(n, f, p->tw, st);
     mark();
   }
@@ -385,18 +391,52 @@ int to_spec_impl(sc_plan* p, const void* phys, void* spec, cudaStream_t st) {
 }
 
 template <typename R>
-int energy_impl(sc_plan* p, const void* const* u, int compact, int weight_k2, double* out, cudaStream_t st) {
+int energy_impl(sc_plan* p, const void* const* u, int compact, int weight_k2, double* out, cudaStream_t st,
+                int mask23 = 0) {
   SC_CU(cudaMemsetAsync(p->dscal + 1, 0, sizeof(double), st));
   const int K1 = compact ? p->K1 : p->n / 2 + 1;
   const int K2 = compact ? p->K2 : p->n;
   sc::launch_spectral_energy<R>(u, p->D, p->D, p->n, K1, K2, compact, p->kc, 2.0 * M_PI / p->l, weight_k2,
-                                p->dscal + 1, st);
+                                p->dscal + 1, st, mask23);
   int rc = check_launch("energy");
   if (rc) return rc;
   double h = 0;
   SC_CU(cudaMemcpyAsync(&h, p->dscal + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
   SC_CU(cudaStreamSynchronize(st));
   *out = h;
+  return SC_OK;
+}
+
+template <typename R>
+int filter_impl(sc_plan* dns, sc_plan* les, const void* const* u, const double* deltas, int nd,
+                void* const* ubar, void* const* tau, cudaStream_t st) {
+  const int D = dns->D;
+  int rc = pack_state<R>(dns, u, dns->S, st);
+  if (rc) return rc;
+  rc = products<R>(dns, dns->S, st, nullptr, les->kc, dns->sig);
+  if (rc) return rc;
+  for (int d = 0; d < nd; ++d) {
+    sc::FilterArgs f{};
+    for (int c = 0; c < D; ++c) { f.udns[c] = dns->S[c]; f.ubar[c] = les->S[c]; }
+    for (int c = 0; c < (D == 3 ? 6 : 3); ++c) { f.sig1[c] = dns->sig[c]; f.tau[c] = les->sig[c]; }
+    f.D = D; f.kcd = dns->kc; f.kcl = les->kc; f.kfac = 2.0 * M_PI / les->l;
+    f.delta = (deltas[d] > 0) ? deltas[d] : 0.0;
+    f.pass = 0;
+    sc::launch_filter<R>(f, st);
+    rc = products<R>(les, les->S, st);
+    if (rc) return rc;
+    f.pass = 1;
+    sc::launch_filter<R>(f, st);
+    rc = unpack_state<R>(les, les->S, ubar + (size_t)D * d, st);
+    if (rc) return rc;
+    sc::PackArgs pa{};
+    const int nt = D == 3 ? 6 : 3;
+    for (int c = 0; c < nt; ++c) { pa.src[c] = les->sig[c]; pa.dst[c] = tau[(size_t)nt * d + c]; }
+    pa.ncomp = nt; pa.D = D; pa.n = les->n; pa.kc = les->kc;
+    sc::launch_unpack<R>(pa, st);
+    rc = check_launch("filter");
+    if (rc) return rc;
+  }
   return SC_OK;
 }
 
@@ -716,6 +756,34 @@ int sc_dissipation(sc_plan* p, const void* const* u, double visc, double* d, voi
   rc = SC_DTYPE_DISPATCH(p, energy_impl, p, u, 0, 1, &s, as_stream(stream));
   if (rc) return rc;
   *d = visc * s;
+  return SC_OK;
+}
+
+int sc_filter_sfs(sc_plan* dns, sc_plan* les, const void* const* u, const double* deltas, int ndelta,
+                  void* const* ubar, void* const* tau, void* stream) {
+  if (!dns || !les || !deltas || ndelta < 1 || !ubar || !tau) return fail(SC_ERR_INVALID, "bad argument");
+  if (dns == les) return fail(SC_ERR_INVALID, "the DNS and LES plans must be distinct objects");
+  if (dns->D != les->D || dns->dtype != les->dtype || dns->dev != les->dev)
+    return fail(SC_ERR_INVALID, "DNS and LES plans differ in dimension, precision or device");
+  if (std::fabs(dns->l - les->l) > 1e-12 * dns->l) return fail(SC_ERR_INVALID, "DNS and LES domain lengths differ");
+  if (les->n > dns->n) return fail(SC_ERR_INVALID, "LES grid (n=%d) finer than the DNS grid (n=%d)", les->n, dns->n);
+  int rc = check_ptrs(u, dns->D);
+  if (!rc) rc = check_ptrs((const void* const*)ubar, dns->D * ndelta);
+  if (!rc) rc = check_ptrs((const void* const*)tau, (dns->D == 3 ? 6 : 3) * ndelta);
+  if (!rc) rc = ensure_device(dns);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(dns, filter_impl, dns, les, u, deltas, ndelta, ubar, tau, as_stream(stream));
+}
+
+int sc_filter_reynolds(sc_plan* les, const void* const* ubar, double visc, double delta, double* out, void* stream) {
+  if (!les || !out || !(visc > 0)) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = check_ptrs(ubar, les->D);
+  if (!rc) rc = ensure_device(les);
+  if (rc) return rc;
+  double a2 = 0;
+  rc = SC_DTYPE_DISPATCH(les, energy_impl, les, ubar, 0, 1, &a2, as_stream(stream), 1);
+  if (rc) return rc;
+  *out = delta * delta * std::sqrt(a2) / visc;
   return SC_OK;
 }
 

@@ -38,10 +38,11 @@ template <int N, int T> struct Col2Cfg {
   static constexpr int NT = T * NJ;
   static constexpr int SR = N2 * T + 8;  // exchange row stride (+8: half-bank shift between rows)
   static constexpr size_t SMEM = size_t(N1) * SR * sizeof(float2);
+  static constexpr int MINB = (3 * NT <= 1024) ? 3 : 1;  // aim at 3 resident CTAs per SM
 };
 
 template <int N, int T, bool INV>
-__global__ void __launch_bounds__(Col2Cfg<N, T>::NT)
+__global__ void __launch_bounds__(Col2Cfg<N, T>::NT, Col2Cfg<N, T>::MINB)
 k_col2(const ColArgs a, const float2* __restrict__ tw) {
   using C = float2;
   using Cfg = Col2Cfg<N, T>;
@@ -128,7 +129,8 @@ template <int N, int D> struct X2Cfg {
   static constexpr size_t ZB = size_t(NPF) * (2 * K1M - 1) * sizeof(float2);
   static constexpr size_t A0 = (RIN + UPH) > ZB ? (RIN + UPH) : ZB;  // Rin+U, later aliased by Z
   static constexpr size_t YB = size_t(NPF) * N1 * N2P * sizeof(float2);
-  static constexpr size_t SMEM = A0 + YB;
+  static constexpr size_t TWB = size_t(N1) * N2 * sizeof(float2);  // twiddles W^(j k1), [k1][j]
+  static constexpr size_t SMEM = A0 + YB + TWB;
 };
 
 template <int N> __device__ __forceinline__ float2 hext2(const float2* row, int K1, int f) {
@@ -151,6 +153,8 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
   float* uph = reinterpret_cast<float*>(smem_raw + Cfg::RIN);     // [D][TR][N]
   C* zb = reinterpret_cast<C*>(smem_raw);                         // [NPF][2*K1M-1] (after F1)
   C* yb = reinterpret_cast<C*>(smem_raw + Cfg::A0);               // [NPF][N1][N2P]
+  C* tws = reinterpret_cast<C*>(smem_raw + Cfg::A0 + Cfg::YB);     // [N1][N2]
+  for (int idx = threadIdx.x; idx < N1 * N2; idx += NT) tws[idx] = __ldg(&tw[(idx % N2) * (idx / N2)]);
   const long long row0 = (long long)blockIdx.x * TR;
   const int K1 = a.K1in;
   const int ko = a.K1out - 1;
@@ -196,7 +200,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
     DFT<N1, true, C>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) {
-      const C w = __ldg(&tw[j * k1]);
+      const C w = tws[k1 * N2 + j];
       v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
     }
     C* yp = yb + p * N1 * N2P;
@@ -251,7 +255,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
     }
     DFT<N1, false, C>::run(v);
 #pragma unroll
-    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(&tw[j * k1]));
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], tws[k1 * N2 + j]);
     C* yp = yb + p * N1 * N2P;
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
@@ -300,6 +304,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }

@@ -81,12 +81,25 @@ struct PackArgs {
   int kc;  // compact half-width
 };
 
+// DNS -> LES filter on the LES compact cube (sfs!, src/data.jl:625-642).
+struct FilterArgs {
+  const void* udns[3];  // DNS compact state (half-width kcd)
+  const void* sig1[6];  // DNS product spectra on the LES compact cube
+  void* ubar[3];        // LES compact filtered velocity
+  void* tau[6];         // in: LES product spectra of ubar; out: tau (in place)
+  int D;
+  int kcd, kcl;         // DNS / LES compact half-widths
+  double kfac, delta;   // delta <= 0: no Gaussian
+  int pass;             // 0: ubar, 1: tau
+};
+
 template <typename R> bool launch_col_inv(int N, const ColArgs& a, const void* tw, cudaStream_t st);
 template <typename R> bool launch_col_fwd(int N, const ColArgs& a, const void* tw, cudaStream_t st);
 template <typename R> bool launch_xsweep_ns(int N, const XArgs& a, const void* tw, cudaStream_t st);
 template <typename R> bool launch_x_c2r(int N, const XPlainArgs& a, const void* tw, cudaStream_t st);
 template <typename R> bool launch_x_r2c(int N, const XPlainArgs& a, const void* tw, cudaStream_t st);
 template <typename R> void launch_epilogue(const EpiArgs& a, cudaStream_t st);
+template <typename R> void launch_filter(const FilterArgs& a, cudaStream_t st);
 template <typename R> void launch_pack(const PackArgs& a, cudaStream_t st);
 template <typename R> void launch_unpack(const PackArgs& a, cudaStream_t st);
 // forcing coefficient A = eps / (2 E_band) of the compact state u into *A
@@ -97,7 +110,7 @@ template <typename R> void launch_band_forcing(const void* const* u, int D, int 
 template <typename R> void launch_spectral_energy(const void* const* u, int ncomp, int D, int n,
                                                   int K1, int K2, int compact, int kc,
                                                   double kfac, int weight_k2, double* out,
-                                                  cudaStream_t st);
+                                                  cudaStream_t st, int mask23 = 0);
 bool fft_size_supported(int n);
 // two-level FP32 engine (sc_fast.cu) for N in {64, 128, 256, 810}
 bool fast_supported(int N);

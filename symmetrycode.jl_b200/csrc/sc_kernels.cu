@@ -48,6 +48,7 @@ template <typename R, int N> struct XPCfg {  // plain c2r / r2c: one buffer per 
 
 template <typename F> static void set_smem(F* f, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+  cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 __device__ __forceinline__ int compact_pos(int f, int N, int kpos, int kneg) {
@@ -438,6 +439,60 @@ __global__ void __launch_bounds__(256) k_epilogue(const EpiArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// DNS -> LES filter (sfs!, src/data.jl:625-642)
+// ---------------------------------------------------------------------------
+// pass 0: ubar = twothirds(G_delta cutoff(u))                 (cutoff!, gaussianfilter!, twothirds!)
+// pass 1: tau  = tracefree(twothirds(G_delta cutoff(sigma_dns) - sigma_les(ubar)))
+// cutoff! (src/filtering.jl:9-34) copies the DNS mode with the same wavenumber;
+// gaussianfilter! (src/filtering.jl:44-67) spares |k|^2 < (3 * 2 pi / l)^2.
+template <typename R, int D>
+__global__ void k_filter(const FilterArgs a) {
+  using C = typename V2<R>::T;
+  const int K1 = a.kcl + 1, K2 = 2 * a.kcl + 1;
+  const long long nm = (long long)K1 * K2 * (D == 3 ? K2 : 1);
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nm) return;
+  const int ix = int(i % K1);
+  const long long r = i / K1;
+  const int py = int(r % K2);
+  const int pz = D == 3 ? int(r / K2) : 0;
+  const int iy = py <= a.kcl ? py : py - K2;
+  const int iz = pz <= a.kcl ? pz : pz - K2;
+  const bool origin = ix == 0 && iy == 0 && iz == 0;
+  const double k2 = a.kfac * a.kfac * double(ix * ix + iy * iy + iz * iz);
+  double w = 1.0;
+  if (a.delta > 0 && !(k2 < 9.0 * a.kfac * a.kfac)) w = exp(-a.delta * a.delta * k2 / 24.0);
+  const R wr = R(w);
+  if (a.pass == 0) {
+    const int K1d = a.kcd + 1, K2d = 2 * a.kcd + 1;
+    const int qy = iy >= 0 ? iy : iy + K2d;
+    const int qz = iz >= 0 ? iz : iz + K2d;
+    const long long j = ix + (long long)K1d * (qy + (long long)K2d * (D == 3 ? qz : 0));
+    for (int c = 0; c < D; ++c) {
+      C v = mk<C>(R(0), R(0));
+      if (!origin) {
+        const C u = static_cast<const C*>(a.udns[c])[j];
+        v = mk<C>(wr * u.x, wr * u.y);
+      }
+      static_cast<C*>(a.ubar[c])[i] = v;
+    }
+  } else {
+    constexpr int NP = D == 3 ? 6 : 3;
+    C t[NP];
+    for (int c = 0; c < NP; ++c) {
+      const C s1 = static_cast<const C*>(a.sig1[c])[i];
+      const C s2 = static_cast<const C*>(a.tau[c])[i];
+      t[c] = origin ? mk<C>(R(0), R(0)) : mk<C>(wr * s1.x - s2.x, wr * s1.y - s2.y);
+    }
+    C tr = mk<C>(R(0), R(0));
+    for (int c = 0; c < D; ++c) tr = cadd(tr, t[c]);
+    tr = mk<C>(tr.x / R(D), tr.y / R(D));
+    for (int c = 0; c < D; ++c) t[c] = csub(t[c], tr);
+    for (int c = 0; c < NP; ++c) static_cast<C*>(a.tau[c])[i] = t[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pack / unpack between the full RFFT layout and the compact 2/3 cube
 // ---------------------------------------------------------------------------
 template <typename R>
@@ -529,14 +584,14 @@ __global__ void k_band_forcing(const PackArgs a, double eps, double* A) {
 
 template <typename R>
 __global__ void k_spectral_energy(const PackArgs a, int K1, int K2, int compact, double kfac, int weight_k2,
-                                  double* out) {
+                                  double* out, int mask23) {
   using C = typename V2<R>::T;
   const long long nm = (long long)K1 * K2 * (a.D == 3 ? K2 : 1);
   double e = 0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += (long long)gridDim.x * blockDim.x) {
     const int ix = int(i % K1);
     double w = (ix == 0 || (!compact && 2 * ix == a.n)) ? 1.0 : 2.0;
-    if (weight_k2) {
+    if (weight_k2 || mask23) {
       const long long r = i / K1;
       const int py = int(r % K2);
       const int pz = a.D == 3 ? int(r / K2) : 0;
@@ -548,7 +603,8 @@ __global__ void k_spectral_energy(const PackArgs a, int K1, int K2, int compact,
         iky = py < a.n / 2 ? py : py - a.n;
         ikz = pz < a.n / 2 ? pz : pz - a.n;
       }
-      w *= kfac * kfac * double(ix * ix + iky * iky + ikz * ikz);
+      if (weight_k2) w *= kfac * kfac * double(ix * ix + iky * iky + ikz * ikz);
+      if (mask23 && (ix > a.kc || iky > a.kc || -iky > a.kc || ikz > a.kc || -ikz > a.kc)) w = 0.0;
     }
     double s = 0;
     for (int c = 0; c < a.ncomp; ++c) {
@@ -726,9 +782,17 @@ template <typename R> void launch_band_forcing(const void* const* u, int D, int 
   (void)K1; (void)K2;
   k_band_forcing<R><<<1, 128, 0, st>>>(a, eps, A);
 }
+template <typename R> void launch_filter(const FilterArgs& a, cudaStream_t st) {
+  const int K1 = a.kcl + 1, K2 = 2 * a.kcl + 1;
+  const long long nm = (long long)K1 * K2 * (a.D == 3 ? K2 : 1);
+  const unsigned nb = unsigned((nm + 255) / 256);
+  if (a.D == 3) k_filter<R, 3><<<nb, 256, 0, st>>>(a);
+  else k_filter<R, 2><<<nb, 256, 0, st>>>(a);
+}
+
 template <typename R> void launch_spectral_energy(const void* const* u, int ncomp, int D, int n, int K1,
                                                   int K2, int compact, int kc, double kfac, int weight_k2,
-                                                  double* out, cudaStream_t st) {
+                                                  double* out, cudaStream_t st, int mask23) {
   PackArgs a{};
   for (int c = 0; c < ncomp; ++c) a.src[c] = u[c];
   a.ncomp = ncomp; a.D = D; a.n = n; a.kc = kc;
@@ -736,7 +800,7 @@ template <typename R> void launch_spectral_energy(const void* const* u, int ncom
   long long nb = (nm + 255) / 256;
   if (nb > 148 * 8) nb = 148 * 8;
   if (nb < 1) nb = 1;
-  k_spectral_energy<R><<<unsigned(nb), 256, 0, st>>>(a, K1, K2, compact, kfac, weight_k2, out);
+  k_spectral_energy<R><<<unsigned(nb), 256, 0, st>>>(a, K1, K2, compact, kfac, weight_k2, out, mask23);
 }
 
 // ---------------------------------------------------------------------------
@@ -813,7 +877,8 @@ template <typename R> void launch_project_full(const PackArgs& a, double kfac, c
   template void launch_band_forcing<R>(const void* const*, int, int, int, int, double, double*,         \
                                        cudaStream_t);                                                   \
   template void launch_spectral_energy<R>(const void* const*, int, int, int, int, int, int, int, double, \
-                                          int, double*, cudaStream_t);
+                                          int, double*, cudaStream_t, int);                               \
+  template void launch_filter<R>(const FilterArgs&, cudaStream_t);
 SC_INST(float)
 SC_INST(double)
 

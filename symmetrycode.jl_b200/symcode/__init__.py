@@ -24,7 +24,8 @@ from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions
 __all__ = [
     "Grid", "SymcodeError", "scalarfield", "vectorfield", "tensorfield", "spacescalarfield",
     "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
-    "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions",
+    "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
+    "State",
 ]
 
 
@@ -219,6 +220,34 @@ def get_dissipation(u, visc, g: Grid, stream=None):
     pu, _k = ptr_array([g._check_spec(c) for c in u])
     out = ct.c_double()
     check(lib().sc_dissipation(g.plan, pu, float(visc), ct.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+def sfs_(ubar, tau, u, g_dns: Grid, g_les: Grid, deltas, stream=None):
+    """``sfs!(; τ, ubar, u, g_dns, g_les, Δ)`` (src/data.jl:625-642) for one or several widths.
+
+    ``deltas``: a float or a list (``None`` = no Gaussian).  For a list, ``ubar``
+    and ``tau`` are lists (one vector / tensor field per width).
+    """
+    single = not isinstance(deltas, (list, tuple))
+    ds = [deltas] if single else list(deltas)
+    ub = [ubar] if single else ubar
+    ta = [tau] if single else tau
+    if len(ub) != len(ds) or len(ta) != len(ds):
+        raise ValueError("one ubar and one tau field per filter width")
+    dv = (ct.c_double * len(ds))(*[(-1.0 if d is None else float(d)) for d in ds])
+    pu, _k1 = ptr_array([g_dns._check_spec(c) for c in u])
+    pb, _k2 = ptr_array([g_les._check_spec(c) for f in ub for c in f])
+    pt, _k3 = ptr_array([g_les._check_spec(c) for f in ta for c in f])
+    check(lib().sc_filter_sfs(g_dns.plan, g_les.plan, pu, dv, len(ds), pb, pt, _stream_ptr(stream)))
+    return ubar, tau
+
+
+def filter_reynolds(ubar, g: Grid, visc, delta, stream=None):
+    """``filter_reynolds(ubar, g, visc, Δ)`` (src/solver.jl:768-774)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in ubar])
+    out = ct.c_double()
+    check(lib().sc_filter_reynolds(g.plan, pu, float(visc), float(delta), ct.byref(out), _stream_ptr(stream)))
     return out.value
 
 

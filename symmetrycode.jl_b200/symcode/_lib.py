@@ -54,6 +54,8 @@ _SIGS = {
     "sc_state_rk4_launches_per_step": ([_vp, ct.c_int], ct.c_int),
     "sc_state_profile_rhs": ([_vp, ct.c_double, ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int), _vp], ct.c_int),
     "sc_microbench": ([ct.c_int, ct.c_int, ct.c_int, ct.c_longlong, ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
+    "sc_filter_sfs": ([_vp, _vp, _pp, ct.POINTER(ct.c_double), ct.c_int, _pp, _pp, _vp], ct.c_int),
+    "sc_filter_reynolds": ([_vp, _pp, ct.c_double, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
 }
