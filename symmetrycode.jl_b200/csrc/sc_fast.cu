@@ -17,6 +17,8 @@
 #include "sc_fft.cuh"
 #include "sc_internal.h"
 
+#include <cstdlib>
+
 namespace sc {
 
 template <int N> struct Split;
@@ -106,6 +108,131 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// persistent column sweep with cp.async prefetch of the next tile
+// ---------------------------------------------------------------------------
+// Each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...  The tile's
+// stored rows (the compact rows on the inverse side, all N on the forward
+// side) are copied asynchronously into a shared stage; as soon as step 1 has
+// read the stage, the copies of the next tile are issued, so they overlap
+// step 2 (and the other resident CTA).
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+template <int N, int T> struct Col3Cfg {
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+  static constexpr int NJ = N1 > N2 ? N1 : N2;
+  static constexpr int NT = T * NJ;
+  static constexpr int SR = N2 * T + 8;
+  static constexpr size_t STAGE = size_t(N) * T * sizeof(float2);
+  static constexpr size_t SMEM = STAGE + size_t(N1) * SR * sizeof(float2);
+};
+
+template <int N, int T, bool INV>
+__device__ __forceinline__ void col3_issue(const ColArgs& a, float2* stage, long long tile, int ntx, int Kc) {
+  constexpr int NT = Col3Cfg<N, T>::NT;
+  const int kxt = int(tile % ntx);
+  const long long r = tile / ntx;
+  const int c = int(r % a.ncols);
+  const int q = int(r / a.ncols);
+  const bool drv = q >= a.ncomp;
+  const float2* in = static_cast<const float2*>(a.in[drv ? a.drv_src[q - a.ncomp] : q]);
+  const int kx0 = kxt * T;
+  const float2* base = in + kx0 + (long long)c * a.in_cs;
+  const int rows = INV ? Kc : N;
+  for (int idx = threadIdx.x; idx < rows * T; idx += NT) {
+    const int row = idx / T, tt = idx % T;
+    if (kx0 + tt < a.K1) {
+      const int e = INV ? (row < a.kpos ? row : row + N - Kc) : row;
+      cp_async8(stage + e * T + tt, base + tt + (long long)row * a.in_es);
+    }
+  }
+}
+
+template <int N, int T, bool INV>
+__global__ void __launch_bounds__(Col3Cfg<N, T>::NT, 2)
+k_col3(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles) {
+  using C = float2;
+  using Cfg = Col3Cfg<N, T>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, SR = Cfg::SR;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* stage = reinterpret_cast<C*>(smem_raw);
+  C* ys = reinterpret_cast<C*>(smem_raw + Cfg::STAGE);
+  const int t = threadIdx.x % T, j = threadIdx.x / T;
+  const int Kc = a.kpos + a.kneg;
+  long long tile = blockIdx.x;
+  if (tile < ntiles) col3_issue<N, T, INV>(a, stage, tile, ntx, Kc);
+  cp_async_commit();
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int kxt = int(tile % ntx);
+    const long long r = tile / ntx;
+    const int c = int(r % a.ncols);
+    const int q = int(r / a.ncols);
+    const bool drv = q >= a.ncomp;
+    const int kx = kxt * T + t;
+    const bool live = kx < a.K1;
+    cp_async_wait_all();
+    __syncthreads();
+    if (j < N2) {
+      C v[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int e = N2 * n1 + j;
+        v[n1] = make_float2(0.f, 0.f);
+        if (INV) {
+          const int p = cpos(e, N, a.kpos, a.kneg);
+          if (live && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
+            v[n1] = stage[e * T + t];
+            if (drv) {
+              const float kk = float(a.kfac * double(p < a.kpos ? p : p - Kc));
+              v[n1] = make_float2(-kk * v[n1].y, kk * v[n1].x);
+            }
+          }
+        } else if (live) {
+          v[n1] = stage[e * T + t];
+        }
+      }
+      DFT<N1, INV, C>::run(v);
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) {
+        C w = __ldg(&tw[j * k1]);
+        if (INV) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+      }
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) ys[k1 * SR + j * T + t] = v[k1];
+    }
+    __syncthreads();
+    {
+      const long long next = tile + gridDim.x;
+      if (next < ntiles) col3_issue<N, T, INV>(a, stage, next, ntx, Kc);
+      cp_async_commit();
+    }
+    if (j < N1 && live) {
+      C w[N2];
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) w[n2] = ys[j * SR + n2 * T + t];
+      DFT<N2, INV, C>::run(w);
+      C* obase = static_cast<C*>(a.out[q]) + kx + (long long)c * a.out_cs;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int e = j + N1 * k2;
+        if (INV) {
+          obase[(long long)e * a.out_es] = w[k2];
+        } else {
+          const int p = cpos(e, N, a.kpos, a.kneg);
+          if (p >= 0) obase[(long long)p * a.out_es] = w[k2];
+        }
+      }
+    }
+  }
+  cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -311,6 +438,8 @@ template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
 
 template <int N> static void init_fast_n() {
   constexpr int T = col_tile<N>();
+  set_smem2(k_col3<N, T, true>, Col3Cfg<N, T>::SMEM);
+  set_smem2(k_col3<N, T, false>, Col3Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, true>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
@@ -330,8 +459,36 @@ bool init_fast(int N) {
   return cudaGetLastError() == cudaSuccess;
 }
 
+static int col_variant() {
+  static const int v = [] {
+    const char* e = getenv("SC_COL_KERNEL");
+    return (e && e[0] == '2') ? 2 : 3;
+  }();
+  return v;
+}
+
+static int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
 template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
   constexpr int T = col_tile<N>();
+  if (col_variant() == 3) {
+    using Cfg = Col3Cfg<N, T>;
+    const int ntx = (a.K1 + T - 1) / T;
+    const long long ntiles = (long long)ntx * a.ncols * (a.ncomp + (INV ? a.ndrv : 0));
+    long long grid = (long long)num_sms() * 2;
+    if (grid > ntiles) grid = ntiles;
+    k_col3<N, T, INV><<<unsigned(grid), Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw), ntx, ntiles);
+    return;
+  }
   using Cfg = Col2Cfg<N, T>;
   dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
   k_col2<N, T, INV><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
