@@ -256,8 +256,7 @@ template <int N, int D> struct X2Cfg {
   static constexpr size_t ZB = size_t(NPF) * (2 * K1M - 1) * sizeof(float2);
   static constexpr size_t A0 = (RIN + UPH) > ZB ? (RIN + UPH) : ZB;  // Rin+U, later aliased by Z
   static constexpr size_t YB = size_t(NPF) * N1 * N2P * sizeof(float2);
-  static constexpr size_t TWB = size_t(N1) * N2 * sizeof(float2);  // twiddles W^(j k1), [k1][j]
-  static constexpr size_t SMEM = A0 + YB + TWB;
+  static constexpr size_t SMEM = A0 + YB;
 };
 
 template <int N> __device__ __forceinline__ float2 hext2(const float2* row, int K1, int f) {
@@ -280,8 +279,6 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
   float* uph = reinterpret_cast<float*>(smem_raw + Cfg::RIN);     // [D][TR][N]
   C* zb = reinterpret_cast<C*>(smem_raw);                         // [NPF][2*K1M-1] (after F1)
   C* yb = reinterpret_cast<C*>(smem_raw + Cfg::A0);               // [NPF][N1][N2P]
-  C* tws = reinterpret_cast<C*>(smem_raw + Cfg::A0 + Cfg::YB);     // [N1][N2]
-  for (int idx = threadIdx.x; idx < N1 * N2; idx += NT) tws[idx] = __ldg(&tw[(idx % N2) * (idx / N2)]);
   const long long row0 = (long long)blockIdx.x * TR;
   const int K1 = a.K1in;
   const int ko = a.K1out - 1;
@@ -327,7 +324,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
     DFT<N1, true, C>::run(v);
 #pragma unroll
     for (int k1 = 1; k1 < N1; ++k1) {
-      const C w = tws[k1 * N2 + j];
+      const C w = __ldg(&tw[j * k1]);
       v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
     }
     C* yp = yb + p * N1 * N2P;
@@ -382,7 +379,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
     }
     DFT<N1, false, C>::run(v);
 #pragma unroll
-    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], tws[k1 * N2 + j]);
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(&tw[j * k1]));
     C* yp = yb + p * N1 * N2P;
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
@@ -459,6 +456,9 @@ bool init_fast(int N) {
   return cudaGetLastError() == cudaSuccess;
 }
 
+// Inverse sweeps (zero-padded input, 2/3 of the loads) run the persistent
+// prefetching kernel; forward sweeps run one tile per CTA, which measured
+// faster for them.  SC_COL_KERNEL=2 selects the one-tile kernel for both.
 static int col_variant() {
   static const int v = [] {
     const char* e = getenv("SC_COL_KERNEL");
@@ -480,7 +480,7 @@ static int num_sms() {
 
 template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
   constexpr int T = col_tile<N>();
-  if (col_variant() == 3) {
+  if (col_variant() == 3 && INV) {
     using Cfg = Col3Cfg<N, T>;
     const int ntx = (a.K1 + T - 1) / T;
     const long long ntiles = (long long)ntx * a.ncols * (a.ncomp + (INV ? a.ndrv : 0));
