@@ -145,6 +145,49 @@ SC_API int sc_microbench(int kernel, int n, int dtype, long long count, int reps
 /* Number of kernels one sc_state_rk4 step launches (for launch accounting). */
 SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
 
+/* ---- LES closures and the LES right-hand side --------------------------------
+ * A closure is the reference's closure object `model(u, G) -> tau`
+ * (src/les.jl:19), bound to a plan.  Kinds and parameters:
+ *   SC_CLOSURE_NONE        no model (les! reduces to convectiondiffusion!)
+ *   SC_CLOSURE_CLARK       create_clark(Delta, g): tau = Delta^2/12 G G^T (src/closures.jl:37-42,64)
+ *   SC_CLOSURE_SMAGORINSKY create_smagorinsky(C_s, Delta, g), params[0] = C_s (default 0.17)
+ *   SC_CLOSURE_VERSTAPPEN  create_verstappen(C, Delta, g), params[0] = C (3D only; default 0.345)
+ *   SC_CLOSURE_DYNAMIC_SMAGORINSKY  create_dynamic_smagorinsky(Delta, g) (src/closures.jl:188-272):
+ *                          Germano-Lilly with a Gaussian(2 Delta) test filter, global FP64 averages
+ *   SC_CLOSURE_BARDINA     create_bardina(s, Delta, g), params[0] = s (default 2; src/closures.jl:81-115)
+ * Closure scratch is allocated at creation; evaluation allocates nothing. */
+#define SC_CLOSURE_NONE 0
+#define SC_CLOSURE_CLARK 1
+#define SC_CLOSURE_SMAGORINSKY 2
+#define SC_CLOSURE_VERSTAPPEN 3
+#define SC_CLOSURE_DYNAMIC_SMAGORINSKY 4
+#define SC_CLOSURE_BARDINA 5
+#define SC_CLOSURE_CNN 6
+typedef struct sc_closure sc_closure;
+SC_API int sc_closure_create(sc_closure** closure, sc_plan* plan, int kind, double delta, const double* params,
+                             int nparams);
+SC_API int sc_closure_destroy(sc_closure* closure);
+/* model(u, G): the packed physical stress tau (3|6 fields, pair order) from
+ * the spectral velocity u_hat (full layout) and the physical velocity
+ * gradient G (D*D fields, G[a + D b] = d u_a / d x_b; Clark, Smagorinsky and
+ * Verstappen read only G, Bardina and dynamic Smagorinsky only u_hat). */
+SC_API int sc_closure_eval(sc_closure* closure, const void* const* u_hat, const void* const* G_phys,
+                           void* const* tau_phys, void* stream);
+/* les!(du, u, grid, cache; model, visc) (src/les.jl:4-33): du = div(stress(u)
+ * + F[model(u, G)]) with G = to_phys(twothirds(vectorgradient(u))); output on
+ * the retained modes as sc_rhs.  closure = NULL gives convectiondiffusion!. */
+SC_API int sc_les_rhs(sc_plan* plan, sc_closure* closure, const void* const* u_hat, void* const* du_hat, double visc,
+                      void* stream);
+/* wray3!(les!, u, dt, grid, cache; model, visc) (src/les.jl:216-219). */
+SC_API int sc_les_wray3_step(sc_plan* plan, sc_closure* closure, void* const* u_hat, double dt, double visc,
+                             void* stream);
+/* RK4 steps of the LES (new), optional band forcing; graph-captured. */
+SC_API int sc_les_rk4_steps(sc_plan* plan, sc_closure* closure, void* const* u_hat, double dt, double visc,
+                            int nsteps, const sc_forcing* forcing, void* stream);
+/* sc_les_rk4_steps on the plan's device-resident state. */
+SC_API int sc_state_les_rk4(sc_plan* plan, sc_closure* closure, double dt, double visc, int nsteps,
+                            const sc_forcing* forcing, void* stream);
+
 /* ---- DNS -> LES filter ------------------------------------------------------
  * sfs!(; tau, ubar, u, g_dns, g_les, Delta) (src/data.jl:625-642) for `ndelta`
  * filter widths at once (the DNS products are computed once and shared):

@@ -15,6 +15,7 @@
 
 #include "sc_fft.cuh"
 #include "sc_internal.h"
+#include "sc_les.h"
 #include "symcode.h"
 
 namespace {
@@ -64,9 +65,31 @@ struct sc_plan {
   std::vector<void*> allocs;
   cudaStream_t cap = nullptr;
   cudaGraphExec_t g_rk4 = nullptr;
-  double k_rk4[4] = {0, 0, 0, 0};
+  double k_rk4[5] = {0, 0, 0, 0, 0};
   cudaGraphExec_t g_wray = nullptr;
-  double k_wray[2] = {0, 0};
+  double k_wray[3] = {0, 0, 0};
+};
+
+// A closure model `model(u, G) -> tau` (src/les.jl:19, src/closures.jl) bound
+// to a plan; owns the scratch its evaluation needs.
+struct sc_closure {
+  sc_plan* p = nullptr;
+  int kind = 0;
+  double delta = 0;
+  double prm[4] = {0, 0, 0, 0};
+  void* gc[9] = {};   // compact spectral scratch (gradient / filtered stress)
+  void* gp[9] = {};   // physical scratch (gradient / L1)
+  void* tp[6] = {};   // physical tau (and S, m1)
+  void* th[6] = {};   // compact tau-hat (the closure's stress spectrum)
+  void* ut[3] = {};   // compact test-filtered velocity
+  void* s2[6] = {};   // compact strain / filtered F[m1]
+  void* ph2[6] = {};  // physical M1
+  void* ph3[6] = {};  // physical S~ then m2
+  void* ph4[3] = {};  // physical test-filtered velocity
+  void* bb[12] = {};  // batched-transform scratch (kx, ky, z)
+  void* cb[12] = {};  // batched-transform scratch (kx, y, z)
+  double* dsum = nullptr;  // [<ML>, <MM>, c]
+  std::vector<void*> allocs;
 };
 
 namespace {
@@ -184,6 +207,191 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
   return check_launch("product pipeline");
 }
 
+// ---------------------------------------------------------------------------
+// batched transforms between the compact cube and physical space
+// (to_phys!(twothirds(.)) and to_spec! of src/solver.jl:210-215, 371-389)
+// ---------------------------------------------------------------------------
+template <typename R>
+int c2p_batch(sc_plan* p, void* const* bb, void* const* cb, void* const* in, void* const* out, int m,
+              cudaStream_t st) {
+  const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+  for (int c0 = 0; c0 < m; c0 += 12) {
+    const int mc = m - c0 < 12 ? m - c0 : 12;
+    sc::ColArgs a{};
+    if (p->D == 3) {
+      for (int c = 0; c < mc; ++c) { a.in[c] = in[c0 + c]; a.out[c] = bb[c]; }
+      a.ncomp = mc; a.K1 = K1; a.ncols = K2;
+      a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
+      a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+      sc::launch_col_inv<R>(n, a, p->tw, st);
+      sc::ColArgs b{};
+      for (int c = 0; c < mc; ++c) { b.in[c] = bb[c]; b.out[c] = cb[c]; }
+      b.ncomp = mc; b.K1 = K1; b.ncols = n;
+      b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
+      b.kpos = kc + 1; b.kneg = kc;
+      sc::launch_col_inv<R>(n, b, p->tw, st);
+    } else {
+      for (int c = 0; c < mc; ++c) { a.in[c] = in[c0 + c]; a.out[c] = cb[c]; }
+      a.ncomp = mc; a.K1 = K1; a.ncols = 1;
+      a.in_cs = 0; a.in_es = K1; a.out_cs = 0; a.out_es = K1;
+      a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+      sc::launch_col_inv<R>(n, a, p->tw, st);
+    }
+    sc::XPlainArgs x{};
+    for (int c = 0; c < mc; ++c) { x.in[c] = cb[c]; x.out[c] = out[c0 + c]; }
+    x.ncomp = mc; x.K1 = K1; x.nrows = p->D == 3 ? (long long)n * n : n; x.scale = 1.0;
+    sc::launch_x_c2r<R>(n, x, p->tw, st);
+  }
+  return check_launch("compact to physical");
+}
+
+template <typename R>
+int p2c_batch(sc_plan* p, void* const* bb, void* const* cb, void* const* in, void* const* out, int m,
+              cudaStream_t st) {
+  const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+  for (int c0 = 0; c0 < m; c0 += 12) {
+    const int mc = m - c0 < 12 ? m - c0 : 12;
+    sc::XPlainArgs x{};
+    for (int c = 0; c < mc; ++c) { x.in[c] = in[c0 + c]; x.out[c] = cb[c]; }
+    x.ncomp = mc; x.K1 = K1; x.nrows = p->D == 3 ? (long long)n * n : n;
+    x.scale = 1.0 / std::pow((double)n, p->D);
+    sc::launch_x_r2c<R>(n, x, p->tw, st);
+    sc::ColArgs f{};
+    if (p->D == 3) {
+      for (int c = 0; c < mc; ++c) { f.in[c] = cb[c]; f.out[c] = bb[c]; }
+      f.ncomp = mc; f.K1 = K1; f.ncols = n;
+      f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = (long long)K1 * K2; f.out_es = K1;
+      f.kpos = kc + 1; f.kneg = kc;
+      sc::launch_col_fwd<R>(n, f, p->tw, st);
+      sc::ColArgs g{};
+      for (int c = 0; c < mc; ++c) { g.in[c] = bb[c]; g.out[c] = out[c0 + c]; }
+      g.ncomp = mc; g.K1 = K1; g.ncols = K2;
+      g.in_cs = K1; g.in_es = (long long)K1 * K2; g.out_cs = K1; g.out_es = (long long)K1 * K2;
+      g.kpos = kc + 1; g.kneg = kc;
+      sc::launch_col_fwd<R>(n, g, p->tw, st);
+    } else {
+      for (int c = 0; c < mc; ++c) { f.in[c] = cb[c]; f.out[c] = out[c0 + c]; }
+      f.ncomp = mc; f.K1 = K1; f.ncols = 1;
+      f.in_cs = 0; f.in_es = K1; f.out_cs = 0; f.out_es = K1;
+      f.kpos = kc + 1; f.kneg = kc;
+      sc::launch_col_fwd<R>(n, f, p->tw, st);
+    }
+  }
+  return check_launch("physical to compact");
+}
+
+sc::LesSpecArgs spec_args(sc_plan* p) {
+  sc::LesSpecArgs a{};
+  a.kc = p->kc;
+  a.nmodes = (long long)p->csz;
+  a.kfac = 2.0 * M_PI / p->l;
+  a.scale = 1.0;
+  return a;
+}
+
+sc::LesPhysArgs phys_args(sc_plan* p) {
+  sc::LesPhysArgs a{};
+  a.npts = (long long)std::pow((double)p->n, p->D);
+  return a;
+}
+
+// Closure stress of the compact state u into cl->th (compact), i.e. the
+// spectrum to_spec!(model(u, G)) that les! adds to sigma (src/les.jl:19-27).
+// Bardina and dynamic Smagorinsky read the product spectra F[u_i u_j]/n^D from
+// p->sig, which the caller has just computed for the same u.
+template <typename R>
+int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const* tau_phys_out = nullptr) {
+  sc_plan* p = cl->p;
+  const int D = p->D, NP = D == 3 ? 6 : 3;
+  int rc = SC_OK;
+  if (cl->kind == sc::kClark || cl->kind == sc::kSmagorinsky || cl->kind == sc::kVerstappen) {
+    sc::LesSpecArgs g = spec_args(p);
+    for (int c = 0; c < D; ++c) g.in[c] = u[c];
+    for (int c = 0; c < D * D; ++c) g.out[c] = cl->gc[c];
+    sc::launch_grad<R>(g, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->gc, cl->gp, D * D, st))) return rc;
+    sc::LesPhysArgs a = phys_args(p);
+    for (int c = 0; c < D * D; ++c) a.in[c] = cl->gp[c];
+    for (int c = 0; c < NP; ++c) a.out[c] = cl->tp[c];
+    a.kind = cl->kind; a.delta = cl->delta; a.p0 = cl->prm[0];
+    sc::launch_closure_pt<R>(a, D, st);
+  } else if (cl->kind == sc::kBardina) {
+    const double dt_ = cl->prm[0] * cl->delta;
+    sc::LesSpecArgs f = spec_args(p);
+    for (int c = 0; c < D; ++c) { f.in[c] = u[c]; f.out[c] = cl->ut[c]; }
+    f.ncomp = D; f.delta = dt_;
+    sc::launch_spec_filter<R>(f, D, st);
+    sc::LesSpecArgs h = spec_args(p);
+    for (int c = 0; c < NP; ++c) { h.in[c] = p->sig[c]; h.out[c] = cl->gc[c]; }
+    h.ncomp = NP; h.delta = dt_;
+    sc::launch_spec_filter<R>(h, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->gc, cl->gp, NP, st))) return rc;
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->ut, cl->ph4, D, st))) return rc;
+    sc::LesPhysArgs a = phys_args(p);
+    for (int c = 0; c < NP; ++c) { a.in[c] = cl->gp[c]; a.out[c] = cl->tp[c]; }
+    for (int c = 0; c < D; ++c) a.in2[c] = cl->ph4[c];
+    a.kind = 1;  // trace-free
+    sc::launch_sub_products<R>(a, D, st);
+  } else if (cl->kind == sc::kDynSmagorinsky) {
+    const double dtl = 2.0 * cl->delta, ddb = std::sqrt(dtl * dtl + cl->delta * cl->delta);
+    sc::LesSpecArgs f = spec_args(p);  // u~ = P G~ u
+    for (int c = 0; c < D; ++c) { f.in[c] = u[c]; f.out[c] = cl->ut[c]; }
+    f.ncomp = D; f.delta = dtl;
+    sc::launch_spec_filter<R>(f, D, st);
+    sc::LesSpecArgs h = spec_args(p);  // P G~ sigma
+    for (int c = 0; c < NP; ++c) { h.in[c] = p->sig[c]; h.out[c] = cl->gc[c]; }
+    h.ncomp = NP; h.delta = dtl;
+    sc::launch_spec_filter<R>(h, D, st);
+    sc::LesSpecArgs sr = spec_args(p);  // S-hat
+    for (int c = 0; c < D; ++c) sr.in[c] = u[c];
+    for (int c = 0; c < NP; ++c) sr.out[c] = cl->s2[c];
+    sc::launch_strain<R>(sr, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->gc, cl->gp, NP, st))) return rc;   // L1
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->ut, cl->ph4, D, st))) return rc;   // u~
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->s2, cl->tp, NP, st))) return rc;   // S
+    sc::LesSpecArgs h2 = spec_args(p);  // P G~ P S-hat, in place
+    for (int c = 0; c < NP; ++c) { h2.in[c] = cl->s2[c]; h2.out[c] = cl->s2[c]; }
+    h2.ncomp = NP; h2.delta = dtl;
+    sc::launch_spec_filter<R>(h2, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->s2, cl->ph3, NP, st))) return rc;  // S~
+    sc::LesPhysArgs m1 = phys_args(p);  // m1 = smag(S, Delta), in place
+    for (int c = 0; c < NP; ++c) { m1.in[c] = cl->tp[c]; m1.out[c] = cl->tp[c]; }
+    m1.delta = cl->delta;
+    sc::launch_smag_tensor<R>(m1, D, st);
+    sc::LesPhysArgs m2 = phys_args(p);  // m2 = smag(S~, sqrt(5) Delta), in place
+    for (int c = 0; c < NP; ++c) { m2.in[c] = cl->ph3[c]; m2.out[c] = cl->ph3[c]; }
+    m2.delta = ddb;
+    sc::launch_smag_tensor<R>(m2, D, st);
+    if ((rc = p2c_batch<R>(p, cl->bb, cl->cb, cl->tp, cl->th, NP, st))) return rc;   // F[m1]
+    sc::LesSpecArgs h3 = spec_args(p);  // P G~ F[m1]
+    for (int c = 0; c < NP; ++c) { h3.in[c] = cl->th[c]; h3.out[c] = cl->s2[c]; }
+    h3.ncomp = NP; h3.delta = dtl;
+    sc::launch_spec_filter<R>(h3, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->s2, cl->ph2, NP, st))) return rc;  // M1
+    SC_CU(cudaMemsetAsync(cl->dsum, 0, 3 * sizeof(double), st));
+    sc::LesPhysArgs ml = phys_args(p);
+    for (int c = 0; c < NP; ++c) { ml.in[c] = cl->gp[c]; ml.in3[c] = cl->ph2[c]; ml.in4[c] = cl->ph3[c]; }
+    for (int c = 0; c < D; ++c) ml.in2[c] = cl->ph4[c];
+    sc::launch_dynsmag_mlmm<R>(ml, D, cl->dsum, st);
+    sc::LesSpecArgs sc_ = spec_args(p);  // tau-hat = c P F[m1]
+    for (int c = 0; c < NP; ++c) { sc_.in[c] = cl->th[c]; sc_.out[c] = cl->th[c]; }
+    sc_.ncomp = NP; sc_.delta = 0; sc_.dscale = cl->dsum + 2;
+    sc::launch_spec_filter<R>(sc_, D, st);
+    if (tau_phys_out) return c2p_batch<R>(p, cl->bb, cl->cb, cl->th, tau_phys_out, NP, st);
+    return check_launch("dynamic Smagorinsky");
+  } else {
+    return fail(SC_ERR_UNSUPPORTED, "closure kind %d has no evaluation in this build", cl->kind);
+  }
+  // tp holds the physical stress
+  if (tau_phys_out) {
+    for (int c = 0; c < NP; ++c)
+      SC_CU(cudaMemcpyAsync(tau_phys_out[c], cl->tp[c], (size_t)phys_args(p).npts * sizeof(R),
+                            cudaMemcpyDeviceToDevice, st));
+    return check_launch("closure");
+  }
+  return p2c_batch<R>(p, cl->bb, cl->cb, cl->tp, cl->th, NP, st);
+}
+
 template <typename R>
 sc::EpiArgs epi_base(sc_plan* p, void* const* us, double visc) {
   sc::EpiArgs e{};
@@ -196,14 +404,30 @@ sc::EpiArgs epi_base(sc_plan* p, void* const* us, double visc) {
 }
 
 template <typename R>
-int rk4_step(sc_plan* p, double dt, double visc, const sc_forcing* frc, cudaStream_t st) {
+void add_closure_stress(sc::EpiArgs& e, sc_closure* cl, int D) {
+  if (!cl || cl->kind == sc::kNoClosure) return;
+  for (int c = 0; c < (D == 3 ? 6 : 3); ++c) e.sig2[c] = cl->th[c];
+  e.has_sig2 = 1;
+}
+
+template <typename R>
+int stage_rhs(sc_plan* p, sc_closure* cl, void* const* us, cudaStream_t st) {
+  int rc = products<R>(p, us, st);
+  if (rc) return rc;
+  if (cl && cl->kind != sc::kNoClosure) return closure_tauhat<R>(cl, us, st);
+  return SC_OK;
+}
+
+template <typename R>
+int rk4_step(sc_plan* p, double dt, double visc, const sc_forcing* frc, cudaStream_t st, sc_closure* cl = nullptr) {
   const bool forced = frc != nullptr && frc->enabled;
   for (int s = 0; s < 4; ++s) {
     void* const* us = s == 0 ? p->U : p->S;
     if (forced) sc::launch_band_forcing<R>(us, p->D, p->K1, p->K2, p->kc, frc->eps, p->dscal, st);
-    int rc = products<R>(p, us, st);
+    int rc = stage_rhs<R>(p, cl, us, st);
     if (rc) return rc;
     sc::EpiArgs e = epi_base<R>(p, us, visc);
+    add_closure_stress<R>(e, cl, p->D);
     e.proj_k = 1;
     e.forcing = forced ? p->dscal : nullptr;
     static const double wa[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
@@ -222,13 +446,14 @@ int rk4_step(sc_plan* p, double dt, double visc, const sc_forcing* frc, cudaStre
 }
 
 template <typename R>
-int wray3_step(sc_plan* p, double dt, double visc, cudaStream_t st) {
+int wray3_step(sc_plan* p, double dt, double visc, cudaStream_t st, sc_closure* cl = nullptr) {
   static const double a[3] = {8.0 / 15, 5.0 / 12, 3.0 / 4};
   static const double b[2] = {1.0 / 4, 0.0};
   for (int s = 0; s < 3; ++s) {
-    int rc = products<R>(p, p->U, st);
+    int rc = stage_rhs<R>(p, cl, p->U, st);
     if (rc) return rc;
     sc::EpiArgs e = epi_base<R>(p, p->U, visc);
+    add_closure_stress<R>(e, cl, p->D);
     e.proj_a = 1;
     for (int c = 0; c < p->D; ++c) {
       e.base_a[c] = s == 0 ? p->U[c] : p->S[c];
@@ -277,13 +502,15 @@ int ensure_device(sc_plan* p) {
 }
 
 template <typename R>
-int run_rk4_graph(sc_plan* p, double dt, double visc, int nsteps, const sc_forcing* frc, cudaStream_t st) {
-  const double key[4] = {dt, visc, (frc && frc->enabled) ? 1.0 : 0.0, (frc && frc->enabled) ? frc->eps : 0.0};
+int run_rk4_graph(sc_plan* p, double dt, double visc, int nsteps, const sc_forcing* frc, cudaStream_t st,
+                  sc_closure* cl = nullptr) {
+  double key[5] = {dt, visc, (frc && frc->enabled) ? 1.0 : 0.0, (frc && frc->enabled) ? frc->eps : 0.0, 0.0};
+  std::memcpy(&key[4], &cl, sizeof(cl));
   if (!p->g_rk4 || std::memcmp(key, p->k_rk4, sizeof(key)) != 0) {
     if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
     cudaGraph_t g;
     SC_CU(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-    int rc = rk4_step<R>(p, dt, visc, frc, p->cap);
+    int rc = rk4_step<R>(p, dt, visc, frc, p->cap, cl);
     cudaError_t e = cudaStreamEndCapture(p->cap, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(SC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -297,13 +524,14 @@ int run_rk4_graph(sc_plan* p, double dt, double visc, int nsteps, const sc_forci
 }
 
 template <typename R>
-int run_wray_graph(sc_plan* p, double dt, double visc, cudaStream_t st) {
-  const double key[2] = {dt, visc};
+int run_wray_graph(sc_plan* p, double dt, double visc, cudaStream_t st, sc_closure* cl = nullptr) {
+  double key[3] = {dt, visc, 0.0};
+  std::memcpy(&key[2], &cl, sizeof(cl));
   if (!p->g_wray || std::memcmp(key, p->k_wray, sizeof(key)) != 0) {
     if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
     cudaGraph_t g;
     SC_CU(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
-    int rc = wray3_step<R>(p, dt, visc, p->cap);
+    int rc = wray3_step<R>(p, dt, visc, p->cap, cl);
     cudaError_t e = cudaStreamEndCapture(p->cap, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return fail(SC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
@@ -785,6 +1013,154 @@ int sc_filter_reynolds(sc_plan* les, const void* const* ubar, double visc, doubl
   if (rc) return rc;
   *out = delta * delta * std::sqrt(a2) / visc;
   return SC_OK;
+}
+
+int sc_closure_create(sc_closure** out, sc_plan* p, int kind, double delta, const double* params, int nparams) {
+  if (!out || !p) return fail(SC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (kind < sc::kNoClosure || kind > sc::kBardina)
+    return fail(kind == sc::kCnn ? SC_ERR_UNSUPPORTED : SC_ERR_INVALID,
+                kind == sc::kCnn ? "the CNN closure is created with sc_cnn_closure_create" : "unknown closure kind %d",
+                kind);
+  if (kind == sc::kVerstappen && p->D != 3) return fail(SC_ERR_INVALID, "Q-R model is only defined in 3D");
+  if (kind != sc::kNoClosure && !(delta > 0)) return fail(SC_ERR_INVALID, "filter width must be positive");
+  if (nparams < 0 || nparams > 4 || (nparams > 0 && !params)) return fail(SC_ERR_INVALID, "bad params");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  sc_closure* cl = new sc_closure();
+  cl->p = p; cl->kind = kind; cl->delta = delta;
+  for (int i = 0; i < nparams; ++i) cl->prm[i] = params[i];
+  if (kind == sc::kSmagorinsky && nparams < 1) cl->prm[0] = 0.17;
+  if (kind == sc::kVerstappen && nparams < 1) cl->prm[0] = 0.345;
+  if (kind == sc::kBardina && nparams < 1) cl->prm[0] = 2.0;
+  const int D = p->D, NP = D == 3 ? 6 : 3;
+  const size_t cb = p->csz * p->esz;
+  const size_t pb = (size_t)std::pow((double)p->n, D) * (p->esz / 2);
+  const size_t mid = (D == 3 ? (size_t)p->K1 * p->K2 * p->n : 0) * p->esz;
+  const size_t plane = (size_t)p->K1 * p->n * (D == 3 ? p->n : 1) * p->esz;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  if (kind != sc::kNoClosure) {
+    for (int c = 0; c < D * D && !rc; ++c) rc = A(&cl->gc[c], cb);
+    for (int c = 0; c < D * D && !rc; ++c) rc = A(&cl->gp[c], pb);
+    for (int c = 0; c < NP && !rc; ++c) rc = A(&cl->tp[c], pb);
+    for (int c = 0; c < NP && !rc; ++c) rc = A(&cl->th[c], cb);
+    for (int c = 0; c < D && !rc; ++c) rc = A(&cl->ut[c], cb);
+    for (int c = 0; c < NP && !rc; ++c) rc = A(&cl->s2[c], cb);
+    for (int c = 0; c < NP && !rc; ++c) rc = A(&cl->ph2[c], pb);
+    for (int c = 0; c < NP && !rc; ++c) rc = A(&cl->ph3[c], pb);
+    for (int c = 0; c < D && !rc; ++c) rc = A(&cl->ph4[c], pb);
+    for (int c = 0; c < 12 && !rc; ++c) rc = A(&cl->cb[c], plane);
+    for (int c = 0; c < 12 && !rc && D == 3; ++c) rc = A(&cl->bb[c], mid);
+    if (!rc) rc = A((void**)&cl->dsum, 4 * sizeof(double));
+  }
+  if (rc) {
+    for (void* a : cl->allocs) cudaFree(a);
+    delete cl;
+    return rc;
+  }
+  *out = cl;
+  return SC_OK;
+}
+
+int sc_closure_destroy(sc_closure* cl) {
+  if (!cl) return SC_OK;
+  sc_plan* p = cl->p;
+  if (p) {
+    ensure_device(p);
+    // cached step graphs may reference this closure's buffers
+    if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
+    if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
+  }
+  for (void* a : cl->allocs) cudaFree(a);
+  delete cl;
+  return SC_OK;
+}
+
+int sc_closure_eval(sc_closure* cl, const void* const* u, const void* const* G, void* const* tau, void* stream) {
+  if (!cl) return fail(SC_ERR_INVALID, "null closure");
+  sc_plan* p = cl->p;
+  const int D = p->D, NP = D == 3 ? 6 : 3;
+  int rc = check_ptrs((const void* const*)tau, NP);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  if (cl->kind == sc::kNoClosure) return fail(SC_ERR_INVALID, "the empty closure has no stress");
+  cudaStream_t st = as_stream(stream);
+  auto body = [&](auto tag) -> int {
+    using R = decltype(tag);
+    if (cl->kind == sc::kClark || cl->kind == sc::kSmagorinsky || cl->kind == sc::kVerstappen) {
+      int r = check_ptrs(G, D * D);
+      if (r) return r;
+      sc::LesPhysArgs a = phys_args(p);
+      for (int c = 0; c < D * D; ++c) a.in[c] = G[c];
+      for (int c = 0; c < NP; ++c) a.out[c] = tau[c];
+      a.kind = cl->kind; a.delta = cl->delta; a.p0 = cl->prm[0];
+      sc::launch_closure_pt<R>(a, D, st);
+      return check_launch("closure");
+    }
+    int r = check_ptrs(u, D);
+    if (r) return r;
+    if ((r = pack_state<R>(p, u, p->S, st))) return r;
+    if ((r = products<R>(p, p->S, st))) return r;
+    return closure_tauhat<R>(cl, p->S, st, tau);
+  };
+  return p->dtype == SC_FLOAT64 ? body(double()) : body(float());
+}
+
+int sc_les_rhs(sc_plan* p, sc_closure* cl, const void* const* u, void* const* du, double visc, void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = check_ptrs((const void* const*)du, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  auto body = [&](auto tag) -> int {
+    using R = decltype(tag);
+    int r = pack_state<R>(p, u, p->S, st);
+    if (r) return r;
+    if ((r = stage_rhs<R>(p, cl, p->S, st))) return r;
+    sc::EpiArgs e = epi_base<R>(p, p->S, visc);
+    add_closure_stress<R>(e, cl, p->D);
+    for (int c = 0; c < p->D; ++c) { e.base_a[c] = nullptr; e.out_a[c] = p->ACC[c]; }
+    e.ca = 1.0;
+    sc::launch_epilogue<R>(e, st);
+    if ((r = check_launch("les rhs"))) return r;
+    return unpack_state<R>(p, p->ACC, du, st);
+  };
+  return p->dtype == SC_FLOAT64 ? body(double()) : body(float());
+}
+
+int sc_state_les_rk4(sc_plan* p, sc_closure* cl, double dt, double visc, int nsteps, const sc_forcing* frc,
+                     void* stream) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  if (nsteps < 0) return fail(SC_ERR_INVALID, "nsteps must be >= 0");
+  int rc = ensure_device(p);
+  if (rc || nsteps == 0) return rc;
+  return SC_DTYPE_DISPATCH(p, run_rk4_graph, p, dt, visc, nsteps, frc, as_stream(stream), cl);
+}
+
+int sc_les_rk4_steps(sc_plan* p, sc_closure* cl, void* const* u, double dt, double visc, int nsteps,
+                     const sc_forcing* frc, void* stream) {
+  int rc = sc_state_load(p, (const void* const*)u, stream);
+  if (rc) return rc;
+  rc = sc_state_les_rk4(p, cl, dt, visc, nsteps, frc, stream);
+  if (rc) return rc;
+  return sc_state_store(p, u, stream);
+}
+
+int sc_les_wray3_step(sc_plan* p, sc_closure* cl, void* const* u, double dt, double visc, void* stream) {
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  int rc = sc_state_load(p, (const void* const*)u, stream);
+  if (rc) return rc;
+  rc = SC_DTYPE_DISPATCH(p, run_wray_graph, p, dt, visc, as_stream(stream), cl);
+  if (rc) return rc;
+  return sc_state_store(p, u, stream);
 }
 
 int sc_twothirds(sc_plan* p, void* const* f, int ncomp, void* stream) {

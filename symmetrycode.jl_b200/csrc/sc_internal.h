@@ -71,6 +71,8 @@ struct EpiArgs {
   int proj_a;           // project out_a (Wray3)
   int has_b;
   const double* forcing;  // device scalar A (nullptr: no forcing)
+  const void* sig2[6];    // optional second stress spectrum added to sig (closure stress)
+  int has_sig2;
 };
 
 struct PackArgs {

@@ -371,6 +371,10 @@ __global__ void __launch_bounds__(256) k_epilogue(const EpiArgs a) {
   constexpr int NP = D == 3 ? 6 : 3;
 #pragma unroll
   for (int c = 0; c < NP; ++c) s[c] = static_cast<const C*>(a.sig[c])[i];
+  if (a.has_sig2) {
+#pragma unroll
+    for (int c = 0; c < NP; ++c) s[c] = cadd(s[c], static_cast<const C*>(a.sig2[c])[i]);
+  }
   // pair order: 3D xx yy zz xy yz zx ; 2D xx yy xy
   constexpr int P3[3][3] = {{0, 3, 5}, {3, 1, 4}, {5, 4, 2}};
   constexpr int P2[2][2] = {{0, 2}, {2, 1}};

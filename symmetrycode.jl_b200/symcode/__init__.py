@@ -25,7 +25,8 @@ __all__ = [
     "Grid", "SymcodeError", "scalarfield", "vectorfield", "tensorfield", "spacescalarfield",
     "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
     "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
-    "State",
+    "State", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
+    "create_dynamic_smagorinsky", "create_bardina", "les_", "les_wray3_", "les_rk4_",
 ]
 
 
@@ -251,6 +252,104 @@ def filter_reynolds(ubar, g: Grid, visc, delta, stream=None):
     return out.value
 
 
+# --------------------------------------------------------------------------
+# closures (src/closures.jl) and the LES right-hand side (src/les.jl:4-33)
+# --------------------------------------------------------------------------
+CLOSURE_NONE, CLOSURE_CLARK, CLOSURE_SMAGORINSKY, CLOSURE_VERSTAPPEN = 0, 1, 2, 3
+CLOSURE_DYNAMIC_SMAGORINSKY, CLOSURE_BARDINA, CLOSURE_CNN = 4, 5, 6
+
+
+class Closure:
+    """A closure model bound to a Grid; ``closure(u, G)`` returns the packed
+    physical stress like the reference's ``model(u, G)`` (src/les.jl:19)."""
+
+    def __init__(self, g: Grid, kind, delta=0.0, params=()):
+        self.g, self.kind, self.delta = g, kind, float(delta)
+        ptr = ct.c_void_p()
+        pa = (ct.c_double * max(1, len(params)))(*params) if params else None
+        with torch.cuda.device(g.device):
+            check(lib().sc_closure_create(ct.byref(ptr), g.plan, int(kind), float(delta), pa, len(params)))
+        self._ptr = ptr
+
+    @property
+    def ptr(self):
+        return self._ptr
+
+    def __call__(self, u, G=None, stream=None):
+        g = self.g
+        tau = [torch.zeros(g.phys_shape, dtype=g.dtype, device=g.device) for _ in range(g.tensordim)]
+        pu, _k1 = ptr_array([g._check_spec(c) for c in u]) if u is not None else (None, None)
+        pg, _k2 = ptr_array([g._check_phys(c) for c in G]) if G is not None else (None, None)
+        pt, _k3 = ptr_array([g._check_phys(c) for c in tau])
+        check(lib().sc_closure_eval(self._ptr, pu, pg, pt, _stream_ptr(stream)))
+        return torch.stack(tau, 0)
+
+    def close(self):
+        if getattr(self, "_ptr", None):
+            with torch.cuda.device(self.g.device):
+                lib().sc_closure_destroy(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def create_clark(delta, g: Grid):
+    """``create_clark(Δ, g)`` (src/closures.jl:64)."""
+    return Closure(g, CLOSURE_CLARK, delta)
+
+
+def create_smagorinsky(CS, delta, g: Grid):
+    """``create_smagorinsky(CS, Δ, g)`` (src/closures.jl:65-66)."""
+    return Closure(g, CLOSURE_SMAGORINSKY, delta, (CS,))
+
+
+def create_verstappen(C, delta, g: Grid):
+    """``create_verstappen(C, Δ, g)`` (src/closures.jl:68-71); 3D only."""
+    return Closure(g, CLOSURE_VERSTAPPEN, delta, (C,))
+
+
+def create_dynamic_smagorinsky(delta, g: Grid):
+    """``create_dynamic_smagorinsky(Δ, g)`` (src/closures.jl:188-272)."""
+    return Closure(g, CLOSURE_DYNAMIC_SMAGORINSKY, delta)
+
+
+def create_bardina(s, delta, g: Grid):
+    """``create_bardina(s, Δ, g)`` (src/closures.jl:81-115)."""
+    return Closure(g, CLOSURE_BARDINA, delta, (s,))
+
+
+def _cl(model):
+    return model.ptr if model is not None else None
+
+
+def les_(du, u, g: Grid, model, visc, stream=None):
+    """``les!(du, u, grid, cache; model, visc)`` (src/les.jl:4-33), retained modes."""
+    pu, _k1 = ptr_array([g._check_spec(c) for c in u])
+    pd, _k2 = ptr_array([g._check_spec(c) for c in du])
+    check(lib().sc_les_rhs(g.plan, _cl(model), pu, pd, float(visc), _stream_ptr(stream)))
+    return du
+
+
+def les_wray3_(u, dt, g: Grid, model, visc, stream=None):
+    """``wray3!(les!, u, Δt, grid, cache; model, visc)`` (src/les.jl:216-219)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    check(lib().sc_les_wray3_step(g.plan, _cl(model), pu, float(dt), float(visc), _stream_ptr(stream)))
+    return u
+
+
+def les_rk4_(u, dt, g: Grid, model, visc, nsteps=1, eps=None, stream=None):
+    """RK4 steps of the LES with closure ``model`` (new)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    f = sc_forcing(1 if eps is not None else 0, float(eps) if eps is not None else 0.0)
+    check(lib().sc_les_rk4_steps(g.plan, _cl(model), pu, float(dt), float(visc), int(nsteps), ct.byref(f),
+                                 _stream_ptr(stream)))
+    return u
+
+
 class State:
     """Device-resident compact state of a plan (sc_state_* entry points)."""
 
@@ -280,6 +379,11 @@ class State:
         nk = ct.c_int()
         check(lib().sc_state_profile_rhs(self.g.plan, float(visc), int(reps), ms, ct.byref(nk), _stream_ptr(stream)))
         return list(ms[: nk.value])
+
+    def les_rk4(self, model, dt, visc, nsteps=1, eps=None, stream=None):
+        f = sc_forcing(1 if eps is not None else 0, float(eps) if eps is not None else 0.0)
+        check(lib().sc_state_les_rk4(self.g.plan, _cl(model), float(dt), float(visc), int(nsteps), ct.byref(f),
+                                     _stream_ptr(stream)))
 
     def launches_per_step(self, forced):
         return lib().sc_state_rk4_launches_per_step(self.g.plan, 1 if forced else 0)

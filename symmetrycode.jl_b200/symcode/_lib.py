@@ -56,6 +56,13 @@ _SIGS = {
     "sc_microbench": ([ct.c_int, ct.c_int, ct.c_int, ct.c_longlong, ct.c_int, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)], ct.c_int),
     "sc_filter_sfs": ([_vp, _vp, _pp, ct.POINTER(ct.c_double), ct.c_int, _pp, _pp, _vp], ct.c_int),
     "sc_filter_reynolds": ([_vp, _pp, ct.c_double, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
+    "sc_closure_create": ([ct.POINTER(_vp), _vp, ct.c_int, ct.c_double, ct.POINTER(ct.c_double), ct.c_int], ct.c_int),
+    "sc_closure_destroy": ([_vp], ct.c_int),
+    "sc_closure_eval": ([_vp, _pp, _pp, _pp, _vp], ct.c_int),
+    "sc_les_rhs": ([_vp, _vp, _pp, _pp, ct.c_double, _vp], ct.c_int),
+    "sc_les_wray3_step": ([_vp, _vp, _pp, ct.c_double, ct.c_double, _vp], ct.c_int),
+    "sc_les_rk4_steps": ([_vp, _vp, _pp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(sc_forcing), _vp], ct.c_int),
+    "sc_state_les_rk4": ([_vp, _vp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(sc_forcing), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
 }

@@ -1,0 +1,108 @@
+"""LES closures and les! through the C ABI against the FP64 oracle."""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import symcode as S
+from _util import rel_l2, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+
+KINDS = ["clark", "smagorinsky", "verstappen", "dynsmag", "bardina"]
+
+
+def _models(kind, delta, g, D):
+    """(CUDA closure, oracle model(u, G) -> packed tau)."""
+    if kind == "clark":
+        return S.create_clark(delta, g), lambda u, G, go: O.clark(G, delta, D)
+    if kind == "smagorinsky":
+        return S.create_smagorinsky(0.17, delta, g), lambda u, G, go: O.smagorinsky(G, 0.17, delta, D)
+    if kind == "verstappen":
+        return S.create_verstappen(0.3, delta, g), lambda u, G, go: O.verstappen(G, 0.3, delta, D)
+    if kind == "dynsmag":
+        return S.create_dynamic_smagorinsky(delta, g), lambda u, G, go: O.dynamic_smagorinsky(u, delta, go)
+    return S.create_bardina(2.0, delta, g), lambda u, G, go: O.bardina(u, 2.0, delta, go)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("D,n", [(3, 24), (2, 48)])
+def test_les_rhs_matches_oracle(kind, D, n):
+    if kind == "verstappen" and D == 2:
+        pytest.skip("Q-R model is only defined in 3D")
+    g = S.Grid(D, n, dtype=torch.float64, device="cuda:0")
+    go = O.Grid(D, n)
+    u = O.random_field(go, seed=21, kpeak=3)
+    delta = 2 * go.l / n
+    cl, ref_model = _models(kind, delta, g, D)
+    ref = [O.twothirds(c, go) for c in O.les_rhs(u, go, lambda uu, GG: ref_model(uu, GG, go), 1e-3)]
+    du = S.vectorfield(g)
+    S.les_(du, [to_dev(c, g) for c in u], g, cl, 1e-3)
+    assert rel_l2([to_np(c) for c in du], ref) < TOL64
+    # the closure protocol model(u, G) itself
+    GG = O.physical_gradient(u, go)
+    tau_ref = ref_model(u, GG, go)
+    names = "xyz"[:D]
+    order = [names[a] + names[b] for b in range(D) for a in range(D)]  # G[a + D b]
+    Gt = [to_dev(GG[k], g) for k in order]
+    tau = cl([to_dev(c, g) for c in u], Gt)
+    assert rel_l2(to_np(tau), tau_ref) < 1e-11
+
+
+def test_les_rhs_no_closure_is_convectiondiffusion():
+    g = S.Grid(3, 16, dtype=torch.float64, device="cuda:0")
+    go = O.Grid(3, 16)
+    u = O.random_field(go, seed=2, kpeak=3)
+    du = S.vectorfield(g)
+    S.les_(du, [to_dev(c, g) for c in u], g, None, 1e-2)
+    ref = [O.twothirds(c, go) for c in O.convectiondiffusion(u, go, 1e-2)]
+    assert rel_l2([to_np(c) for c in du], ref) < TOL64
+
+
+@pytest.mark.parametrize("kind", ["clark", "dynsmag"])
+def test_les_wray3_matches_oracle(kind):
+    g = S.Grid(3, 24, dtype=torch.float64, device="cuda:0")
+    go = O.Grid(3, 24)
+    u = O.random_field(go, seed=5, kpeak=3)
+    delta = 4 * go.l / 24
+    cl, ref_model = _models(kind, delta, g, 3)
+    f = lambda uu, gg, visc: O.les_rhs(uu, gg, lambda a, b: ref_model(a, b, gg), visc)  # noqa: E731
+    ref = [O.twothirds(c, go) for c in O.wray3(f, u, 0.01, go, visc=2e-3)]
+    ut = [to_dev(c, g) for c in u]
+    S.les_wray3_(ut, 0.01, g, cl, 2e-3)
+    assert rel_l2([to_np(c) for c in ut], ref) < TOL64
+
+
+def test_les_rk4_fp32_dynsmag():
+    g = S.Grid(3, 32, dtype=torch.float32, device="cuda:0")
+    go = O.Grid(3, 32)
+    u = O.random_field(go, seed=6, kpeak=3)
+    delta = 2 * go.l / 32
+    cl = S.create_dynamic_smagorinsky(delta, g)
+    model = lambda uu, gg: O.dynamic_smagorinsky(uu, delta, go)  # noqa: E731
+    ref = u
+    for _ in range(2):
+        def rhs(v):
+            d = O.les_rhs(v, go, model, 1e-3)
+            return O.project([O.twothirds(c, go) for c in d], go)
+        k1 = rhs(ref)
+        k2 = rhs([a + 0.005 * b for a, b in zip(ref, k1)])
+        k3 = rhs([a + 0.005 * b for a, b in zip(ref, k2)])
+        k4 = rhs([a + 0.01 * b for a, b in zip(ref, k3)])
+        ref = [a + 0.01 / 6 * (b + 2 * c + 2 * d + e) for a, b, c, d, e in zip(ref, k1, k2, k3, k4)]
+    ut = [to_dev(c, g) for c in u]
+    S.les_rk4_(ut, 0.01, g, cl, 1e-3, nsteps=2)
+    assert rel_l2([to_np(c) for c in ut], ref) < 2e-5
+
+
+def test_closure_rejects_bad_arguments():
+    g2 = S.Grid(2, 16, dtype=torch.float64, device="cuda:0")
+    with pytest.raises(S.SymcodeError):
+        S.create_verstappen(0.3, 0.1, g2)  # test/test_closures.jl:56-59
+    with pytest.raises(S.SymcodeError):
+        S.create_clark(-1.0, g2)
