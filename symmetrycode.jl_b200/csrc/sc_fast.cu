@@ -40,7 +40,7 @@ template <int N, int T> struct Col2Cfg {
   static constexpr int NT = T * NJ;
   static constexpr int SR = N2 * T + 8;  // exchange row stride (+8: half-bank shift between rows)
   static constexpr size_t SMEM = size_t(N1) * SR * sizeof(float2);
-  static constexpr int MINB = (3 * NT <= 1024) ? 3 : 1;  // aim at 3 resident CTAs per SM
+  static constexpr int MINB = 1;
 };
 
 template <int N, int T, bool INV>

@@ -1,0 +1,120 @@
+"""
+    SymCodeB200
+
+Julia binding of `libsymcode.so` (C ABI in `include/symcode.h`): the B200 path
+behind SymmetryCode.jl's solver and closure calls.  Each method takes the same
+arguments as the reference function it replaces and operates on `CuArray`s of
+the reference layout (`Complex{T}` of size `(n÷2+1, n, n)`, column-major).
+
+This file is not executed in this repository's test suite (no Julia toolchain
+in the build environment); the same entry points are exercised from Python.
+"""
+module SymCodeB200
+
+using CUDA
+
+const LIB = get(ENV, "SYMCODE_LIB", joinpath(@__DIR__, "..", "libsymcode.so"))
+
+struct SCForcing
+    enabled::Cint
+    eps::Cdouble
+end
+
+function check(status::Cint)
+    status == 0 && return nothing
+    msg = unsafe_string(ccall((:sc_last_error_string, LIB), Cstring, ()))
+    error("libsymcode error $(status): $(msg)")
+end
+
+"Device plan standing in for `Grid{D}(; l, n)` + `getcache(grid)` (src/solver.jl:147, :956)."
+mutable struct Plan
+    ptr::Ptr{Cvoid}
+    D::Int
+    n::Int
+    l::Float64
+    T::DataType
+end
+
+function Plan(D::Int, n::Int, l::Real, ::Type{T}) where {T <: Union{Float32, Float64}}
+    ref = Ref{Ptr{Cvoid}}(C_NULL)
+    ws = Ref{Csize_t}(0)
+    check(ccall((:sc_plan_create, LIB), Cint, (Ptr{Ptr{Cvoid}}, Cint, Cint, Cdouble, Cint, Ptr{Csize_t}),
+        ref, D, n, l, T === Float32 ? 0 : 1, ws))
+    p = Plan(ref[], D, n, Float64(l), T)
+    finalizer(p -> ccall((:sc_plan_destroy, LIB), Cint, (Ptr{Cvoid},), p.ptr), p)
+    return p
+end
+
+stream() = CUDA.stream().handle
+ptrs(u) = [Base.unsafe_convert(CuPtr{Cvoid}, pointer(c)) for c in u]
+
+"`convectiondiffusion!(du, u, grid, cache; visc)` (src/solver.jl:949)."
+function convectiondiffusion!(du, u, p::Plan; visc)
+    check(ccall((:sc_rhs, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Ptr{CuPtr{Cvoid}}, Cdouble, Ptr{Cvoid}),
+        p.ptr, ptrs(u), ptrs(du), visc, stream()))
+    return nothing
+end
+
+"`wray3!(convectiondiffusion!, u, Δt, grid, cache; visc)` (src/solver.jl:968)."
+function wray3!(u, Δt, p::Plan; visc)
+    check(ccall((:sc_wray3_step, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cdouble, Cdouble, Ptr{Cvoid}),
+        p.ptr, ptrs(u), Δt, visc, stream()))
+    return u
+end
+
+"RK4 steps with optional linear band forcing at injection rate `eps` (new)."
+function rk4!(u, Δt, p::Plan; visc, nsteps = 1, eps = nothing)
+    f = Ref(SCForcing(isnothing(eps) ? 0 : 1, isnothing(eps) ? 0.0 : eps))
+    check(ccall((:sc_rk4_steps, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cdouble, Cdouble, Cint, Ptr{SCForcing}, Ptr{Cvoid}),
+        p.ptr, ptrs(u), Δt, visc, nsteps, f, stream()))
+    return u
+end
+
+"`sfs!(; τ, ubar, u, g_dns, g_les, Δ)` (src/data.jl:625) for several widths at once."
+function sfs!(ubars, τs, u, dns::Plan, les::Plan, Δs)
+    d = Cdouble[isnothing(x) ? -1.0 : x for x in Δs]
+    check(ccall((:sc_filter_sfs, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Ptr{Cdouble}, Cint, Ptr{CuPtr{Cvoid}}, Ptr{CuPtr{Cvoid}}, Ptr{Cvoid}),
+        dns.ptr, les.ptr, ptrs(u), d, length(d), reduce(vcat, ptrs.(ubars)), reduce(vcat, ptrs.(τs)), stream()))
+    return nothing
+end
+
+"A closure `model(u, G)` bound to a plan (`create_clark`, `create_dynamic_smagorinsky`, ...)."
+mutable struct Closure
+    ptr::Ptr{Cvoid}
+    plan::Plan
+end
+
+function Closure(p::Plan, kind::Integer, Δ::Real, params::Vector{Float64} = Float64[])
+    ref = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:sc_closure_create, LIB), Cint, (Ptr{Ptr{Cvoid}}, Ptr{Cvoid}, Cint, Cdouble, Ptr{Cdouble}, Cint),
+        ref, p.ptr, kind, Δ, params, length(params)))
+    c = Closure(ref[], p)
+    finalizer(c -> ccall((:sc_closure_destroy, LIB), Cint, (Ptr{Cvoid},), c.ptr), c)
+    return c
+end
+create_clark(Δ, p) = Closure(p, 1, Δ)
+create_smagorinsky(CS, Δ, p) = Closure(p, 2, Δ, [Float64(CS)])
+create_verstappen(C, Δ, p) = Closure(p, 3, Δ, [Float64(C)])
+create_dynamic_smagorinsky(Δ, p) = Closure(p, 4, Δ)
+create_bardina(s, Δ, p) = Closure(p, 5, Δ, [Float64(s)])
+
+"`les!(du, u, grid, cache; model, visc)` (src/les.jl:4)."
+function les!(du, u, p::Plan; model::Union{Nothing, Closure}, visc)
+    m = isnothing(model) ? C_NULL : model.ptr
+    check(ccall((:sc_les_rhs, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Ptr{CuPtr{Cvoid}}, Cdouble, Ptr{Cvoid}),
+        p.ptr, m, ptrs(u), ptrs(du), visc, stream()))
+    return nothing
+end
+
+"`energy(u)` (src/solver.jl:643), FP64 on the device."
+function energy(u, p::Plan)
+    e = Ref{Cdouble}(0)
+    check(ccall((:sc_energy, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, ptrs(u), e, stream()))
+    return e[]
+end
+
+end # module
