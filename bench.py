@@ -222,6 +222,86 @@ def run_reference(args):
     return 0
 
 
+LES_NU = (1e-3, 6e-4, 3e-4, 1.5e-4)
+LES_DH = (2, 4, 8)
+LES_N, LES_DT, LES_SEED = 128, 5e-3, 3
+
+
+def les_batch_measure(dev, steps, warmup, plain_steps=2):
+    """Batched LES at 128^3: 12 instances nu x Delta/h in one graph-captured step,
+    against the plain per-instance FP64 path (one instance after another, eager
+    launches, no graph).  Initial fields: sfs! of a seeded 256^3 field."""
+    import torch
+    import symcode as S
+
+    gd = S.Grid(3, 256, dtype=torch.float32, device=dev)
+    uc = initial_compact(256, LES_SEED)
+    u_dns = [c.to(dev) for c in to_full(uc, 256, torch.float32)]
+    specs = [(nu, dh, i % 2) for i, (nu, dh) in enumerate((nu, dh) for nu in LES_NU for dh in LES_DH)]
+    fields = {}
+    for dh in LES_DH:
+        gl = S.Grid(3, LES_N, dtype=torch.float32, device=dev)
+        ub, ta = S.vectorfield(gl), S.tensorfield(gl)
+        S.sfs_(ub, ta, u_dns, gd, gl, dh * gl.l / LES_N)
+        fields[dh] = [c.clone() for c in ub]
+        gl.close()
+    del u_dns
+    gd.close()
+
+    def make(dtype):
+        insts, keep = [], []
+        for nu, dh, kind in specs:
+            g = S.Grid(3, LES_N, dtype=dtype, device=dev)
+            delta = dh * g.l / LES_N
+            cl = S.create_dynamic_smagorinsky(delta, g) if kind == 0 else S.create_clark(delta, g)
+            S.State(g).load([c.to(g.cdtype) for c in fields[dh]])
+            insts.append(dict(grid=g, closure=cl, visc=nu, dt=LES_DT, eps=None))
+            keep.append((g, cl))
+        return insts, keep
+
+    stream = torch.cuda.current_stream()
+    insts, keep = make(torch.float32)
+    batch = S.LesBatch(insts)
+    batch.run(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_batch = e0.elapsed_time(e1) / steps
+    status, _ = batch.status()
+    batch.close()
+    del insts, keep
+    torch.cuda.empty_cache()
+
+    insts64, keep64 = make(torch.float64)
+    for d in insts64:
+        S.set_option(d["grid"], 1, 0)  # eager launches
+        S.State(d["grid"]).les_rk4(d["closure"], LES_DT, d["visc"], 1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(plain_steps):
+        for d in insts64:
+            S.State(d["grid"]).les_rk4(d["closure"], LES_DT, d["visc"], 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_plain = e0.elapsed_time(e1) / plain_steps
+    del insts64, keep64
+    torch.cuda.empty_cache()
+    return {
+        "metric": "batched LES steps/s (12 x 128^3, one RK4 step of every instance per step)",
+        "value": 1e3 / ms_batch, "unit": "steps/s", "ms_per_step": ms_batch,
+        "plain_fp64_per_instance_steps_per_s": 1e3 / ms_plain,
+        "speedup_vs_plain": ms_plain / ms_batch,
+        "closures": "6 dynamic Smagorinsky + 6 Clark (CNN closure not built in this build)",
+        "instances": [{"nu": nu, "delta_over_h": dh, "closure": "dynsmag" if k == 0 else "clark"} for nu, dh, k in specs],
+        "diverged": [i for i, s_ in enumerate(status) if s_ != 0],
+        "config": f"FP32, RK4 dt={LES_DT}, unforced, initial fields sfs! of a seeded 256^3 field (k_p=4, seed {LES_SEED}); "
+                  "plain path: the same instances in FP64, one after another, eager launches",
+    }
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -327,6 +407,10 @@ def run_gpu(args):
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps + 8}
 
+    les = None
+    if rank == 0 and not args.skip_les:
+        les = les_batch_measure(dev, args.les_steps, 3)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         sec = cpu_sample_steps(args.cpu_sample_n, 1)
@@ -354,6 +438,7 @@ def run_gpu(args):
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
+            "les_batch": les,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -373,6 +458,8 @@ def main():
     ap.add_argument("--cpu-sample-n", type=int, default=256)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-les", action="store_true")
+    ap.add_argument("--les-steps", type=int, default=10)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

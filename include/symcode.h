@@ -188,6 +188,35 @@ SC_API int sc_les_rk4_steps(sc_plan* plan, sc_closure* closure, void* const* u_h
 SC_API int sc_state_les_rk4(sc_plan* plan, sc_closure* closure, double dt, double visc, int nsteps,
                             const sc_forcing* forcing, void* stream);
 
+/* ---- batched LES ----------------------------------------------------------------
+ * No reference counterpart (the reference runs one LES per process,
+ * src/les.jl:56-186).  Each instance owns a plan (its device-resident state is
+ * loaded with sc_state_load), an optional closure, nu, dt and forcing.  One RK4
+ * step of every active instance is captured into one CUDA graph (one branch
+ * per instance, so instances run concurrently) followed by an FP64 energy
+ * guard; sc_les_batch_run replays it.  An instance whose energy exceeds 1e5 or
+ * is not finite gets status SC_ERR_DIVERGED (the blow-up guard of solve_les!,
+ * src/les.jl:224-237); sc_les_batch_status(..., freeze = 1) drops such
+ * instances from later steps without stopping the others. */
+typedef struct sc_les_instance {
+  sc_plan* plan;
+  sc_closure* closure;
+  double visc;
+  double dt;
+  int forced;
+  double eps;
+} sc_les_instance;
+typedef struct sc_les_batch sc_les_batch;
+SC_API int sc_les_batch_create(sc_les_batch** batch, const sc_les_instance* instances, int ninstances);
+SC_API int sc_les_batch_run(sc_les_batch* batch, int nsteps, void* stream);
+/* Synchronous: per-instance status and energy (energy may be NULL). */
+SC_API int sc_les_batch_status(sc_les_batch* batch, int* status, double* energy, int freeze, void* stream);
+SC_API int sc_les_batch_destroy(sc_les_batch* batch);
+
+/* ---- plan options ---------------------------------------------------------------- */
+#define SC_OPT_USE_GRAPH 1 /* 1 (default): steppers replay a captured CUDA graph; 0: launch eagerly */
+SC_API int sc_plan_set_option(sc_plan* plan, int option, long long value);
+
 /* ---- DNS -> LES filter ------------------------------------------------------
  * sfs!(; tau, ubar, u, g_dns, g_les, Delta) (src/data.jl:625-642) for `ndelta`
  * filter widths at once (the DNS products are computed once and shared):

@@ -68,6 +68,7 @@ struct sc_plan {
   double k_rk4[5] = {0, 0, 0, 0, 0};
   cudaGraphExec_t g_wray = nullptr;
   double k_wray[3] = {0, 0, 0};
+  int use_graph = 1;  // SC_OPT_USE_GRAPH
 };
 
 // A closure model `model(u, G) -> tau` (src/les.jl:19, src/closures.jl) bound
@@ -90,6 +91,21 @@ struct sc_closure {
   void* cb[12] = {};  // batched-transform scratch (kx, y, z)
   double* dsum = nullptr;  // [<ML>, <MM>, c]
   std::vector<void*> allocs;
+};
+
+// Batched LES: several independent instances (own plan, state, closure, nu,
+// dt, forcing) advanced by one CUDA graph per step with one branch per instance.
+struct sc_les_batch {
+  std::vector<sc_les_instance> inst;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  std::vector<int> active;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  double* energy = nullptr;  // [ninst] FP64 energies of the last guard
+  int* status = nullptr;     // [ninst] 0 ok, SC_ERR_DIVERGED
+  int dev = 0;
 };
 
 namespace {
@@ -524,6 +540,17 @@ int run_rk4_graph(sc_plan* p, double dt, double visc, int nsteps, const sc_forci
 }
 
 template <typename R>
+int run_rk4(sc_plan* p, double dt, double visc, int nsteps, const sc_forcing* frc, cudaStream_t st,
+            sc_closure* cl = nullptr) {
+  if (p->use_graph) return run_rk4_graph<R>(p, dt, visc, nsteps, frc, st, cl);
+  for (int i = 0; i < nsteps; ++i) {
+    int rc = rk4_step<R>(p, dt, visc, frc, st, cl);
+    if (rc) return rc;
+  }
+  return SC_OK;
+}
+
+template <typename R>
 int run_wray_graph(sc_plan* p, double dt, double visc, cudaStream_t st, sc_closure* cl = nullptr) {
   double key[3] = {dt, visc, 0.0};
   std::memcpy(&key[2], &cl, sizeof(cl));
@@ -810,7 +837,7 @@ int sc_state_rk4(sc_plan* p, double dt, double visc, int nsteps, const sc_forcin
   int rc = ensure_device(p);
   if (rc) return rc;
   if (nsteps == 0) return SC_OK;
-  return SC_DTYPE_DISPATCH(p, run_rk4_graph, p, dt, visc, nsteps, frc, as_stream(stream));
+  return SC_DTYPE_DISPATCH(p, run_rk4, p, dt, visc, nsteps, frc, as_stream(stream));
 }
 
 int sc_state_rk4_launches_per_step(const sc_plan* p, int forced) {
@@ -1142,7 +1169,7 @@ int sc_state_les_rk4(sc_plan* p, sc_closure* cl, double dt, double visc, int nst
   if (nsteps < 0) return fail(SC_ERR_INVALID, "nsteps must be >= 0");
   int rc = ensure_device(p);
   if (rc || nsteps == 0) return rc;
-  return SC_DTYPE_DISPATCH(p, run_rk4_graph, p, dt, visc, nsteps, frc, as_stream(stream), cl);
+  return SC_DTYPE_DISPATCH(p, run_rk4, p, dt, visc, nsteps, frc, as_stream(stream), cl);
 }
 
 int sc_les_rk4_steps(sc_plan* p, sc_closure* cl, void* const* u, double dt, double visc, int nsteps,
@@ -1161,6 +1188,149 @@ int sc_les_wray3_step(sc_plan* p, sc_closure* cl, void* const* u, double dt, dou
   rc = SC_DTYPE_DISPATCH(p, run_wray_graph, p, dt, visc, as_stream(stream), cl);
   if (rc) return rc;
   return sc_state_store(p, u, stream);
+}
+
+int sc_plan_set_option(sc_plan* p, int option, long long value) {
+  if (!p) return fail(SC_ERR_INVALID, "null plan");
+  if (option == SC_OPT_USE_GRAPH) { p->use_graph = value ? 1 : 0; return SC_OK; }
+  return fail(SC_ERR_INVALID, "unknown option %d", option);
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void k_guard(const double* e, int* status, int n, double limit) {
+  const int i = threadIdx.x;
+  if (i < n) {
+    const double v = e[i];
+    if (!(v <= limit)) status[i] = SC_ERR_DIVERGED;  // also catches NaN
+  }
+}
+
+int batch_capture(sc_les_batch* b) {
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  const int ni = (int)b->inst.size();
+  cudaGraph_t g;
+  SC_CU(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
+  int rc = SC_OK;
+  cudaEventRecord(b->fork, b->origin);
+  for (int i = 0; i < ni && !rc; ++i) {
+    if (!b->active[i]) continue;
+    const sc_les_instance& in = b->inst[i];
+    cudaStreamWaitEvent(b->streams[i], b->fork, 0);
+    sc_forcing f{in.forced, in.eps};
+    rc = in.plan->dtype == SC_FLOAT64
+             ? rk4_step<double>(in.plan, in.dt, in.visc, &f, b->streams[i], in.closure)
+             : rk4_step<float>(in.plan, in.dt, in.visc, &f, b->streams[i], in.closure);
+    if (rc) break;
+    cudaMemsetAsync(b->energy + i, 0, sizeof(double), b->streams[i]);
+    sc_plan* p = in.plan;
+    if (p->dtype == SC_FLOAT64)
+      sc::launch_spectral_energy<double>((const void* const*)p->U, p->D, p->D, p->n, p->K1, p->K2, 1, p->kc,
+                                         2.0 * M_PI / p->l, 0, b->energy + i, b->streams[i]);
+    else
+      sc::launch_spectral_energy<float>((const void* const*)p->U, p->D, p->D, p->n, p->K1, p->K2, 1, p->kc,
+                                        2.0 * M_PI / p->l, 0, b->energy + i, b->streams[i]);
+    cudaEventRecord(b->events[i], b->streams[i]);
+    cudaStreamWaitEvent(b->origin, b->events[i], 0);
+  }
+  // energy is accumulated as sum |u|^2 (RFFT weights); the guard limit is 2 * 1e5
+  k_guard<<<1, 256, 0, b->origin>>>(b->energy, b->status, ni, 2.0e5);
+  cudaError_t e = cudaStreamEndCapture(b->origin, &g);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(SC_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { b->graph = nullptr; return fail(SC_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e)); }
+  return SC_OK;
+}
+
+void batch_free(sc_les_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto s : b->streams) cudaStreamDestroy(s);
+  for (auto e : b->events) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  if (b->energy) cudaFree(b->energy);
+  if (b->status) cudaFree(b->status);
+}
+}  // namespace
+
+extern "C" {
+
+int sc_les_batch_create(sc_les_batch** out, const sc_les_instance* inst, int ninst) {
+  if (!out || !inst || ninst < 1 || ninst > 256) return fail(SC_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  int dev = inst[0].plan ? inst[0].plan->dev : 0;
+  for (int i = 0; i < ninst; ++i) {
+    if (!inst[i].plan) return fail(SC_ERR_INVALID, "instance %d has no plan", i);
+    if (inst[i].plan->dev != dev) return fail(SC_ERR_INVALID, "instances must share one device");
+    if (inst[i].closure && inst[i].closure->p != inst[i].plan)
+      return fail(SC_ERR_INVALID, "instance %d: closure belongs to another plan", i);
+    for (int j = 0; j < i; ++j)
+      if (inst[j].plan == inst[i].plan) return fail(SC_ERR_INVALID, "instances %d and %d share a plan", j, i);
+  }
+  SC_CU(cudaSetDevice(dev));
+  sc_les_batch* b = new sc_les_batch();
+  b->inst.assign(inst, inst + ninst);
+  b->active.assign(ninst, 1);
+  b->dev = dev;
+  int rc = SC_OK;
+  if (cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaMalloc((void**)&b->energy, ninst * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&b->status, ninst * sizeof(int)) != cudaSuccess)
+    rc = fail(SC_ERR_CUDA, "batch resources");
+  for (int i = 0; i < ninst && !rc; ++i) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      rc = fail(SC_ERR_CUDA, "batch streams");
+      break;
+    }
+    b->streams.push_back(s);
+    b->events.push_back(e);
+  }
+  if (!rc && cudaMemset(b->status, 0, ninst * sizeof(int)) != cudaSuccess) rc = fail(SC_ERR_CUDA, "memset");
+  if (!rc) rc = batch_capture(b);
+  if (rc) { batch_free(b); delete b; return rc; }
+  *out = b;
+  return SC_OK;
+}
+
+int sc_les_batch_run(sc_les_batch* b, int nsteps, void* stream) {
+  if (!b || nsteps < 0) return fail(SC_ERR_INVALID, "bad argument");
+  SC_CU(cudaSetDevice(b->dev));
+  for (int i = 0; i < nsteps; ++i) SC_CU(cudaGraphLaunch(b->graph, as_stream(stream)));
+  return SC_OK;
+}
+
+int sc_les_batch_status(sc_les_batch* b, int* status, double* energy, int freeze, void* stream) {
+  if (!b || !status) return fail(SC_ERR_INVALID, "bad argument");
+  SC_CU(cudaSetDevice(b->dev));
+  const int ni = (int)b->inst.size();
+  std::vector<double> e(ni);
+  SC_CU(cudaMemcpyAsync(status, b->status, ni * sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream)));
+  SC_CU(cudaMemcpyAsync(e.data(), b->energy, ni * sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)));
+  SC_CU(cudaStreamSynchronize(as_stream(stream)));
+  if (energy)
+    for (int i = 0; i < ni; ++i) energy[i] = 0.5 * e[i];
+  if (freeze) {
+    bool changed = false;
+    for (int i = 0; i < ni; ++i)
+      if (status[i] != 0 && b->active[i]) { b->active[i] = 0; changed = true; }
+    if (changed) return batch_capture(b);
+  }
+  return SC_OK;
+}
+
+int sc_les_batch_destroy(sc_les_batch* b) {
+  if (!b) return SC_OK;
+  cudaSetDevice(b->dev);
+  batch_free(b);
+  delete b;
+  return SC_OK;
 }
 
 int sc_twothirds(sc_plan* p, void* const* f, int ncomp, void* stream) {

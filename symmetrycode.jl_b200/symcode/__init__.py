@@ -19,13 +19,13 @@ import math
 import torch
 
 from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
-                   ptr_array, sc_forcing)
+                   ptr_array, sc_forcing, sc_les_instance)
 
 __all__ = [
     "Grid", "SymcodeError", "scalarfield", "vectorfield", "tensorfield", "spacescalarfield",
     "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
     "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
-    "State", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
+    "State", "LesBatch", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
     "create_dynamic_smagorinsky", "create_bardina", "les_", "les_wray3_", "les_rk4_",
 ]
 
@@ -348,6 +348,51 @@ def les_rk4_(u, dt, g: Grid, model, visc, nsteps=1, eps=None, stream=None):
     check(lib().sc_les_rk4_steps(g.plan, _cl(model), pu, float(dt), float(visc), int(nsteps), ct.byref(f),
                                  _stream_ptr(stream)))
     return u
+
+
+class LesBatch:
+    """Batched LES (``sc_les_batch_*``): instances = list of dicts with keys
+    ``grid`` (its State already loaded), ``closure`` (or None), ``visc``, ``dt``,
+    ``eps`` (None = unforced).  One CUDA graph advances all of them per step."""
+
+    def __init__(self, instances):
+        n = len(instances)
+        arr = (sc_les_instance * n)()
+        for i, d in enumerate(instances):
+            eps = d.get("eps")
+            arr[i] = sc_les_instance(d["grid"].plan.value, _cl(d.get("closure")).value if d.get("closure") else None,
+                                     float(d["visc"]), float(d["dt"]), 1 if eps is not None else 0,
+                                     float(eps or 0.0))
+        self.n = n
+        self.instances = instances
+        ptr = ct.c_void_p()
+        check(lib().sc_les_batch_create(ct.byref(ptr), arr, n))
+        self._ptr = ptr
+
+    def run(self, nsteps, stream=None):
+        check(lib().sc_les_batch_run(self._ptr, int(nsteps), _stream_ptr(stream)))
+
+    def status(self, freeze=False, stream=None):
+        st = (ct.c_int * self.n)()
+        en = (ct.c_double * self.n)()
+        check(lib().sc_les_batch_status(self._ptr, st, en, 1 if freeze else 0, _stream_ptr(stream)))
+        return list(st), list(en)
+
+    def close(self):
+        if getattr(self, "_ptr", None):
+            lib().sc_les_batch_destroy(self._ptr)
+            self._ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def set_option(g: Grid, option, value):
+    """``sc_plan_set_option`` (1 = use CUDA graphs for the steppers)."""
+    check(lib().sc_plan_set_option(g.plan, int(option), int(value)))
 
 
 class State:

@@ -30,6 +30,11 @@ class sc_forcing(ct.Structure):
     _fields_ = [("enabled", ct.c_int), ("eps", ct.c_double)]
 
 
+class sc_les_instance(ct.Structure):
+    _fields_ = [("plan", ct.c_void_p), ("closure", ct.c_void_p), ("visc", ct.c_double), ("dt", ct.c_double),
+                ("forced", ct.c_int), ("eps", ct.c_double)]
+
+
 _vp = ct.c_void_p
 _pp = ct.POINTER(ct.c_void_p)
 
@@ -63,6 +68,11 @@ _SIGS = {
     "sc_les_wray3_step": ([_vp, _vp, _pp, ct.c_double, ct.c_double, _vp], ct.c_int),
     "sc_les_rk4_steps": ([_vp, _vp, _pp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(sc_forcing), _vp], ct.c_int),
     "sc_state_les_rk4": ([_vp, _vp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(sc_forcing), _vp], ct.c_int),
+    "sc_les_batch_create": ([ct.POINTER(_vp), ct.POINTER(sc_les_instance), ct.c_int], ct.c_int),
+    "sc_les_batch_run": ([_vp, ct.c_int, _vp], ct.c_int),
+    "sc_les_batch_status": ([_vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, _vp], ct.c_int),
+    "sc_les_batch_destroy": ([_vp], ct.c_int),
+    "sc_plan_set_option": ([_vp, ct.c_int, ct.c_longlong], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
 }

@@ -106,3 +106,43 @@ def test_closure_rejects_bad_arguments():
         S.create_verstappen(0.3, 0.1, g2)  # test/test_closures.jl:56-59
     with pytest.raises(S.SymcodeError):
         S.create_clark(-1.0, g2)
+
+
+def test_les_batch_matches_single_instances_and_guard():
+    """Three heterogeneous instances in one graph equal the same instances run one
+    by one; a blown-up instance is flagged and frozen without stopping the others."""
+    n = 32
+    go = O.Grid(3, n)
+    specs = [(1e-3, "dynsmag", 2, 0.1), (6e-4, "clark", 4, None), (3e-4, "smagorinsky", 2, 0.1),
+             (1e-3, "clark", 2, None)]
+    fields = [O.random_field(go, seed=30 + i, kpeak=3) for i in range(len(specs))]
+    fields[3] = [c * 2e3 for c in fields[3]]  # energy far above the 1e5 blow-up limit
+    ref = []
+    for (nu, kind, dh, eps), u in zip(specs, fields):
+        g = S.Grid(3, n, dtype=torch.float32, device="cuda:0")
+        cl, _ = _models(kind, dh * go.l / n, g, 3)
+        st = S.State(g)
+        st.load([to_dev(c, g) for c in u])
+        st.les_rk4(cl, 2e-3, nu, nsteps=3, eps=eps)
+        out = S.vectorfield(g)
+        st.store(out)
+        ref.append([to_np(c) for c in out])
+    grids, insts = [], []
+    for (nu, kind, dh, eps), u in zip(specs, fields):
+        g = S.Grid(3, n, dtype=torch.float32, device="cuda:0")
+        cl, _ = _models(kind, dh * go.l / n, g, 3)
+        S.State(g).load([to_dev(c, g) for c in u])
+        grids.append((g, cl))
+        insts.append(dict(grid=g, closure=cl, visc=nu, dt=2e-3, eps=eps))
+    b = S.LesBatch(insts)
+    b.run(3)
+    status, energy = b.status(freeze=True)
+    assert status[:3] == [0, 0, 0] and status[3] != 0
+    for i in range(3):
+        g = grids[i][0]
+        out = S.vectorfield(g)
+        S.State(g).store(out)
+        assert rel_l2([to_np(c) for c in out], ref[i]) < 1e-6
+    b.run(2)  # the frozen instance no longer advances; the others keep going
+    status2, _ = b.status()
+    assert status2[:3] == [0, 0, 0]
