@@ -54,7 +54,8 @@ typedef enum sc_status {
   SC_ERR_CUDA = 3,         /* CUDA runtime error */
   SC_ERR_OOM = 4,          /* device allocation failed */
   SC_ERR_DIVERGED = 5,     /* blow-up guard tripped (energy > limit or non-finite) */
-  SC_ERR_UNSUPPORTED = 6   /* valid request outside what this build implements */
+  SC_ERR_UNSUPPORTED = 6,  /* valid request outside what this build implements */
+  SC_ERR_TIMEOUT = 7       /* a bounded device-side wait ran out (kernel returned early) */
 } sc_status;
 
 /* Linear band forcing of the RK4 stepper: f_hat = A u_hat on 1 <= |k|^2 < 9
@@ -167,6 +168,18 @@ typedef struct sc_closure sc_closure;
 SC_API int sc_closure_create(sc_closure** closure, sc_plan* plan, int kind, double delta, const double* params,
                              int nparams);
 SC_API int sc_closure_destroy(sc_closure* closure);
+/* CNN closure (new; no reference counterpart; SURVEY configs[3]): input u (3
+ * physical channels) plus the standardised log Re_Delta, (log(Delta^2
+ * sqrt(<|grad u|^2>)/visc) - mu)/sigma, as a 4th constant channel (the
+ * convention of fullchain, src/nets.jl:311-331); four 3x3x3 periodic
+ * convolutions 4->32->32->32->6 with exact GELU between them; output tau in
+ * pair order.  BF16 weights and activations, FP32 accumulation on tcgen05
+ * tensor cores.  weights[l]: host FP32 (C_out, C_in, 3, 3, 3) (rounded to BF16
+ * here), biases[l]: host FP32 (C_out).  FP32 3D plans with n = 128. */
+SC_API int sc_cnn_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc,
+                                 const float* const* weights, const float* const* biases, double mu, double sigma);
+/* Synchronous: SC_ERR_TIMEOUT if a bounded wait of the closure's kernels ran out. */
+SC_API int sc_closure_status(sc_closure* closure, int* status);
 /* model(u, G): the packed physical stress tau (3|6 fields, pair order) from
  * the spectral velocity u_hat (full layout) and the physical velocity
  * gradient G (D*D fields, G[a + D b] = d u_a / d x_b; Clark, Smagorinsky and

@@ -30,3 +30,4 @@ from .spectral import *  # noqa: F401,F403
 from .filtering import *  # noqa: F401,F403
 from .closures import *  # noqa: F401,F403
 from .les import *  # noqa: F401,F403
+from .cnn import *  # noqa: F401,F403

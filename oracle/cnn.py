@@ -1,0 +1,74 @@
+"""FP64 restatement of the CNN closure (new; no reference counterpart) with the
+BF16 rounding of weights and activations emulated, for checking the tensor-core
+kernels.  Test infrastructure only (see ``oracle/__init__.py``).
+
+The network: input channels (u_x, u_y, u_z, z) with z = (log Re_Delta - mu)/sigma,
+Re_Delta = Delta^2 sqrt(<|grad u|^2>)/nu (the ``fullchain`` convention,
+src/nets.jl:311-331); four 3x3x3 periodic cross-correlations
+4->32->32->32->6 with exact GELU between them.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+from scipy.special import erf
+
+from .spectral import Grid, getenergy, twothirds, vectorgradient
+
+__all__ = ["bf16", "cnn_redelta_channel", "cnn_rows"]
+
+
+def bf16(x):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    f = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    b = f.view(np.uint32).astype(np.uint64)
+    lsb = (b >> 16) & 1
+    b = ((b + 0x7FFF + lsb) & 0xFFFF0000).astype(np.uint32)
+    return b.view(np.float32).astype(np.float64)
+
+
+def cnn_redelta_channel(u, g: Grid, delta, nu, mu=0.0, sigma=1.0):
+    A = vectorgradient(u, g)
+    a2 = sum(getenergy(twothirds(v, g)) for v in A.values())
+    return (math.log(delta * delta * math.sqrt(a2) / nu) - mu) / sigma
+
+
+def _conv(act, w, b, z_lo, z_hi, y_lo, y_hi):
+    """Periodic 3x3x3 cross-correlation on the window; act: (C, Z, Y, X) covering
+    rows z_lo-1..z_hi+1, y_lo-1..y_hi+1 (window-relative), full periodic x."""
+    cout = w.shape[0]
+    Z = z_hi - z_lo + 1
+    Y = y_hi - y_lo + 1
+    X = act.shape[-1]
+    out = np.zeros((cout, Z, Y, X))
+    for kz in range(3):
+        for ky in range(3):
+            for kx in range(3):
+                sl = act[:, z_lo + kz - 1:z_lo + kz - 1 + Z, y_lo + ky - 1:y_lo + ky - 1 + Y, :]
+                sl = np.roll(sl, -(kx - 1), axis=-1)
+                out += np.einsum("oc,czyx->ozyx", w[:, :, kz, ky, kx], sl)
+    return out + b[:, None, None, None]
+
+
+def cnn_rows(uphys, zval, weights, biases, rows):
+    """tau (6, len(rows), n) at the x-rows ``rows`` = [(y, z), ...] of the periodic grid.
+
+    uphys: (3, n, n, n) physical velocity indexed [c, z, y, x].
+    """
+    n = uphys.shape[-1]
+    ws = [bf16(w) for w in weights]
+    out = []
+    for (y0, z0) in rows:
+        idx_z = [(z0 + d) % n for d in range(-4, 5)]
+        idx_y = [(y0 + d) % n for d in range(-4, 5)]
+        win = uphys[:, idx_z][:, :, idx_y]  # (3, 9, 9, n)
+        act = np.concatenate([bf16(win), np.full((1,) + win.shape[1:], bf16(np.array([zval]))[0])], 0)
+        for li in range(4):
+            h = 4 - li  # input window half-width
+            act = _conv(act, ws[li], biases[li].astype(np.float64), 1, 2 * h - 1, 1, 2 * h - 1)
+            if li < 3:
+                act = bf16(0.5 * act * (1.0 + erf(act / math.sqrt(2.0))))
+        out.append(act[:, 0, 0, :])
+    return np.stack(out, 1)

@@ -16,6 +16,7 @@
 #include "sc_fft.cuh"
 #include "sc_internal.h"
 #include "sc_les.h"
+#include "sc_cnn.h"
 #include "symcode.h"
 
 namespace {
@@ -89,7 +90,13 @@ struct sc_closure {
   void* ph4[3] = {};  // physical test-filtered velocity
   void* bb[12] = {};  // batched-transform scratch (kx, ky, z)
   void* cb[12] = {};  // batched-transform scratch (kx, y, z)
-  double* dsum = nullptr;  // [<ML>, <MM>, c]
+  double* dsum = nullptr;  // [<ML>, <MM>, c] (dynamic Smagorinsky); [a2, -, -, z] (CNN)
+  // CNN closure
+  void* cw[4] = {};   // packed BF16 weights per layer
+  void* cbias[4] = {};
+  void* act[3] = {};  // BF16 activations
+  int* err = nullptr;
+  double nu = 0, mu = 0, sigma = 1;
   std::vector<void*> allocs;
 };
 
@@ -395,6 +402,29 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
     sc::launch_spec_filter<R>(sc_, D, st);
     if (tau_phys_out) return c2p_batch<R>(p, cl->bb, cl->cb, cl->th, tau_phys_out, NP, st);
     return check_launch("dynamic Smagorinsky");
+  } else if (cl->kind == sc::kCnn) {
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, u, cl->gp, D, st))) return rc;  // u (physical)
+    SC_CU(cudaMemsetAsync(cl->dsum, 0, sizeof(double), st));
+    sc::launch_spectral_energy<R>(u, D, D, p->n, p->K1, p->K2, 1, p->kc, 2.0 * M_PI / p->l, 1, cl->dsum, st);
+    sc::CnnArgs a{};
+    for (int c = 0; c < 3; ++c) a.u[c] = cl->gp[c];
+    for (int l = 0; l < 4; ++l) {
+      a.w[l] = static_cast<const __nv_bfloat16*>(cl->cw[l]);
+      a.b[l] = static_cast<const float*>(cl->cbias[l]);
+    }
+    a.act0 = static_cast<__nv_bfloat16*>(cl->act[0]);
+    a.act1 = static_cast<__nv_bfloat16*>(cl->act[1]);
+    a.act2 = static_cast<__nv_bfloat16*>(cl->act[2]);
+    for (int c = 0; c < 6; ++c) a.tau.p[c] = static_cast<float*>(cl->tp[c]);
+    a.a2 = cl->dsum; a.z = cl->dsum + 3;
+    a.delta = cl->delta; a.nu = cl->nu; a.mu = cl->mu; a.sigma = cl->sigma;
+    a.err = cl->err;
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    a.nsm = nsm;
+    sc::launch_cnn_forward(a, st);
+    if ((rc = check_launch("cnn closure"))) return rc;
   } else {
     return fail(SC_ERR_UNSUPPORTED, "closure kind %d has no evaluation in this build", cl->kind);
   }
@@ -1094,6 +1124,83 @@ int sc_closure_create(sc_closure** out, sc_plan* p, int kind, double delta, cons
   return SC_OK;
 }
 
+static uint16_t host_bf16(float f) {
+  uint32_t x;
+  std::memcpy(&x, &f, 4);
+  if ((x & 0x7f800000u) == 0x7f800000u) return uint16_t((x >> 16) | ((x & 0xffffu) ? 0x40u : 0u));  // inf/nan
+  const uint32_t lsb = (x >> 16) & 1u;
+  x += 0x7fffu + lsb;  // round to nearest even
+  return uint16_t(x >> 16);
+}
+
+int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, const float* const* weights,
+                          const float* const* biases, double mu, double sigma) {
+  if (!out || !p || !weights || !biases) return fail(SC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->dtype != SC_FLOAT32 || !sc::cnn_supported(p->n, p->D))
+    return fail(SC_ERR_UNSUPPORTED, "the CNN closure runs on FP32 3D plans with n = 128");
+  if (!(delta > 0) || !(visc > 0) || !(sigma > 0)) return fail(SC_ERR_INVALID, "delta, visc and sigma must be positive");
+  for (int l = 0; l < 4; ++l)
+    if (!weights[l] || !biases[l]) return fail(SC_ERR_INVALID, "missing weights of layer %d", l);
+  sc_closure* cl = nullptr;
+  int rc = sc_closure_create(&cl, p, sc::kClark, delta, nullptr, 0);  // allocates the common scratch
+  if (rc) return rc;
+  cl->kind = sc::kCnn;
+  cl->nu = visc; cl->mu = mu; cl->sigma = sigma;
+  static const int cin[4] = {4, 32, 32, 32}, cout[4] = {32, 32, 32, 6}, cp[4] = {16, 32, 32, 32},
+                   cop[4] = {32, 32, 32, 16};
+  const size_t npts = (size_t)p->n * p->n * p->n;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  for (int l = 0; l < 4 && !rc; ++l) {
+    const int cpc = cp[l] / 8;
+    std::vector<uint16_t> wp((size_t)27 * cpc * cop[l] * 8, 0);
+    for (int t = 0; t < 27; ++t)
+      for (int kc = 0; kc < cpc; ++kc)
+        for (int nn = 0; nn < cout[l]; ++nn)
+          for (int j = 0; j < 8; ++j) {
+            const int ci = 8 * kc + j;
+            if (ci >= cin[l]) continue;
+            // PyTorch conv3d layout (Cout, Cin, kz, ky, kx); tap t = kz*9 + ky*3 + kx
+            const float w = weights[l][((size_t)nn * cin[l] + ci) * 27 + t];
+            wp[(((size_t)t * cpc + kc) * cop[l] + nn) * 8 + j] = host_bf16(w);
+          }
+    std::vector<float> bp(cop[l], 0.f);
+    for (int nn = 0; nn < cout[l]; ++nn) bp[nn] = biases[l][nn];
+    if (!rc) rc = A(&cl->cw[l], wp.size() * 2);
+    if (!rc) rc = A(&cl->cbias[l], bp.size() * 4);
+    if (!rc && (cudaMemcpy(cl->cw[l], wp.data(), wp.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+                cudaMemcpy(cl->cbias[l], bp.data(), bp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+      rc = fail(SC_ERR_CUDA, "weight upload");
+  }
+  if (!rc) rc = A(&cl->act[0], npts * 16 * 2);
+  if (!rc) rc = A(&cl->act[1], npts * 32 * 2);
+  if (!rc) rc = A(&cl->act[2], npts * 32 * 2);
+  if (!rc) rc = A((void**)&cl->err, sizeof(int));
+  if (!rc && cudaMemset(cl->err, 0, sizeof(int)) != cudaSuccess) rc = fail(SC_ERR_CUDA, "memset");
+  if (!rc) {
+    sc::cnn_init();
+    if (cudaGetLastError() != cudaSuccess) rc = fail(SC_ERR_CUDA, "CNN kernel setup");
+  }
+  if (rc) { sc_closure_destroy(cl); return rc; }
+  *out = cl;
+  return SC_OK;
+}
+
+int sc_closure_status(sc_closure* cl, int* status) {
+  if (!cl || !status) return fail(SC_ERR_INVALID, "null argument");
+  *status = 0;
+  if (!cl->err) return SC_OK;
+  int h = 0;
+  SC_CU(cudaMemcpy(&h, cl->err, sizeof(int), cudaMemcpyDeviceToHost));
+  *status = h ? SC_ERR_TIMEOUT : SC_OK;
+  return SC_OK;
+}
+
 int sc_closure_destroy(sc_closure* cl) {
   if (!cl) return SC_OK;
   sc_plan* p = cl->p;
@@ -1133,7 +1240,14 @@ int sc_closure_eval(sc_closure* cl, const void* const* u, const void* const* G, 
     if (r) return r;
     if ((r = pack_state<R>(p, u, p->S, st))) return r;
     if ((r = products<R>(p, p->S, st))) return r;
-    return closure_tauhat<R>(cl, p->S, st, tau);
+    if ((r = closure_tauhat<R>(cl, p->S, st, tau))) return r;
+    if (cl->err) {
+      int h = 0;
+      SC_CU(cudaMemcpyAsync(&h, cl->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+      SC_CU(cudaStreamSynchronize(st));
+      if (h) return fail(SC_ERR_TIMEOUT, "a bounded wait of the CNN kernel ran out");
+    }
+    return SC_OK;
   };
   return p->dtype == SC_FLOAT64 ? body(double()) : body(float());
 }

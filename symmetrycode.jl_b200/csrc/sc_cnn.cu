@@ -1,0 +1,274 @@
+// CNN closure (new; no reference counterpart): 3x3x3 periodic convolutions on
+// the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32
+// accumulators in tensor memory).
+//
+// Network (per LES instance, 128^3): input u (3 physical channels) and the
+// standardised log Re_Delta as a constant 4th channel, conv 4->32, GELU,
+// conv 32->32, GELU, conv 32->32, GELU, conv 32->6 -> tau (pair order).
+//
+// One CTA computes one output x-row (128 voxels = the MMA's M) at a time.  The
+// nine input rows (y-1..y+1, z-1..z+1) are staged once in shared memory in the
+// UMMA K-major no-swizzle layout [row][k-chunk][x+1][8 channels] with a one-voxel
+// periodic halo in x, so the 27 taps are 27 descriptors into the same slab:
+// the x shift of a tap is a 16-byte offset of the descriptor's start address.
+// All weights of the layer stay in shared memory for the CTA's lifetime.
+// One elected thread issues the MMAs; tcgen05.commit signals an mbarrier; the
+// accumulator (128 lanes x C_out columns) is read back with tcgen05.ld for the
+// bias + GELU + BF16 epilogue.  Every mbarrier wait is bounded: on timeout the
+// kernel raises an error flag, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "sc_cnn.h"
+
+namespace sc {
+
+namespace {
+
+constexpr int kN = 128;        // grid size handled (one x-row = one MMA tile)
+constexpr int kRowPlane = (kN + 2) * 16;  // bytes of one k-chunk plane of one staged row
+constexpr long long kSpinLimit = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // UMMA shared-memory descriptor, K-major, no swizzle (layout type 0), version 1
+  uint64_t d = 0;
+  d |= uint64_t((saddr >> 4) & 0x3FFF);
+  d |= uint64_t((lbo >> 4) & 0x3FFF) << 16;
+  d |= uint64_t((sbo >> 4) & 0x3FFF) << 32;
+  d |= uint64_t(1) << 46;
+  return d;
+}
+
+template <int NOUT>
+__host__ __device__ constexpr uint32_t make_idesc() {
+  // kind::f16: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16 (10-12 = 1),
+  // both K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 128)
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(NOUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  uint32_t mask[4] = {0, 0, 0, 0};
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(mask[0]), "r"(mask[1]), "r"(mask[2]), "r"(mask[3]));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int NCOL>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float* v);
+
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+
+}  // namespace
+
+// One convolution layer.  act_in: BF16 channels-last [n^3][CP]; weights:
+// BF16 [27][CP/8][COP][8] (UMMA K-major planes per tap); out: BF16 channels-last
+// [n^3][COP] with GELU (LAST = false) or FP32 planar tau[6][n^3] (LAST = true).
+template <int CP, int COP, bool LAST>
+__global__ void __launch_bounds__(256, 1)
+k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restrict__ wgt,
+        const float* __restrict__ bias, __nv_bfloat16* __restrict__ act_out, const TauPtrs tau_out,
+        int* __restrict__ err) {
+  constexpr int CPC = CP / 8;              // 16-byte channel chunks
+  constexpr int PLANE_ROW = CPC * kRowPlane;
+  constexpr int SIN = 9 * PLANE_ROW;
+  constexpr int SW = 27 * CPC * COP * 16;
+  constexpr uint32_t IDESC = make_idesc<COP>();
+  extern __shared__ __align__(128) unsigned char sm[];
+  unsigned char* s_in = sm;
+  unsigned char* s_w = sm + SIN;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + SIN + SW);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SIN + SW + 8);
+  const int tid = threadIdx.x, warp = tid / 32;
+
+  // weights -> shared memory (once)
+  for (int i = tid; i < SW / 16; i += blockDim.x)
+    reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(wgt) + i);
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(32));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool ok = true;
+
+  const int nrows = kN * kN;
+  for (int row = blockIdx.x; row < nrows && ok; row += gridDim.x) {
+    const int y = row % kN, z = row / kN;
+    // stage the 9 neighbouring input rows with the periodic x halo
+    constexpr int CHUNKS = 9 * (kN + 2) * CPC;
+    for (int i = tid; i < CHUNKS; i += blockDim.x) {
+      const int kc = i % CPC;
+      const int xi = (i / CPC) % (kN + 2);
+      const int r = i / (CPC * (kN + 2));
+      const int zz = (z + r / 3 - 1 + kN) % kN, yy = (y + r % 3 - 1 + kN) % kN;
+      const int x = (xi - 1 + kN) % kN;
+      const long long vox = ((long long)zz * kN + yy) * kN + x;
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
+      *reinterpret_cast<uint4*>(s_in + r * PLANE_ROW + kc * kRowPlane + xi * 16) = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = smem_u32(s_in), b0 = smem_u32(s_w);
+      uint32_t acc = 0;
+#pragma unroll 1
+      for (int t = 0; t < 27; ++t) {
+        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+        const int r = (dz + 1) * 3 + (dy + 1);
+#pragma unroll
+        for (int h = 0; h < CPC / 2; ++h) {
+          const uint64_t da = make_desc(a0 + r * PLANE_ROW + 2 * h * kRowPlane + (1 + dx) * 16, kRowPlane, 128);
+          const uint64_t db = make_desc(b0 + (t * CPC + 2 * h) * COP * 16, COP * 16, 128);
+          mma_bf16(tmem, da, db, IDESC, acc);
+          acc = 1;
+        }
+      }
+      mma_commit(bar);
+    }
+    // the decision to continue is collective, so that no thread is left at a barrier
+    ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
+    phase ^= 1;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok) {
+      // warps w and w+4 share TMEM lanes 32(w%4)..+31 and split the columns
+      const int lane_base = 32 * (warp % 4);
+      const int col0 = (warp / 4) * (COP / 2);
+      const int x = lane_base + tid % 32;
+      float v[16];
+      if (COP / 2 == 16) {
+        tmem_ld<16>(tmem + (uint32_t(lane_base) << 16) + col0, v);
+      } else {
+        // COP = 16: warps 0-3 read columns 0-15, warps 4-7 idle (reads are warp-wide)
+        if (warp < 4) tmem_ld<16>(tmem + (uint32_t(lane_base) << 16), v);
+      }
+      const long long vox = (long long)row * kN + x;
+      if (!LAST) {
+        __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16_rn(gelu(v[c] + bias[col0 + c]));
+        uint4* dst = reinterpret_cast<uint4*>(act_out + vox * COP + col0);
+        dst[0] = reinterpret_cast<uint4*>(o)[0];
+        dst[1] = reinterpret_cast<uint4*>(o)[1];
+      } else if (warp < 4) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) tau_out.p[c][vox] = v[c] + bias[c];
+      }
+    } else if (tid == 0) {
+      atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+  }
+  if (!ok) {
+    // a wait ran out: give the MMAs in flight one more bounded wait before
+    // the tensor memory they write is released
+    mbar_wait(bar, phase ^ 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32));
+}
+
+// input channels: u (3 physical FP32 fields) and the constant channel *z -> BF16 [n^3][16]
+__global__ void k_cnn_input(const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
+                            const double* __restrict__ z, __nv_bfloat16* __restrict__ out, long long npts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  __align__(16) __nv_bfloat16 o[16];
+  o[0] = __float2bfloat16_rn(ux[i]);
+  o[1] = __float2bfloat16_rn(uy[i]);
+  o[2] = __float2bfloat16_rn(uz[i]);
+  o[3] = __float2bfloat16_rn(float(*z));
+#pragma unroll
+  for (int c = 4; c < 16; ++c) o[c] = __float2bfloat16_rn(0.f);
+  uint4* dst = reinterpret_cast<uint4*>(out + i * 16);
+  dst[0] = reinterpret_cast<uint4*>(o)[0];
+  dst[1] = reinterpret_cast<uint4*>(o)[1];
+}
+
+// z = (log(Delta^2 sqrt(a2) / nu) - mu) / sigma   (Re_Delta channel, src/nets.jl:311-331 convention)
+__global__ void k_cnn_redelta(const double* a2, double* z, double delta, double nu, double mu, double sigma) {
+  const double re = delta * delta * sqrt(*a2) / nu;
+  *z = (log(re) - mu) / sigma;
+}
+
+template <int CP, int COP, bool LAST> static size_t conv_smem() {
+  return size_t(9) * (CP / 8) * kRowPlane + size_t(27) * (CP / 8) * COP * 16 + 16;
+}
+
+template <int CP, int COP, bool LAST> static void conv_attr() {
+  cudaFuncSetAttribute(k_conv3<CP, COP, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(conv_smem<CP, COP, LAST>()));
+}
+
+bool cnn_supported(int n, int D) { return n == kN && D == 3; }
+
+void cnn_init() {
+  conv_attr<16, 32, false>();
+  conv_attr<32, 32, false>();
+  conv_attr<32, 16, true>();
+}
+
+void launch_cnn_forward(const CnnArgs& a, cudaStream_t st) {
+  const long long npts = (long long)kN * kN * kN;
+  k_cnn_redelta<<<1, 1, 0, st>>>(a.a2, a.z, a.delta, a.nu, a.mu, a.sigma);
+  k_cnn_input<<<unsigned((npts + 255) / 256), 256, 0, st>>>(
+      static_cast<const float*>(a.u[0]), static_cast<const float*>(a.u[1]), static_cast<const float*>(a.u[2]), a.z,
+      a.act0, npts);
+  const int grid = a.nsm > 0 ? a.nsm : 148;
+  const TauPtrs none{};
+  k_conv3<16, 32, false><<<grid, 256, conv_smem<16, 32, false>(), st>>>(a.act0, a.w[0], a.b[0], a.act1, none, a.err);
+  k_conv3<32, 32, false><<<grid, 256, conv_smem<32, 32, false>(), st>>>(a.act1, a.w[1], a.b[1], a.act2, none, a.err);
+  k_conv3<32, 32, false><<<grid, 256, conv_smem<32, 32, false>(), st>>>(a.act2, a.w[2], a.b[2], a.act1, none, a.err);
+  k_conv3<32, 16, true><<<grid, 256, conv_smem<32, 16, true>(), st>>>(a.act1, a.w[3], a.b[3], nullptr, a.tau, a.err);
+}
+
+}  // namespace sc

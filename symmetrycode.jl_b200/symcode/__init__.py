@@ -26,7 +26,7 @@ __all__ = [
     "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
     "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
     "State", "LesBatch", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
-    "create_dynamic_smagorinsky", "create_bardina", "les_", "les_wray3_", "les_rk4_",
+    "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights", "les_", "les_wray3_", "les_rk4_",
 ]
 
 
@@ -320,6 +320,36 @@ def create_dynamic_smagorinsky(delta, g: Grid):
 def create_bardina(s, delta, g: Grid):
     """``create_bardina(s, Δ, g)`` (src/closures.jl:81-115)."""
     return Closure(g, CLOSURE_BARDINA, delta, (s,))
+
+
+def kaiming_cnn_weights(seed, layers=((4, 32), (32, 32), (32, 32), (32, 6))):
+    """Seeded Kaiming-normal weights (std sqrt(2 / fan_in), fan_in = 27 C_in)
+    for the CNN closure, PyTorch conv3d layout (C_out, C_in, 3, 3, 3), zero biases."""
+    import numpy as np
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ws, bs = [], []
+    for cin, cout in layers:
+        ws.append((rng.standard_normal((cout, cin, 3, 3, 3)) * (2.0 / (27 * cin)) ** 0.5).astype(np.float32))
+        bs.append(np.zeros(cout, dtype=np.float32))
+    return ws, bs
+
+
+def create_cnn_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0):
+    """The tensor-core CNN closure (``sc_cnn_closure_create``); FP32, 3D, n = 128."""
+    import numpy as np
+    ws = [np.ascontiguousarray(w, dtype=np.float32) for w in weights]
+    bs = [np.ascontiguousarray(b, dtype=np.float32) for b in biases]
+    FP = ct.POINTER(ct.c_float)
+    wa = (FP * 4)(*[w.ctypes.data_as(FP) for w in ws])
+    ba = (FP * 4)(*[b.ctypes.data_as(FP) for b in bs])
+    cl = Closure.__new__(Closure)
+    cl.g, cl.kind, cl.delta = g, CLOSURE_CNN, float(delta)
+    ptr = ct.c_void_p()
+    with torch.cuda.device(g.device):
+        check(lib().sc_cnn_closure_create(ct.byref(ptr), g.plan, float(delta), float(visc), wa, ba, float(mu),
+                                          float(sigma)))
+    cl._ptr = ptr
+    return cl
 
 
 def _cl(model):

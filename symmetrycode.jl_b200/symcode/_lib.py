@@ -14,7 +14,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libsymcode.so")
 HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "symcode.h")
 
-SC_OK, SC_ERR_INVALID, SC_ERR_SIZE, SC_ERR_CUDA, SC_ERR_OOM, SC_ERR_DIVERGED, SC_ERR_UNSUPPORTED = range(7)
+SC_OK, SC_ERR_INVALID, SC_ERR_SIZE, SC_ERR_CUDA, SC_ERR_OOM, SC_ERR_DIVERGED, SC_ERR_UNSUPPORTED, SC_ERR_TIMEOUT = range(8)
 SC_FLOAT32, SC_FLOAT64 = 0, 1
 
 
@@ -63,6 +63,9 @@ _SIGS = {
     "sc_filter_reynolds": ([_vp, _pp, ct.c_double, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_closure_create": ([ct.POINTER(_vp), _vp, ct.c_int, ct.c_double, ct.POINTER(ct.c_double), ct.c_int], ct.c_int),
     "sc_closure_destroy": ([_vp], ct.c_int),
+    "sc_cnn_closure_create": ([ct.POINTER(_vp), _vp, ct.c_double, ct.c_double, ct.POINTER(ct.POINTER(ct.c_float)),
+                               ct.POINTER(ct.POINTER(ct.c_float)), ct.c_double, ct.c_double], ct.c_int),
+    "sc_closure_status": ([_vp, ct.POINTER(ct.c_int)], ct.c_int),
     "sc_closure_eval": ([_vp, _pp, _pp, _pp, _vp], ct.c_int),
     "sc_les_rhs": ([_vp, _vp, _pp, _pp, ct.c_double, _vp], ct.c_int),
     "sc_les_wray3_step": ([_vp, _vp, _pp, ct.c_double, ct.c_double, _vp], ct.c_int),

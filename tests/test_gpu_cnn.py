@@ -1,0 +1,65 @@
+"""Tensor-core CNN closure (tcgen05, BF16 x BF16 -> FP32) against the FP64
+oracle with BF16 rounding emulated, on sampled output rows of a 128^3 field.
+
+Tolerance: 5e-3 relative L2 -- accumulation order (FP32 on the tensor cores vs
+FP64 in the oracle) occasionally moves a pre-activation across a BF16 rounding
+boundary, a one-ulp (0.4 %) change of that activation.
+"""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+import symcode as S
+from _util import rel_l2, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    n = 128
+    g = S.Grid(3, n, dtype=torch.float32, device="cuda:0")
+    go = O.Grid(3, n)
+    u = O.random_field(go, seed=40, kpeak=4)
+    delta, nu = 4 * go.l / n, 3e-4
+    ws, bs = S.kaiming_cnn_weights(7)
+    bs = [b + 0.05 * np.arange(b.size, dtype=np.float32) for b in bs]  # exercise the bias path
+    cl = S.create_cnn_closure(delta, nu, g, ws, bs, mu=1.0, sigma=2.0)
+    return g, go, u, delta, nu, ws, bs, cl
+
+
+def test_cnn_closure_matches_oracle(setup):
+    g, go, u, delta, nu, ws, bs, cl = setup
+    ut = [to_dev(c, g) for c in u]
+    tau = to_np(cl(ut, None))
+    uphys = np.stack([to_np(S.to_phys_(S.spacescalarfield(g), c, g)) for c in ut], 0)
+    # the closure sees u through twothirds! (k = 0 removed); the field has no mean
+    zval = O.cnn_redelta_channel(u, go, delta, nu, mu=1.0, sigma=2.0)
+    rows = [(0, 0), (17, 5), (64, 127), (101, 63), (127, 90)]
+    ref = O.cnn_rows(uphys, zval, ws, bs, rows)
+    got = np.stack([tau[:, z, y, :] for (y, z) in rows], 1)
+    assert np.isfinite(got).all()
+    assert rel_l2(got, ref) < 5e-3
+    st = torch.zeros(1)
+    import ctypes as ct
+    status = ct.c_int()
+    S.lib().sc_closure_status(cl.ptr, ct.byref(status))
+    assert status.value == 0
+
+
+def test_les_rhs_with_cnn_adds_divergence_of_tau(setup):
+    g, go, u, delta, nu, ws, bs, cl = setup
+    ut = [to_dev(c, g) for c in u]
+    du_c = S.vectorfield(g)
+    du_0 = S.vectorfield(g)
+    S.les_(du_c, ut, g, cl, nu)
+    S.les_(du_0, ut, g, None, nu)
+    tau = to_np(cl(ut, None))
+    sig = [O.twothirds(O.to_spec(t, go), go) for t in tau]
+    extra = O.tensordivergence(sig, go)
+    diff = [to_np(a) - to_np(b) for a, b in zip(du_c, du_0)]
+    assert rel_l2(diff, [O.twothirds(e, go) for e in extra]) < 1e-4

@@ -1,0 +1,39 @@
+"""The CNN oracle's windowed evaluation equals a full periodic evaluation (CPU)."""
+
+import numpy as np
+
+import oracle as O
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1.0 + 2 ** -9, 1.0 + 3 * 2 ** -9, -2.5, 3.14159])
+    r = O.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -7 and r[3] == -2.5
+    assert abs(r[4] - 3.140625) < 1e-12
+
+
+def test_cnn_rows_window_matches_full_grid():
+    n = 12
+    rng = np.random.default_rng(0)
+    u = rng.standard_normal((3, n, n, n)) * 0.5
+    layers = ((4, 5), (5, 5), (5, 5), (5, 6))
+    ws = [rng.standard_normal((co, ci, 3, 3, 3)) * 0.2 for ci, co in layers]
+    bs = [rng.standard_normal(co) * 0.1 for ci, co in layers]
+    rows = [(3, 7), (0, 0), (11, 5)]
+    got = O.cnn_rows(u, 0.3, ws, bs, rows)
+    # full-grid evaluation with np.roll in every direction
+    act = np.concatenate([O.bf16(u), np.full((1, n, n, n), O.bf16(np.array([0.3]))[0])], 0)
+    for li, (w, b) in enumerate(zip(ws, bs)):
+        wb = O.bf16(w)
+        out = np.zeros((w.shape[0], n, n, n))
+        for kz in range(3):
+            for ky in range(3):
+                for kx in range(3):
+                    sh = np.roll(act, (-(kz - 1), -(ky - 1), -(kx - 1)), axis=(1, 2, 3))
+                    out += np.einsum("oc,czyx->ozyx", wb[:, :, kz, ky, kx], sh)
+        act = out + b[:, None, None, None]
+        if li < 3:
+            from scipy.special import erf
+            act = O.bf16(0.5 * act * (1 + erf(act / np.sqrt(2))))
+    ref = np.stack([act[:, z, y, :] for (y, z) in rows], 1)
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
