@@ -102,6 +102,12 @@ template <typename R> bool launch_x_c2r(int N, const XPlainArgs& a, const void* 
 template <typename R> bool launch_x_r2c(int N, const XPlainArgs& a, const void* tw, cudaStream_t st);
 template <typename R> void launch_epilogue(const EpiArgs& a, cudaStream_t st);
 template <typename R> void launch_filter(const FilterArgs& a, cudaStream_t st);
+// max |u| over the physical points of D rows-of-spectra (x inverse fused with the reduction)
+template <typename R> bool launch_x_vmax(int N, const XPlainArgs& a, const void* tw, unsigned long long* out,
+                                         cudaStream_t st);
+// shells 1..2 on the compact state held in a.dst: mode 0 measures into eref[0..1], mode 1 rescales
+template <typename R> void launch_shell_clamp(const PackArgs& a, double* eref, int mode, cudaStream_t st);
+template <typename R> void launch_spectrum(const PackArgs& a, int nshell, double* s, cudaStream_t st);
 template <typename R> void launch_pack(const PackArgs& a, cudaStream_t st);
 template <typename R> void launch_unpack(const PackArgs& a, cudaStream_t st);
 // forcing coefficient A = eps / (2 E_band) of the compact state u into *A

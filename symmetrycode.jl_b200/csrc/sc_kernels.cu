@@ -622,6 +622,127 @@ __global__ void k_spectral_energy(const PackArgs a, int K1, int K2, int compact,
 }
 
 // ---------------------------------------------------------------------------
+// CFL velocity maximum, shell clamp, spectrum
+// ---------------------------------------------------------------------------
+// max over physical points of |u| from D spectral x-rows (propose_timestep,
+// src/solver.jl:931-947); the rows hold the y/z-inverse transforms of P u.
+// Result as float bits (non-negative floats order like their bit patterns).
+template <typename R, int N>
+__global__ void __launch_bounds__(XPCfg<R, N>::NT)
+k_x_vmax(const XPlainArgs a, const typename V2<R>::T* __restrict__ tw, unsigned long long* out) {
+  using C = typename V2<R>::T;
+  constexpr int TR = XPCfg<R, N>::TR / 2 > 0 ? XPCfg<R, N>::TR / 2 : 1, NT = XPCfg<R, N>::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);  // [2][TR][N]: (u1 + i u2) and (u3 + 0 i) per row
+  const long long row0 = (long long)blockIdx.x * TR;
+  for (int idx = threadIdx.x; idx < TR * N; idx += NT) {
+    const int t = idx / N, f = idx % N;
+    const long long row = row0 + t;
+    C z1 = mk<C>(R(0), R(0)), z2 = mk<C>(R(0), R(0));
+    if (row < a.nrows) {
+      z1 = pack_pair(hext<C, N>(static_cast<const C*>(a.in[0]) + row * a.K1, a.K1, f),
+                     hext<C, N>(static_cast<const C*>(a.in[1]) + row * a.K1, a.K1, f));
+      if (a.ncomp == 3) z2 = hext<C, N>(static_cast<const C*>(a.in[2]) + row * a.K1, a.K1, f);
+    }
+    s[t * N + f] = z1;
+    s[(TR + t) * N + f] = z2;
+  }
+  __syncthreads();
+  tile_fft<C, N, 2 * TR, NT, true, false>(s, tw);
+  double m = 0;
+  for (int idx = threadIdx.x; idx < TR * N; idx += NT) {
+    const int t = idx / N;
+    if (row0 + t >= a.nrows) continue;
+    const C z1 = s[idx], z2 = s[TR * N + idx];
+    const double v = sqrt(double(z1.x) * z1.x + double(z1.y) * z1.y + double(z2.x) * z2.x);
+    m = v > m ? v : m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double q = __shfl_down_sync(0xffffffffu, m, o);
+    m = q > m ? q : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// maintain_shell_energy! (src/solver.jl:1135-1152) for shells 1..2 on the
+// compact state in one block: energies of 1 <= |k|^2 < 4 and 4 <= |k|^2 < 9
+// (RFFT double count), then u *= sqrt(eref / e) on each shell.  mode 0 only
+// measures (eref output), mode 1 rescales to eref.
+template <typename R>
+__global__ void k_shell_clamp(const PackArgs a, double* eref, int mode) {
+  using C = typename V2<R>::T;
+  __shared__ double e1s[32], e2s[32];
+  const int K1 = a.kc + 1, K2 = 2 * a.kc + 1;
+  double e1 = 0, e2 = 0;
+  const int t = threadIdx.x;  // 3 * 5 * 5 candidates
+  long long idx = -1;
+  int shell = 0;
+  if (t < 75) {
+    const int ix = t % 3, iy = (t / 3) % 5 - 2, iz = t / 15 - 2;
+    const int k2 = ix * ix + iy * iy + (a.D == 3 ? iz * iz : 0);
+    const bool ok = ix <= a.kc && iy <= a.kc && -iy <= a.kc && (a.D == 2 ? iz == 0 : (iz <= a.kc && -iz <= a.kc));
+    if (ok && k2 >= 1 && k2 < 9) {
+      const int py = iy >= 0 ? iy : iy + K2, pz = iz >= 0 ? iz : iz + K2;
+      idx = ix + (long long)K1 * (py + (long long)K2 * (a.D == 3 ? pz : 0));
+      shell = k2 < 4 ? 1 : 2;
+      const double w = ix > 0 ? 2.0 : 1.0;
+      double e = 0;
+      for (int c = 0; c < a.D; ++c) {
+        const C v = static_cast<const C*>(a.dst[c])[idx];
+        e += w * (double(v.x) * v.x + double(v.y) * v.y);
+      }
+      if (shell == 1) e1 = 0.5 * e; else e2 = 0.5 * e;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    e1 += __shfl_down_sync(0xffffffffu, e1, o);
+    e2 += __shfl_down_sync(0xffffffffu, e2, o);
+  }
+  if ((t & 31) == 0) { e1s[t / 32] = e1; e2s[t / 32] = e2; }
+  __syncthreads();
+  double E1 = 0, E2 = 0;
+  for (int w = 0; w < int(blockDim.x / 32); ++w) { E1 += e1s[w]; E2 += e2s[w]; }
+  if (mode == 0) {
+    if (t == 0) { eref[0] = E1; eref[1] = E2; }
+    return;
+  }
+  if (idx >= 0) {
+    const double es = shell == 1 ? E1 : E2, er = shell == 1 ? eref[0] : eref[1];
+    const R f = R(sqrt(er / es));
+    for (int c = 0; c < a.D; ++c) {
+      C* p = static_cast<C*>(a.dst[c]) + idx;
+      *p = mk<C>(p->x * f, p->y * f);
+    }
+  }
+}
+
+// spectrum (src/solver.jl:693-699): s[i-1] += 1/2 sum over modes with i <= |k| < i+1 (RFFT double count)
+template <typename R>
+__global__ void k_spectrum(const PackArgs a, int nshell, double* s) {
+  using C = typename V2<R>::T;
+  const int K1 = a.kc + 1, K2 = 2 * a.kc + 1;
+  const long long nm = (long long)K1 * K2 * (a.D == 3 ? K2 : 1);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = int(i % K1);
+    const long long r = i / K1;
+    const int py = int(r % K2), pz = a.D == 3 ? int(r / K2) : 0;
+    const int iy = py <= a.kc ? py : py - K2, iz = pz <= a.kc ? pz : pz - K2;
+    const long long k2 = (long long)ix * ix + (long long)iy * iy + (long long)iz * iz;
+    int sh = int(sqrt(double(k2)));
+    while ((long long)(sh + 1) * (sh + 1) <= k2) ++sh;
+    while ((long long)sh * sh > k2) --sh;
+    if (sh < 1 || sh > nshell) continue;
+    double e = 0;
+    for (int c = 0; c < a.D; ++c) {
+      const C v = static_cast<const C*>(a.src[c])[i];
+      e += double(v.x) * v.x + double(v.y) * v.y;
+    }
+    atomicAdd(&s[sh - 1], 0.5 * (ix > 0 ? 2.0 : 1.0) * e);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
 #define SC_SIZES(X) \
@@ -760,6 +881,43 @@ template <typename R> bool launch_x_r2c(int N, const XPlainArgs& a, const void* 
   }
 }
 
+template <typename R, int N> static bool xvmax_n(const XPlainArgs& a, const void* tw, unsigned long long* out,
+                                                 cudaStream_t st) {
+  using C = typename V2<R>::T;
+  using Cfg = XPCfg<R, N>;
+  constexpr int TR = Cfg::TR / 2 > 0 ? Cfg::TR / 2 : 1;
+  const size_t smem = size_t(2) * TR * N * sizeof(C);
+  static bool init = false;
+  if (!init) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_x_vmax<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    init = true;
+  }
+  const unsigned nb = unsigned((a.nrows + TR - 1) / TR);
+  k_x_vmax<R, N><<<nb, Cfg::NT, smem, st>>>(a, static_cast<const C*>(tw), out);
+  return true;
+}
+
+template <typename R> bool launch_x_vmax(int N, const XPlainArgs& a, const void* tw, unsigned long long* out,
+                                         cudaStream_t st) {
+  switch (N) {
+#define SC_CASE(NN) case NN: return xvmax_n<R, NN>(a, tw, out, st);
+    SC_SIZES(SC_CASE)
+#undef SC_CASE
+    default: return false;
+  }
+}
+
+template <typename R> void launch_shell_clamp(const PackArgs& a, double* eref, int mode, cudaStream_t st) {
+  k_shell_clamp<R><<<1, 96, 0, st>>>(a, eref, mode);
+}
+
+template <typename R> void launch_spectrum(const PackArgs& a, int nshell, double* s, cudaStream_t st) {
+  const long long nm = (long long)(a.kc + 1) * (2 * a.kc + 1) * (a.D == 3 ? (2 * a.kc + 1) : 1);
+  long long nb = (nm + 255) / 256;
+  if (nb > 148 * 8) nb = 148 * 8;
+  k_spectrum<R><<<unsigned(nb), 256, 0, st>>>(a, nshell, s);
+}
+
 template <typename R> void launch_epilogue(const EpiArgs& a, cudaStream_t st) {
   const long long nm = (long long)a.K1 * a.K2 * (a.D == 3 ? a.K2 : 1);
   const unsigned nb = unsigned((nm + 255) / 256);
@@ -882,7 +1040,10 @@ template <typename R> void launch_project_full(const PackArgs& a, double kfac, c
                                        cudaStream_t);                                                   \
   template void launch_spectral_energy<R>(const void* const*, int, int, int, int, int, int, int, double, \
                                           int, double*, cudaStream_t, int);                               \
-  template void launch_filter<R>(const FilterArgs&, cudaStream_t);
+  template void launch_filter<R>(const FilterArgs&, cudaStream_t);                                   \
+  template bool launch_x_vmax<R>(int, const XPlainArgs&, const void*, unsigned long long*, cudaStream_t); \
+  template void launch_shell_clamp<R>(const PackArgs&, double*, int, cudaStream_t);                   \
+  template void launch_spectrum<R>(const PackArgs&, int, double*, cudaStream_t);
 SC_INST(float)
 SC_INST(double)
 
