@@ -248,12 +248,19 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
     del u_dns
     gd.close()
 
+    cnn_w, cnn_b = S.kaiming_cnn_weights(LES_SEED)
+
     def make(dtype):
         insts, keep = [], []
         for nu, dh, kind in specs:
             g = S.Grid(3, LES_N, dtype=dtype, device=dev)
             delta = dh * g.l / LES_N
-            cl = S.create_dynamic_smagorinsky(delta, g) if kind == 0 else S.create_clark(delta, g)
+            if kind == 0:
+                cl = S.create_dynamic_smagorinsky(delta, g)
+            elif dtype == torch.float32:
+                cl = S.create_cnn_closure(delta, nu, g, cnn_w, cnn_b, mu=5.0, sigma=2.0)
+            else:  # the CNN runs on the FP32 tensor-core path only; the FP64 plain path uses Clark
+                cl = S.create_clark(delta, g)
             S.State(g).load([c.to(g.cdtype) for c in fields[dh]])
             insts.append(dict(grid=g, closure=cl, visc=nu, dt=LES_DT, eps=None))
             keep.append((g, cl))
@@ -294,8 +301,10 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
         "value": 1e3 / ms_batch, "unit": "steps/s", "ms_per_step": ms_batch,
         "plain_fp64_per_instance_steps_per_s": 1e3 / ms_plain,
         "speedup_vs_plain": ms_plain / ms_batch,
-        "closures": "6 dynamic Smagorinsky + 6 Clark (CNN closure not built in this build)",
-        "instances": [{"nu": nu, "delta_over_h": dh, "closure": "dynsmag" if k == 0 else "clark"} for nu, dh, k in specs],
+        "closures": "6 dynamic Smagorinsky (FP64 Lilly averages) + 6 CNN (4 layers 3x3x3, 32 channels, GELU, "
+                    "seeded Kaiming BF16 weights, tcgen05 BF16 MMA / FP32 accumulate); the FP64 plain path runs "
+                    "Clark in place of the CNN (no FP64 tensor-core CNN)",
+        "instances": [{"nu": nu, "delta_over_h": dh, "closure": "dynsmag" if k == 0 else "cnn"} for nu, dh, k in specs],
         "diverged": [i for i, s_ in enumerate(status) if s_ != 0],
         "config": f"FP32, RK4 dt={LES_DT}, unforced, initial fields sfs! of a seeded 256^3 field (k_p=4, seed {LES_SEED}); "
                   "plain path: the same instances in FP64, one after another, eager launches",

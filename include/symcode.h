@@ -249,6 +249,21 @@ SC_API int sc_filter_sfs(sc_plan* dns, sc_plan* les, const void* const* u_hat, c
 SC_API int sc_filter_reynolds(sc_plan* les, const void* const* ubar_hat, double visc, double delta, double* re,
                               void* stream);
 
+/* ---- CFL step, forcing by shell clamp, spectrum ------------------------------- */
+/* propose_timestep(u, grid, visc, cache) (src/solver.jl:931-947):
+ * min(h / max|P u|, h^2 / (2 D visc)); the caller multiplies by cfl.  Synchronous. */
+SC_API int sc_propose_timestep(sc_plan* plan, const void* const* u_hat, double visc, double* dt, void* stream);
+/* energy_shells(grid, [1, 2], u) (src/solver.jl:1135-1140): the reference
+ * energies of shells 1 <= |k| < 2 and 2 <= |k| < 3 (eref[0..1]).  Synchronous. */
+SC_API int sc_shell_energies(sc_plan* plan, const void* const* u_hat, double* eref, void* stream);
+/* maintain_shell_energy!(u, shells) (src/solver.jl:1146-1152): rescale those
+ * shells of u_hat (retained modes) to eref.  Synchronous. */
+SC_API int sc_maintain_shell_energy(sc_plan* plan, void* const* u_hat, const double* eref, void* stream);
+SC_API int sc_state_maintain_shell_energy(sc_plan* plan, const double* eref, void* stream);
+/* spectrum(u, grid) (src/solver.jl:693-699) on shells 1..nshell (nshell <= n/3):
+ * s[i-1] = 1/2 sum_{i <= |k| < i+1} |u_hat|^2 with the RFFT double count.  Synchronous. */
+SC_API int sc_spectrum(sc_plan* plan, const void* const* u_hat, int nshell, double* s, void* stream);
+
 /* ---- diagnostics (FP64 on the device; synchronous, result to host) ------- */
 /* energy(u) (src/solver.jl:643-646): 1/2 sum_i getenergy(u_i). */
 SC_API int sc_energy(sc_plan* plan, const void* const* u_hat, double* energy, void* stream);

@@ -31,7 +31,7 @@ __all__ = [
     "maintain_shell_energy", "peak_profile", "random_field", "random_field_compact",
     "retained_shape", "pack_retained", "unpack_retained", "vectorgradient",
     "strainrate", "make_tracefree", "turbulence_statistics", "taylorgreen",
-    "pairs", "rel_l2", "SYM_PAIRS_3D", "SYM_PAIRS_2D",
+    "pairs", "rel_l2", "SYM_PAIRS_3D", "SYM_PAIRS_2D", "spectrum",
 ]
 
 WORKERS = int(os.environ.get("SC_ORACLE_WORKERS", os.cpu_count() or 1))
@@ -381,6 +381,22 @@ def maintain_shell_energy(u, shells):
         for c in u:
             c[inds] *= f
     return u
+
+
+def spectrum(u, g: Grid, nshell=None):
+    """``spectrum`` with ``spectral_stuff`` shells 1..n÷3 (src/solver.jl:664-699):
+    s_i = ½ Σ_{i <= |k| < i+1} |û|² over the RFFT array plus the conjugate interior."""
+    nshell = nshell or g.n // 3
+    k2 = k2_int(g)
+    K = g.n // 2 + 1
+    w = np.ones(g.spec_shape)
+    w[..., 1:K - 1] = 2.0
+    e = sum(np.abs(c) ** 2 for c in u) * w / 2
+    out = []
+    for i in range(1, nshell + 1):
+        m = (k2 >= i * i) & (k2 < (i + 1) * (i + 1))
+        out.append(float(e[m].sum()))
+    return out
 
 
 # --------------------------------------------------------------------------

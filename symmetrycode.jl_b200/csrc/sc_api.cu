@@ -1304,6 +1304,146 @@ int sc_les_wray3_step(sc_plan* p, sc_closure* cl, void* const* u, double dt, dou
   return sc_state_store(p, u, stream);
 }
 
+}  // extern "C"
+
+namespace {
+template <typename R>
+int vmax_impl(sc_plan* p, void* const* uc, double* vmax, cudaStream_t st) {
+  // y/z inverse of the D components (zero-padded, k = 0 masked) into the pencil scratch
+  const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc, D = p->D;
+  if (D == 3) {
+    sc::ColArgs a{};
+    for (int c = 0; c < 3; ++c) { a.in[c] = uc[c]; a.out[c] = p->be[c]; }
+    a.ncomp = 3; a.K1 = K1; a.ncols = K2;
+    a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
+    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    sc::launch_col_inv<R>(n, a, p->tw, st);
+    sc::ColArgs b{};
+    for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
+    b.ncomp = 3; b.K1 = K1; b.ncols = n;
+    b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
+    b.kpos = kc + 1; b.kneg = kc;
+    sc::launch_col_inv<R>(n, b, p->tw, st);
+  } else {
+    sc::ColArgs a{};
+    for (int c = 0; c < 2; ++c) { a.in[c] = uc[c]; a.out[c] = p->cc[c]; }
+    a.ncomp = 2; a.K1 = K1; a.ncols = 1;
+    a.in_cs = 0; a.in_es = K1; a.out_cs = 0; a.out_es = K1;
+    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    sc::launch_col_inv<R>(n, a, p->tw, st);
+  }
+  SC_CU(cudaMemsetAsync(p->dscal + 2, 0, sizeof(double), st));
+  sc::XPlainArgs x{};
+  for (int c = 0; c < D; ++c) x.in[c] = p->cc[c];
+  x.ncomp = D; x.K1 = K1; x.nrows = D == 3 ? (long long)n * n : n;
+  sc::launch_x_vmax<R>(n, x, p->tw, reinterpret_cast<unsigned long long*>(p->dscal + 2), st);
+  int rc = check_launch("vmax");
+  if (rc) return rc;
+  double h = 0;
+  SC_CU(cudaMemcpyAsync(&h, p->dscal + 2, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SC_CU(cudaStreamSynchronize(st));
+  *vmax = h;
+  return SC_OK;
+}
+
+template <typename R>
+int clamp_impl(sc_plan* p, void* const* uc, double* eref_host, int mode, cudaStream_t st) {
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) a.dst[c] = uc[c];
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  if (mode == 1) SC_CU(cudaMemcpyAsync(p->dscal + 4, eref_host, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+  sc::launch_shell_clamp<R>(a, p->dscal + 4, mode, st);
+  int rc = check_launch("shell clamp");
+  if (rc) return rc;
+  if (mode == 0) {
+    SC_CU(cudaMemcpyAsync(eref_host, p->dscal + 4, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SC_CU(cudaStreamSynchronize(st));
+  }
+  return SC_OK;
+}
+
+template <typename R>
+int spectrum_impl(sc_plan* p, void* const* uc, int nshell, double* out, cudaStream_t st) {
+  double* d = nullptr;
+  SC_CU(cudaMallocAsync((void**)&d, nshell * sizeof(double), st));
+  cudaMemsetAsync(d, 0, nshell * sizeof(double), st);
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) a.src[c] = uc[c];
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  sc::launch_spectrum<R>(a, nshell, d, st);
+  int rc = check_launch("spectrum");
+  cudaMemcpyAsync(out, d, nshell * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  SC_CU(cudaStreamSynchronize(st));
+  return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int sc_propose_timestep(sc_plan* p, const void* const* u, double visc, double* dt, void* stream) {
+  if (!p || !dt || !(visc > 0)) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  double vmax = 0;
+  rc = SC_DTYPE_DISPATCH(p, pack_state, p, u, p->S, st);
+  if (!rc) rc = SC_DTYPE_DISPATCH(p, vmax_impl, p, p->S, &vmax, st);
+  if (rc) return rc;
+  const double h = p->l / p->n;
+  const double dconv = h / vmax, ddiff = h * h / p->D / 2 / visc;
+  *dt = dconv < ddiff ? dconv : ddiff;
+  return SC_OK;
+}
+
+int sc_shell_energies(sc_plan* p, const void* const* u, double* eref, void* stream) {
+  if (!p || !eref) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  rc = SC_DTYPE_DISPATCH(p, pack_state, p, u, p->S, st);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, clamp_impl, p, p->S, eref, 0, st);
+}
+
+int sc_maintain_shell_energy(sc_plan* p, void* const* u, const double* eref, void* stream) {
+  if (!p || !eref) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = check_ptrs((const void* const*)u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  double e[2] = {eref[0], eref[1]};
+  rc = SC_DTYPE_DISPATCH(p, pack_state, p, (const void* const*)u, p->S, st);
+  if (!rc) rc = SC_DTYPE_DISPATCH(p, clamp_impl, p, p->S, e, 1, st);
+  if (!rc) rc = SC_DTYPE_DISPATCH(p, unpack_state, p, p->S, u, st);
+  if (!rc) SC_CU(cudaStreamSynchronize(st));
+  return rc;
+}
+
+int sc_state_maintain_shell_energy(sc_plan* p, const double* eref, void* stream) {
+  if (!p || !eref) return fail(SC_ERR_INVALID, "bad argument");
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  double e[2] = {eref[0], eref[1]};
+  rc = SC_DTYPE_DISPATCH(p, clamp_impl, p, p->U, e, 1, as_stream(stream));
+  if (!rc) SC_CU(cudaStreamSynchronize(as_stream(stream)));
+  return rc;
+}
+
+int sc_spectrum(sc_plan* p, const void* const* u, int nshell, double* s, void* stream) {
+  if (!p || !s || nshell < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (nshell > p->kc) return fail(SC_ERR_INVALID, "shells beyond n/3 are not retained (nshell <= %d)", p->kc);
+  int rc = check_ptrs(u, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  rc = SC_DTYPE_DISPATCH(p, pack_state, p, u, p->S, st);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, spectrum_impl, p, p->S, nshell, s, st);
+}
+
 int sc_plan_set_option(sc_plan* p, int option, long long value) {
   if (!p) return fail(SC_ERR_INVALID, "null plan");
   if (option == SC_OPT_USE_GRAPH) { p->use_graph = value ? 1 : 0; return SC_OK; }

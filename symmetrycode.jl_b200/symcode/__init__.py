@@ -25,7 +25,8 @@ __all__ = [
     "Grid", "SymcodeError", "scalarfield", "vectorfield", "tensorfield", "spacescalarfield",
     "spacevectorfield", "to_phys_", "to_spec_", "twothirds_", "project_", "convectiondiffusion_",
     "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
-    "State", "LesBatch", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
+    "State", "LesBatch", "propose_timestep", "energy_shells", "maintain_shell_energy_", "spectrum",
+    "turbulence_statistics", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
     "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights", "les_", "les_wray3_", "les_rk4_",
 ]
 
@@ -423,6 +424,52 @@ class LesBatch:
 def set_option(g: Grid, option, value):
     """``sc_plan_set_option`` (1 = use CUDA graphs for the steppers)."""
     check(lib().sc_plan_set_option(g.plan, int(option), int(value)))
+
+
+def propose_timestep(u, g: Grid, visc, stream=None):
+    """``propose_timestep(u, grid, visc, cache)`` (src/solver.jl:931-947)."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    out = ct.c_double()
+    check(lib().sc_propose_timestep(g.plan, pu, float(visc), ct.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+def energy_shells(g: Grid, u, stream=None):
+    """``energy_shells(grid, [1, 2], u)`` (src/solver.jl:1135-1140): reference shell energies."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    e = (ct.c_double * 2)()
+    check(lib().sc_shell_energies(g.plan, pu, e, _stream_ptr(stream)))
+    return [e[0], e[1]]
+
+
+def maintain_shell_energy_(u, eref, g: Grid, stream=None):
+    """``maintain_shell_energy!(u, shells)`` (src/solver.jl:1146-1152) for shells 1 and 2."""
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    e = (ct.c_double * 2)(*eref)
+    check(lib().sc_maintain_shell_energy(g.plan, pu, e, _stream_ptr(stream)))
+    return u
+
+
+def spectrum(u, g: Grid, nshell=None, stream=None):
+    """``spectrum(u, grid)`` (src/solver.jl:693-699) on shells 1..nshell (default n÷3)."""
+    nshell = nshell or g.n // 3
+    pu, _k = ptr_array([g._check_spec(c) for c in u])
+    s = (ct.c_double * nshell)()
+    check(lib().sc_spectrum(g.plan, pu, int(nshell), s, _stream_ptr(stream)))
+    return list(s)
+
+
+def turbulence_statistics(u, visc, g: Grid):
+    """``turbulence_statistics`` (src/solver.jl:836-852) from the device FP64 reductions."""
+    e = energy(u, g)
+    diss = get_dissipation(u, visc, g)
+    uavg = math.sqrt(2 * e / g.D)
+    l_kol = (visc ** 3 / diss) ** 0.25
+    l_tay = math.sqrt(15 * visc / diss) * uavg
+    l_int = uavg ** 3 / diss
+    return dict(e=e, uavg=uavg, diss=diss, l_int=l_int, l_tay=l_tay, l_kol=l_kol, t_int=l_int / uavg,
+                t_tay=l_tay / uavg, t_kol=math.sqrt(visc / diss), Re_int=l_int * uavg / visc,
+                Re_tay=l_tay * uavg / visc, kmax_eta=(math.pi * g.n / g.l) * l_kol)
 
 
 class State:
