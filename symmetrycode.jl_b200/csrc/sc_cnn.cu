@@ -101,9 +101,17 @@ __device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.f + erff(x
 
 }  // namespace
 
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
 // One convolution layer.  act_in: BF16 channels-last [n^3][CP]; weights:
 // BF16 [27][CP/8][COP][8] (UMMA K-major planes per tap); out: BF16 channels-last
-// [n^3][COP] with GELU (LAST = false) or FP32 planar tau[6][n^3] (LAST = true).
+// [n^3][COP] with GELU (LAST = false) or FP32 planar tau (LAST = true).
+// Each CTA walks a contiguous run of x-rows (y fastest).  Staged input rows
+// live in a ring of 4 y-slots per z-offset (12 rows); moving from y to y+1
+// reuses 6 of the 9 rows, and the 3 rows of y+2 are fetched with cp.async
+// while the MMAs of row y run.
 template <int CP, int COP, bool LAST>
 __global__ void __launch_bounds__(256, 1)
 k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restrict__ wgt,
@@ -111,7 +119,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
         int* __restrict__ err) {
   constexpr int CPC = CP / 8;              // 16-byte channel chunks
   constexpr int PLANE_ROW = CPC * kRowPlane;
-  constexpr int SIN = 9 * PLANE_ROW;
+  constexpr int SIN = 12 * PLANE_ROW;      // [zr][slot] staged rows
   constexpr int SW = 27 * CPC * COP * 16;
   constexpr uint32_t IDESC = make_idesc<COP>();
   extern __shared__ __align__(128) unsigned char sm[];
@@ -121,7 +129,6 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SIN + SW + 8);
   const int tid = threadIdx.x, warp = tid / 32;
 
-  // weights -> shared memory (once)
   for (int i = tid; i < SW / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(wgt) + i);
   if (tid == 0) {
@@ -140,21 +147,37 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   uint32_t phase = 0;
   bool ok = true;
 
-  const int nrows = kN * kN;
-  for (int row = blockIdx.x; row < nrows && ok; row += gridDim.x) {
-    const int y = row % kN, z = row / kN;
-    // stage the 9 neighbouring input rows with the periodic x halo
-    constexpr int CHUNKS = 9 * (kN + 2) * CPC;
-    for (int i = tid; i < CHUNKS; i += blockDim.x) {
+  // copy the x-rows (y + dyv[*]) of the three z-offsets into their ring slots
+  auto stage = [&](int y, int z, int ylo, int yhi) {
+    const int nyr = yhi - ylo + 1;
+    const int chunks = 3 * nyr * (kN + 2) * CPC;
+    for (int i = tid; i < chunks; i += blockDim.x) {
       const int kc = i % CPC;
       const int xi = (i / CPC) % (kN + 2);
-      const int r = i / (CPC * (kN + 2));
-      const int zz = (z + r / 3 - 1 + kN) % kN, yy = (y + r % 3 - 1 + kN) % kN;
+      const int q = i / (CPC * (kN + 2));
+      const int zr = q / nyr, yv = ylo + q % nyr;
+      const int zz = (z + zr - 1 + kN) % kN, yy = (yv + kN) % kN;
       const int x = (xi - 1 + kN) % kN;
       const long long vox = ((long long)zz * kN + yy) * kN + x;
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
-      *reinterpret_cast<uint4*>(s_in + r * PLANE_ROW + kc * kRowPlane + xi * 16) = v;
+      unsigned char* dst = s_in + (zr * 4 + (yv & 3)) * PLANE_ROW + kc * kRowPlane + xi * 16;
+      cp_async16(dst, reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    (void)y;
+  };
+
+  const int nrows = kN * kN;
+  const int per = (nrows + gridDim.x - 1) / gridDim.x;
+  const int rbeg = blockIdx.x * per;
+  const int rend = min(rbeg + per, nrows);
+  int cur_z = -1;
+  for (int row = rbeg; row < rend && ok; ++row) {
+    const int y = row % kN, z = row / kN;
+    if (z != cur_z) {  // (re)start a z-plane: rows y-1, y, y+1
+      stage(y, z, y - 1, y + 1);
+      cur_z = z;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -164,7 +187,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
 #pragma unroll 1
       for (int t = 0; t < 27; ++t) {
         const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-        const int r = (dz + 1) * 3 + (dy + 1);
+        const int r = (dz + 1) * 4 + ((y + dy + kN) & 3);
 #pragma unroll
         for (int h = 0; h < CPC / 2; ++h) {
           const uint64_t da = make_desc(a0 + r * PLANE_ROW + 2 * h * kRowPlane + (1 + dx) * 16, kRowPlane, 128);
@@ -175,6 +198,8 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
       }
       mma_commit(bar);
     }
+    // prefetch row y+2 of the same plane into the slot of y-2 (unused by these MMAs)
+    if (row + 1 < rend && (row + 1) / kN == z) stage(y, z, y + 2, y + 2);
     // the decision to continue is collective, so that no thread is left at a barrier
     ok = __syncthreads_and(mbar_wait(bar, phase)) != 0;
     phase ^= 1;
@@ -209,6 +234,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!ok) {
     // a wait ran out: give the MMAs in flight one more bounded wait before
     // the tensor memory they write is released
@@ -242,7 +268,7 @@ __global__ void k_cnn_redelta(const double* a2, double* z, double delta, double 
 }
 
 template <int CP, int COP, bool LAST> static size_t conv_smem() {
-  return size_t(9) * (CP / 8) * kRowPlane + size_t(27) * (CP / 8) * COP * 16 + 16;
+  return size_t(12) * (CP / 8) * kRowPlane + size_t(27) * (CP / 8) * COP * 16 + 16;
 }
 
 template <int CP, int COP, bool LAST> static void conv_attr() {

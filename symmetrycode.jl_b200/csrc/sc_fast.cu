@@ -424,11 +424,175 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
+// 3D x sweep, rows paired: u3 of rows 2q and 2q+1 share one inverse transform
+// (1.5 inverse transforms per row instead of 2) and the forward side runs in
+// two halves of TR/2 rows so that every phase keeps ~90 % of the threads busy.
+// ---------------------------------------------------------------------------
+template <int N> struct X3Rows;
+template <> struct X3Rows<810> { static constexpr int TR = 4; };
+template <> struct X3Rows<256> { static constexpr int TR = 8; };
+template <> struct X3Rows<128> { static constexpr int TR = 16; };
+template <> struct X3Rows<64> { static constexpr int TR = 32; };
+
+template <int N> struct X3Cfg {
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, N2P = N2 + 1;
+  static constexpr int TR = X3Rows<N>::TR, TH = TR / 2;
+  static constexpr int K1M = N / 3 + 1;
+  static constexpr int NPI = TR + TH;   // inverse pencils: u1 + i u2 per row, u3 pairs
+  static constexpr int NPF = 3 * TH;    // forward pencils of one half
+  static constexpr int NT = 192;
+  static constexpr size_t RIN = size_t(3) * TR * K1M * sizeof(float2);
+  static constexpr size_t ZB = size_t(NPF) * (2 * K1M - 1) * sizeof(float2);
+  static constexpr size_t A0 = RIN > ZB ? RIN : ZB;  // Rin, later Z of each half
+  static constexpr size_t UPH = size_t(3) * TR * N * sizeof(float);
+  static constexpr int NPY = NPI > NPF ? NPI : NPF;
+  static constexpr size_t YB = size_t(NPY) * N1 * N2P * sizeof(float2);
+  static constexpr size_t SMEM = A0 + UPH + YB;
+};
+
+template <int N>
+__global__ void __launch_bounds__(X3Cfg<N>::NT)
+k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
+  using C = float2;
+  using Cfg = X3Cfg<N>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, N2P = Cfg::N2P, TR = Cfg::TR, TH = Cfg::TH, K1M = Cfg::K1M;
+  constexpr int NPI = Cfg::NPI, NPF = Cfg::NPF, NT = Cfg::NT;
+  constexpr int ZS = 2 * K1M - 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* rin = reinterpret_cast<C*>(smem_raw);                         // [3][TR][K1M]
+  C* zb = reinterpret_cast<C*>(smem_raw);                          // [NPF][ZS] after I1
+  float* uph = reinterpret_cast<float*>(smem_raw + Cfg::A0);       // [3][TR][N]
+  C* yb = reinterpret_cast<C*>(smem_raw + Cfg::A0 + Cfg::UPH);     // [NPY][N1][N2P]
+  const long long row0 = (long long)blockIdx.x * TR;
+  const int K1 = a.K1in;
+  const int ko = a.K1out - 1;
+  {
+    constexpr int TOT = 3 * TR * K1M;
+    constexpr int LPT = (TOT + NT - 1) / NT;
+    C v[LPT];
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      v[i] = make_float2(0.f, 0.f);
+      const int cmp = idx / (TR * K1M), r = (idx / K1M) % TR, kx = idx % K1M;
+      if (idx < TOT && kx < K1 && row0 + r < a.nrows)
+        v[i] = __ldg(static_cast<const C*>(a.in[cmp]) + (row0 + r) * K1 + kx);
+    }
+#pragma unroll
+    for (int i = 0; i < LPT; ++i) {
+      const int idx = threadIdx.x + i * NT;
+      if (idx < TOT) rin[idx] = v[i];
+    }
+  }
+  __syncthreads();
+  // I1: pencils p < TR: u1 + i u2 of row p; p >= TR: u3(row 2q) + i u3(row 2q+1), q = p - TR
+  for (int it = threadIdx.x; it < NPI * N2; it += NT) {
+    const int p = it / N2, j = it % N2;
+    const C* ra;
+    const C* rb;
+    if (p < TR) { ra = rin + (0 * TR + p) * K1M; rb = rin + (1 * TR + p) * K1M; }
+    else { const int q = p - TR; ra = rin + (2 * TR + 2 * q) * K1M; rb = rin + (2 * TR + 2 * q + 1) * K1M; }
+    C v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int f = N2 * n1 + j;
+      const C x1 = hext2<N>(ra, K1, f), x2 = hext2<N>(rb, K1, f);
+      v[n1] = make_float2(x1.x - x2.y, x1.y + x2.x);
+    }
+    DFT<N1, true, C>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+      const C w = __ldg(&tw[j * k1]);
+      v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
+    }
+    C* yp = yb + p * N1 * N2P;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+  }
+  __syncthreads();
+  // I2: physical velocities
+  for (int it = threadIdx.x; it < NPI * N1; it += NT) {
+    const int p = it / N1, i = it % N1;
+    C w[N2];
+    const C* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+    DFT<N2, true, C>::run(w);
+    float* oa;
+    float* ob;
+    if (p < TR) { oa = uph + (0 * TR + p) * N; ob = uph + (1 * TR + p) * N; }
+    else { const int q = p - TR; oa = uph + (2 * TR + 2 * q) * N; ob = uph + (2 * TR + 2 * q + 1) * N; }
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) { oa[i + N1 * k2] = w[k2].x; ob[i + N1 * k2] = w[k2].y; }
+  }
+  __syncthreads();
+  const float sc = float(a.scale);
+  const int K1o = a.K1out;
+#pragma unroll 1
+  for (int half = 0; half < 2; ++half) {
+    // F1: products of the half's rows, forward step 1 (pencil p: row half*TH + p % TH, kind p / TH)
+    for (int it = threadIdx.x; it < NPF * N2; it += NT) {
+      const int p = it / N2, j = it % N2;
+      const int r = half * TH + p % TH, kind = p / TH;
+      const float* u1 = uph + (0 * TR + r) * N;
+      const float* u2 = uph + (1 * TR + r) * N;
+      const float* u3 = uph + (2 * TR + r) * N;
+      C v[N1];
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int x = N2 * n1 + j;
+        const float a1 = u1[x], a2 = u2[x], a3 = u3[x];
+        v[n1] = kind == 0 ? make_float2(a1 * a1 * sc, a2 * a2 * sc)
+              : kind == 1 ? make_float2(a3 * a3 * sc, a1 * a2 * sc)
+                          : make_float2(a2 * a3 * sc, a3 * a1 * sc);
+      }
+      DFT<N1, false, C>::run(v);
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(&tw[j * k1]));
+      C* yp = yb + p * N1 * N2P;
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+    }
+    __syncthreads();
+    // F2: forward step 2 into Z (the staged input rows are no longer needed)
+    for (int it = threadIdx.x; it < NPF * N1; it += NT) {
+      const int p = it / N1, i = it % N1;
+      C w[N2];
+      const C* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+      DFT<N2, false, C>::run(w);
+      C* zp = zb + p * ZS;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int k = i + N1 * k2;
+        if (k <= ko) zp[k] = w[k2];
+        else if (k >= N - ko) zp[ko + (N - k)] = w[k2];
+      }
+    }
+    __syncthreads();
+    // S: split and store the half's product rows
+    for (int it = threadIdx.x; it < TH * K1o; it += NT) {
+      const int rr = it / K1o, kx = it % K1o;
+      const long long row = row0 + half * TH + rr;
+      if (row >= a.nrows) continue;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        const C* zp = zb + (b * TH + rr) * ZS;
+        const C z = zp[kx], zc = zp[kx == 0 ? 0 : ko + kx];
+        static_cast<C*>(a.out[2 * b])[row * K1o + kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+        static_cast<C*>(a.out[2 * b + 1])[row * K1o + kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-  cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
@@ -441,6 +605,7 @@ template <int N> static void init_fast_n() {
   set_smem2(k_col2<N, T, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
   set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
+  set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
 }
 
 bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64; }
@@ -504,9 +669,20 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
   }
 }
 
+static bool x3_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("SC_X_KERNEL");
+    return !(e && e[0] == '2');
+  }();
+  return on;
+}
+
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
-  if (a.D == 3) k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  if (a.D == 3 && x3_enabled()) {
+    const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
+    k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  } else if (a.D == 3) k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, static_cast<const float2*>(tw));
   else k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, static_cast<const float2*>(tw));
 }
 

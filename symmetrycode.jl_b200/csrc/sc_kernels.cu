@@ -48,7 +48,6 @@ template <typename R, int N> struct XPCfg {  // plain c2r / r2c: one buffer per 
 
 template <typename F> static void set_smem(F* f, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-  cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
 __device__ __forceinline__ int compact_pos(int f, int N, int kpos, int kneg) {
