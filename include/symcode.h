@@ -164,6 +164,7 @@ SC_API int sc_state_rk4_launches_per_step(const sc_plan* plan, int forced);
 #define SC_CLOSURE_DYNAMIC_SMAGORINSKY 4
 #define SC_CLOSURE_BARDINA 5
 #define SC_CLOSURE_CNN 6
+#define SC_CLOSURE_CNN_FP 7
 typedef struct sc_closure sc_closure;
 SC_API int sc_closure_create(sc_closure** closure, sc_plan* plan, int kind, double delta, const double* params,
                              int nparams);
@@ -178,6 +179,15 @@ SC_API int sc_closure_destroy(sc_closure* closure);
  * here), biases[l]: host FP32 (C_out).  FP32 3D plans with n = 128. */
 SC_API int sc_cnn_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc,
                                  const float* const* weights, const float* const* biases, double mu, double sigma);
+/* The same CNN on CUDA cores in the plan's precision (FP32 or FP64, any 3D
+ * grid), without BF16 rounding: the closure the a-posteriori adjoint
+ * differentiates, and the FP64 per-instance reference of the tensor-core CNN. */
+SC_API int sc_cnn_fp_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc,
+                                    const float* const* weights, const float* const* biases, double mu,
+                                    double sigma);
+/* Flat parameter vector of the FP32/FP64 CNN closure, layer by layer [w (C_out, C_in, 27), b (C_out)]. */
+SC_API int sc_closure_num_params(const sc_closure* closure, long long* nparams);
+SC_API int sc_closure_set_params(sc_closure* closure, const double* theta);
 /* Synchronous: SC_ERR_TIMEOUT if a bounded wait of the closure's kernels ran out. */
 SC_API int sc_closure_status(sc_closure* closure, int* status);
 /* model(u, G): the packed physical stress tau (3|6 fields, pair order) from
@@ -229,6 +239,29 @@ SC_API int sc_les_batch_destroy(sc_les_batch* batch);
 /* ---- plan options ---------------------------------------------------------------- */
 #define SC_OPT_USE_GRAPH 1 /* 1 (default): steppers replay a captured CUDA graph; 0: launch eagerly */
 SC_API int sc_plan_set_option(sc_plan* plan, int option, long long value);
+
+/* ---- a-posteriori training: rollout, loss and hand-written adjoint ----------
+ * New (the reference trains a-priori only, src/training.jl:3-109).  A rollout
+ * is `nsteps` RK4 steps (projected stage derivatives, no forcing) of the LES
+ * with `closure` from u0 (full layout).  A trajectory is `nsteps` compact
+ * states (retained modes, the plan's precision) on the device, size
+ * sc_rollout_traj_bytes.  The loss is the trajectory MSE
+ *   L = 1/nsteps sum_s <u_s - u*_s, u_s - u*_s>,
+ * <a, b> = sum over the half spectrum of w Re(conj a b) (the physical mean of
+ * the product).  sc_rollout_adjoint returns L and dL/dtheta (host, FP64,
+ * sc_closure_num_params entries) by the discrete adjoint of the RK4 steps and
+ * of the LES right-hand side (FFT transposes, product and viscous terms,
+ * projection, the CNN's convolutions and GELUs and its Re_Delta channel),
+ * recomputing the states from checkpoints every `ckpt_every` steps.
+ * All three are synchronous. */
+SC_API size_t sc_rollout_traj_bytes(const sc_plan* plan, int nsteps);
+SC_API int sc_rollout_record(sc_plan* plan, sc_closure* closure, const void* const* u0, double dt, double visc,
+                             int nsteps, void* traj, void* stream);
+SC_API int sc_rollout_loss(sc_plan* plan, sc_closure* closure, const void* const* u0, const void* traj, double dt,
+                           double visc, int nsteps, double* loss, void* stream);
+SC_API int sc_rollout_adjoint(sc_plan* plan, sc_closure* closure, const void* const* u0, const void* traj,
+                              double dt, double visc, int nsteps, int ckpt_every, double* loss, double* grad,
+                              void* stream);
 
 /* ---- DNS -> LES filter ------------------------------------------------------
  * sfs!(; tau, ubar, u, g_dns, g_les, Delta) (src/data.jl:625-642) for `ndelta`

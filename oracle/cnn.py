@@ -52,23 +52,25 @@ def _conv(act, w, b, z_lo, z_hi, y_lo, y_hi):
     return out + b[:, None, None, None]
 
 
-def cnn_rows(uphys, zval, weights, biases, rows):
+def cnn_rows(uphys, zval, weights, biases, rows, round_bf16=True):
     """tau (6, len(rows), n) at the x-rows ``rows`` = [(y, z), ...] of the periodic grid.
 
-    uphys: (3, n, n, n) physical velocity indexed [c, z, y, x].
+    uphys: (3, n, n, n) physical velocity indexed [c, z, y, x].  With
+    ``round_bf16=False`` the network is evaluated in FP64 without rounding.
     """
     n = uphys.shape[-1]
-    ws = [bf16(w) for w in weights]
+    rnd = bf16 if round_bf16 else (lambda x: np.asarray(x, dtype=np.float64))
+    ws = [rnd(w) for w in weights]
     out = []
     for (y0, z0) in rows:
         idx_z = [(z0 + d) % n for d in range(-4, 5)]
         idx_y = [(y0 + d) % n for d in range(-4, 5)]
         win = uphys[:, idx_z][:, :, idx_y]  # (3, 9, 9, n)
-        act = np.concatenate([bf16(win), np.full((1,) + win.shape[1:], bf16(np.array([zval]))[0])], 0)
+        act = np.concatenate([rnd(win), np.full((1,) + win.shape[1:], rnd(np.array([zval]))[0])], 0)
         for li in range(4):
             h = 4 - li  # input window half-width
             act = _conv(act, ws[li], biases[li].astype(np.float64), 1, 2 * h - 1, 1, 2 * h - 1)
             if li < 3:
-                act = bf16(0.5 * act * (1.0 + erf(act / math.sqrt(2.0))))
+                act = rnd(0.5 * act * (1.0 + erf(act / math.sqrt(2.0))))
         out.append(act[:, 0, 0, :])
     return np.stack(out, 1)

@@ -17,6 +17,7 @@
 #include "sc_internal.h"
 #include "sc_les.h"
 #include "sc_cnn.h"
+#include "sc_cnn_cc.h"
 #include "symcode.h"
 
 namespace {
@@ -97,6 +98,15 @@ struct sc_closure {
   void* act[3] = {};  // BF16 activations
   int* err = nullptr;
   double nu = 0, mu = 0, sigma = 1;
+  // CUDA-core CNN (FP32/FP64): weights, activations a0 h1 a1 h2 a2 h3 a3, tau, gradients
+  void* ccw[4] = {};
+  void* ccb[4] = {};
+  void* cca[7] = {};
+  void* cctau = nullptr;   // [6][npts]
+  void* ccg[2] = {};       // [32][npts] gradient ping-pong
+  void* ccg0 = nullptr;    // [4][npts]
+  double* gw = nullptr;    // flat parameter gradient (FP64)
+  long long nparam = 0;
   std::vector<void*> allocs;
 };
 
@@ -318,6 +328,76 @@ sc::LesPhysArgs phys_args(sc_plan* p) {
   return a;
 }
 
+// ---------------------------------------------------------------------------
+// CUDA-core CNN closure (FP32/FP64): forward with stored activations, backward
+// ---------------------------------------------------------------------------
+static const int kCcCin[4] = {4, 32, 32, 32}, kCcCout[4] = {32, 32, 32, 6};
+
+long long cc_layer_offset(int l) {  // offset of layer l in the flat parameter vector [w, b]
+  long long o = 0;
+  for (int i = 0; i < l; ++i) o += (long long)kCcCout[i] * kCcCin[i] * 27 + kCcCout[i];
+  return o;
+}
+
+template <typename R>
+int cc_forward(sc_closure* cl, void* const* u, cudaStream_t st) {
+  sc_plan* p = cl->p;
+  const long long np = phys_args(p).npts;
+  int rc = c2p_batch<R>(p, cl->bb, cl->cb, u, cl->gp, 3, st);  // v = T(u)
+  if (rc) return rc;
+  SC_CU(cudaMemsetAsync(cl->dsum, 0, sizeof(double), st));
+  sc::launch_spectral_energy<R>(u, 3, 3, p->n, p->K1, p->K2, 1, p->kc, 2.0 * M_PI / p->l, 1, cl->dsum, st);
+  sc::launch_redelta(cl->dsum, cl->dsum + 3, cl->delta, cl->nu, cl->mu, cl->sigma, st);
+  R* const* A = reinterpret_cast<R* const*>(cl->cca);
+  sc::launch_cc_input<R>(static_cast<const R*>(cl->gp[0]), static_cast<const R*>(cl->gp[1]),
+                         static_cast<const R*>(cl->gp[2]), cl->dsum + 3, A[0], np, st);
+  const R* inp = A[0];
+  for (int l = 0; l < 4; ++l) {
+    sc::ConvArgs c{};
+    c.in = inp; c.w = cl->ccw[l]; c.b = cl->ccb[l];
+    c.out = l < 3 ? (void*)A[1 + 2 * l] : cl->cctau;
+    c.n = p->n; c.cin = kCcCin[l]; c.cout = kCcCout[l];
+    sc::launch_conv_fwd<R>(c, st);
+    if (l < 3) {
+      sc::launch_gelu<R>(A[1 + 2 * l], A[2 + 2 * l], (long long)kCcCout[l] * np, st);
+      inp = A[2 + 2 * l];
+    }
+  }
+  return check_launch("cnn forward (CUDA cores)");
+}
+
+// Given g_tau (dL/dtau, planar [6][npts]) after cc_forward at the same u:
+// parameter gradients accumulate into cl->gw; dL/dv (3 planar) is left in
+// ccg0[0..2], dL/dz in cl->dsum[1].
+template <typename R>
+int cc_backward(sc_closure* cl, const R* gtau, cudaStream_t st) {
+  sc_plan* p = cl->p;
+  const long long np = phys_args(p).npts;
+  R* const* A = reinterpret_cast<R* const*>(cl->cca);
+  R* g0 = static_cast<R*>(cl->ccg[0]);
+  R* g1 = static_cast<R*>(cl->ccg[1]);
+  const R* gout = gtau;
+  R* gin = g0;
+  for (int l = 3; l >= 0; --l) {
+    sc::ConvArgs c{};
+    c.in = l > 0 ? (const void*)A[2 * l] : (const void*)A[0];
+    c.w = cl->ccw[l];
+    c.out = const_cast<R*>(gout);
+    c.in_grad = l > 0 ? (void*)gin : cl->ccg0;
+    c.n = p->n; c.cin = kCcCin[l]; c.cout = kCcCout[l];
+    const long long off = cc_layer_offset(l);
+    sc::launch_conv_bwd<R>(c, cl->gw + off, cl->gw + off + (long long)kCcCout[l] * kCcCin[l] * 27, st);
+    if (l > 0) {
+      sc::launch_gelu_bwd<R>(A[2 * l - 1], gin, (long long)kCcCin[l] * np, st);  // pre-activation h_l
+      gout = gin;
+      gin = (gin == g0) ? g1 : g0;
+    }
+  }
+  SC_CU(cudaMemsetAsync(cl->dsum + 1, 0, sizeof(double), st));
+  sc::launch_sum<R>(static_cast<const R*>(cl->ccg0) + 3 * np, np, cl->dsum + 1, st);
+  return check_launch("cnn backward (CUDA cores)");
+}
+
 // Closure stress of the compact state u into cl->th (compact), i.e. the
 // spectrum to_spec!(model(u, G)) that les! adds to sigma (src/les.jl:19-27).
 // Bardina and dynamic Smagorinsky read the product spectra F[u_i u_j]/n^D from
@@ -425,6 +505,17 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
     a.nsm = nsm;
     sc::launch_cnn_forward(a, st);
     if ((rc = check_launch("cnn closure"))) return rc;
+  } else if (cl->kind == sc::kCnnFp) {
+    if ((rc = cc_forward<R>(cl, u, st))) return rc;
+    void* tslice[6];
+    for (int c = 0; c < 6; ++c) tslice[c] = static_cast<R*>(cl->cctau) + (size_t)c * phys_args(p).npts;
+    if (tau_phys_out) {
+      for (int c = 0; c < 6; ++c)
+        SC_CU(cudaMemcpyAsync(tau_phys_out[c], tslice[c], (size_t)phys_args(p).npts * sizeof(R),
+                              cudaMemcpyDeviceToDevice, st));
+      return check_launch("closure");
+    }
+    return p2c_batch<R>(p, cl->bb, cl->cb, tslice, cl->th, NP, st);
   } else {
     return fail(SC_ERR_UNSUPPORTED, "closure kind %d has no evaluation in this build", cl->kind);
   }
@@ -1191,6 +1282,77 @@ int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
   return SC_OK;
 }
 
+int sc_cnn_fp_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, const float* const* weights,
+                             const float* const* biases, double mu, double sigma) {
+  if (!out || !p || !weights || !biases) return fail(SC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (p->D != 3) return fail(SC_ERR_UNSUPPORTED, "the CNN closure is 3D");
+  if (!(delta > 0) || !(visc > 0) || !(sigma > 0)) return fail(SC_ERR_INVALID, "delta, visc and sigma must be positive");
+  for (int l = 0; l < 4; ++l)
+    if (!weights[l] || !biases[l]) return fail(SC_ERR_INVALID, "missing weights of layer %d", l);
+  sc_closure* cl = nullptr;
+  int rc = sc_closure_create(&cl, p, sc::kClark, delta, nullptr, 0);
+  if (rc) return rc;
+  cl->kind = sc::kCnnFp;
+  cl->nu = visc; cl->mu = mu; cl->sigma = sigma;
+  const size_t es = p->esz / 2;  // bytes per real
+  const size_t np = (size_t)p->n * p->n * p->n;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  cl->nparam = cc_layer_offset(4);
+  for (int l = 0; l < 4 && !rc; ++l) {
+    const size_t nw = (size_t)kCcCout[l] * kCcCin[l] * 27;
+    rc = A(&cl->ccw[l], nw * es);
+    if (!rc) rc = A(&cl->ccb[l], kCcCout[l] * es);
+  }
+  static const int chans[7] = {4, 32, 32, 32, 32, 32, 32};
+  for (int i = 0; i < 7 && !rc; ++i) rc = A(&cl->cca[i], chans[i] * np * es);
+  if (!rc) rc = A(&cl->cctau, 6 * np * es);
+  for (int i = 0; i < 2 && !rc; ++i) rc = A(&cl->ccg[i], 32 * np * es);
+  if (!rc) rc = A(&cl->ccg0, 4 * np * es);
+  if (!rc) rc = A((void**)&cl->gw, cl->nparam * sizeof(double));
+  if (rc) { sc_closure_destroy(cl); return rc; }
+  std::vector<double> theta(cl->nparam);
+  for (int l = 0; l < 4; ++l) {
+    const long long o = cc_layer_offset(l), nw = (long long)kCcCout[l] * kCcCin[l] * 27;
+    for (long long i = 0; i < nw; ++i) theta[o + i] = weights[l][i];
+    for (int i = 0; i < kCcCout[l]; ++i) theta[o + nw + i] = biases[l][i];
+  }
+  rc = sc_closure_set_params(cl, theta.data());
+  if (rc) { sc_closure_destroy(cl); return rc; }
+  *out = cl;
+  return SC_OK;
+}
+
+int sc_closure_num_params(const sc_closure* cl, long long* n) {
+  if (!cl || !n) return fail(SC_ERR_INVALID, "null argument");
+  *n = cl->kind == sc::kCnnFp ? cl->nparam : 0;
+  return SC_OK;
+}
+
+int sc_closure_set_params(sc_closure* cl, const double* theta) {
+  if (!cl || !theta) return fail(SC_ERR_INVALID, "null argument");
+  if (cl->kind != sc::kCnnFp) return fail(SC_ERR_UNSUPPORTED, "only the FP32/FP64 CNN closure has a parameter vector");
+  const bool f64 = cl->p->dtype == SC_FLOAT64;
+  for (int l = 0; l < 4; ++l) {
+    const long long o = cc_layer_offset(l), nw = (long long)kCcCout[l] * kCcCin[l] * 27, nb_ = kCcCout[l];
+    if (f64) {
+      SC_CU(cudaMemcpy(cl->ccw[l], theta + o, nw * 8, cudaMemcpyHostToDevice));
+      SC_CU(cudaMemcpy(cl->ccb[l], theta + o + nw, nb_ * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> w(theta + o, theta + o + nw), b(theta + o + nw, theta + o + nw + nb_);
+      SC_CU(cudaMemcpy(cl->ccw[l], w.data(), nw * 4, cudaMemcpyHostToDevice));
+      SC_CU(cudaMemcpy(cl->ccb[l], b.data(), nb_ * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  // cached step graphs captured the old weights by pointer, which stay valid
+  return SC_OK;
+}
+
 int sc_closure_status(sc_closure* cl, int* status) {
   if (!cl || !status) return fail(SC_ERR_INVALID, "null argument");
   *status = 0;
@@ -1442,6 +1604,281 @@ int sc_spectrum(sc_plan* p, const void* const* u, int nshell, double* s, void* s
   rc = SC_DTYPE_DISPATCH(p, pack_state, p, u, p->S, st);
   if (rc) return rc;
   return SC_DTYPE_DISPATCH(p, spectrum_impl, p, p->S, nshell, s, st);
+}
+
+size_t sc_rollout_traj_bytes(const sc_plan* p, int nsteps) {
+  if (!p || nsteps < 1) return 0;
+  return (size_t)nsteps * p->D * p->csz * p->esz;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Stage derivative F(u) = P[div(stress(u) + closure)] of the compact state u into k.
+template <typename R>
+int stage_F(sc_plan* p, sc_closure* cl, void* const* u, void* const* k, double visc, cudaStream_t st) {
+  int rc = stage_rhs<R>(p, cl, u, st);
+  if (rc) return rc;
+  sc::EpiArgs e = epi_base<R>(p, u, visc);
+  add_closure_stress<R>(e, cl, p->D);
+  e.proj_k = 1;
+  for (int c = 0; c < p->D; ++c) { e.base_a[c] = nullptr; e.out_a[c] = k[c]; }
+  e.ca = 1.0;
+  sc::launch_epilogue<R>(e, st);
+  return check_launch("stage derivative");
+}
+
+// Adjoint of one stage: mu = (dF/du)^T lam at u; parameter gradients of the
+// closure accumulate into cl->gw.  Scratch: closure buffers (gp, s2, ph2, th).
+template <typename R>
+int stage_adjoint(sc_plan* p, sc_closure* cl, void* const* u, void* const* lam, void* const* mu, double visc,
+                  cudaStream_t st) {
+  const int D = p->D, NP = D == 3 ? 6 : 3;
+  const long long np = phys_args(p).npts;
+  const double N = double(np);
+  void* const* lsig = cl->s2;  // compact [NP]
+  sc::AdjSpecArgs as{};
+  for (int c = 0; c < D; ++c) { as.lam[c] = lam[c]; as.u[c] = u[c]; as.mu[c] = mu[c]; }
+  for (int c = 0; c < NP; ++c) as.lsig[c] = lsig[c];
+  as.D = D; as.kc = p->kc; as.kfac = 2.0 * M_PI / p->l; as.visc = visc;
+  sc::launch_adj_spec<R>(as, st);
+  const bool cnn = cl && cl->kind == sc::kCnnFp;
+  int rc = SC_OK;
+  // physical velocity of the stage (and the CNN activations) at u
+  if (cnn) rc = cc_forward<R>(cl, u, st);  // v in gp[0..2]
+  else rc = c2p_batch<R>(p, cl->bb, cl->cb, u, cl->gp, D, st);
+  if (rc) return rc;
+  // m = T(lsig) / N, physical: into the CNN tau buffer (as dL/dtau) or gp[3..]
+  void* m[6];
+  for (int c = 0; c < NP; ++c)
+    m[c] = cnn ? (void*)(static_cast<R*>(cl->cctau) + (size_t)c * np) : cl->gp[3 + c];
+  {
+    // c2p with the 1/N factor folded into the x-direction c2r
+    const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
+    for (int c0 = 0; c0 < NP; c0 += 12) {
+      const int mc = NP - c0 < 12 ? NP - c0 : 12;
+      sc::ColArgs a{};
+      for (int c = 0; c < mc; ++c) { a.in[c] = lsig[c0 + c]; a.out[c] = cl->bb[c]; }
+      a.ncomp = mc; a.K1 = K1; a.ncols = K2; a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1;
+      a.out_es = (long long)K1 * K2; a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+      sc::launch_col_inv<R>(n, a, p->tw, st);
+      sc::ColArgs b{};
+      for (int c = 0; c < mc; ++c) { b.in[c] = cl->bb[c]; b.out[c] = cl->cb[c]; }
+      b.ncomp = mc; b.K1 = K1; b.ncols = n; b.in_cs = (long long)K1 * K2; b.in_es = K1;
+      b.out_cs = (long long)K1 * n; b.out_es = K1; b.kpos = kc + 1; b.kneg = kc;
+      sc::launch_col_inv<R>(n, b, p->tw, st);
+      sc::XPlainArgs x{};
+      for (int c = 0; c < mc; ++c) { x.in[c] = cl->cb[c]; x.out[c] = m[c0 + c]; }
+      x.ncomp = mc; x.K1 = K1; x.nrows = (long long)n * n; x.scale = 1.0 / N;
+      sc::launch_x_c2r<R>(n, x, p->tw, st);
+    }
+    if ((rc = check_launch("adjoint stress to physical"))) return rc;
+  }
+  if (cnn && (rc = cc_backward<R>(cl, static_cast<const R*>(cl->cctau), st))) return rc;
+  sc::AdjPhysArgs ap{};
+  for (int c = 0; c < D; ++c) {
+    ap.v[c] = cl->gp[c];
+    ap.add[c] = cnn ? (const void*)(static_cast<R*>(cl->ccg0) + (size_t)c * np) : nullptr;
+    ap.lv[c] = cl->ph2[c];
+  }
+  for (int c = 0; c < NP; ++c) ap.m[c] = m[c];
+  ap.D = D; ap.npts = np; ap.inv_npts = 1.0;
+  sc::launch_adj_products<R>(ap, st);
+  if ((rc = p2c_batch<R>(p, cl->bb, cl->cb, cl->ph2, cl->th, D, st))) return rc;
+  sc::AdjAccArgs aa{};
+  for (int c = 0; c < D; ++c) { aa.mu[c] = mu[c]; aa.x[c] = cl->th[c]; aa.u[c] = u[c]; }
+  aa.lamz = cnn ? cl->dsum + 1 : nullptr;
+  aa.a2 = cl->dsum;
+  aa.sigma = cnn ? cl->sigma : 1.0;
+  aa.scale = N; aa.kfac = 2.0 * M_PI / p->l; aa.D = D; aa.kc = p->kc;
+  sc::launch_adj_acc<R>(aa, st);
+  return check_launch("stage adjoint");
+}
+
+struct RolloutBufs {
+  std::vector<void*> all;
+  void* u[4][3];   // stage inputs
+  void* k[3];      // stage derivative scratch
+  void* lam[3], *lk[3], *mu[3];
+  void* ck = nullptr;  // checkpoints
+  void* seg = nullptr; // segment states
+  double* dloss = nullptr;
+};
+
+template <typename R>
+int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* traj, double dt, double visc,
+                 int nsteps, int ck, double* loss, double* grad, void* rec, cudaStream_t st) {
+  const int D = p->D;
+  const size_t cbytes = p->csz * p->esz;  // one compact component
+  const size_t sbytes = D * cbytes;       // one compact state
+  RolloutBufs B{};
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMallocAsync(ptr, bytes, st);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "rollout scratch: %s", cudaGetErrorString(e)); }
+    B.all.push_back(*ptr);
+    return SC_OK;
+  };
+  auto freeall = [&]() { for (void* a : B.all) cudaFreeAsync(a, st); };
+  int rc = SC_OK;
+  const bool adj = grad != nullptr;
+  const int nck = adj ? nsteps / ck + 1 : 0;
+  for (int s_ = 0; s_ < 4 && !rc; ++s_)
+    for (int c = 0; c < D && !rc; ++c) rc = A(&B.u[s_][c], cbytes);
+  for (int c = 0; c < D && !rc; ++c) {
+    rc = A(&B.k[c], cbytes);
+    if (!rc) rc = A(&B.lam[c], cbytes);
+    if (!rc) rc = A(&B.lk[c], cbytes);
+    if (!rc) rc = A(&B.mu[c], cbytes);
+  }
+  if (!rc && adj) rc = A(&B.ck, nck * sbytes);
+  if (!rc && adj) rc = A(&B.seg, (ck + 1) * sbytes);
+  if (!rc) rc = A((void**)&B.dloss, 2 * sizeof(double));  // [loss, scratch]
+  if (rc) { freeall(); return rc; }
+  auto state_ptrs = [&](void* base, long long idx, void** out3) {
+    for (int c = 0; c < D; ++c) out3[c] = static_cast<char*>(base) + (size_t)idx * sbytes + c * cbytes;
+  };
+  auto traj_ptrs = [&](int step, const void** out3) {  // target after `step` steps (1-based)
+    for (int c = 0; c < D; ++c)
+      out3[c] = static_cast<const char*>(traj) + (size_t)(step - 1) * sbytes + c * cbytes;
+  };
+  // one RK4 step of the state in x (in place) using B.u / B.k
+  auto step = [&](void* const* x) -> int {
+    const long long nm = (long long)p->csz;
+    for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[0][c], x[c], cbytes, cudaMemcpyDeviceToDevice, st));
+    static const double cst[3] = {0.5, 0.5, 1.0};
+    static const double w[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+    for (int s_ = 0; s_ < 4; ++s_) {
+      int r = stage_F<R>(p, cl, B.u[s_], B.k, visc, st);
+      if (r) return r;
+      sc::launch_axpby<R>(x, (const void* const*)B.k, w[s_] * dt, 1.0, D, nm, st);  // x += w dt k
+      if (s_ < 3) {
+        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[s_ + 1][c], B.u[0][c], cbytes, cudaMemcpyDeviceToDevice, st));
+        sc::launch_axpby<R>(B.u[s_ + 1], (const void* const*)B.k, cst[s_] * dt, 1.0, D, nm, st);
+      }
+    }
+    return check_launch("rollout step");
+  };
+  // forward rollout: loss, checkpoints / trajectory record
+  void* x[3];
+  state_ptrs(B.seg, 0, x);
+  if ((rc = pack_state<R>(p, u0, x, st))) { freeall(); return rc; }
+  SC_CU(cudaMemsetAsync(B.dloss, 0, sizeof(double), st));
+  if (adj) SC_CU(cudaMemcpyAsync(B.ck, x[0], sbytes, cudaMemcpyDeviceToDevice, st));
+  for (int s_ = 1; s_ <= nsteps && !rc; ++s_) {
+    rc = step(x);
+    if (rc) break;
+    if (rec) SC_CU(cudaMemcpyAsync(static_cast<char*>(rec) + (size_t)(s_ - 1) * sbytes, x[0], sbytes,
+                                   cudaMemcpyDeviceToDevice, st));
+    if (traj) {
+      const void* t3[3];
+      traj_ptrs(s_, t3);
+      sc::launch_mse<R>((const void* const*)x, t3, nullptr, 0.0, D, p->kc, B.dloss, st);
+    }
+    if (adj && s_ % ck == 0)
+      SC_CU(cudaMemcpyAsync(static_cast<char*>(B.ck) + (size_t)(s_ / ck) * sbytes, x[0], sbytes,
+                            cudaMemcpyDeviceToDevice, st));
+  }
+  if (!rc && adj) {
+    SC_CU(cudaMemsetAsync(cl ? (void*)cl->gw : nullptr, 0, cl ? cl->nparam * sizeof(double) : 0, st));
+    sc::launch_axpby<R>(B.lam, nullptr, 0.0, 0.0, D, (long long)p->csz, st);  // lam = 0
+    const double coef = 2.0 / nsteps;
+    for (int seg = (nsteps - 1) / ck; seg >= 0 && !rc; --seg) {
+      const int c0 = seg * ck, c1 = std::min(nsteps, c0 + ck);
+      // recompute u_{c0} .. u_{c1} into the segment buffer
+      SC_CU(cudaMemcpyAsync(B.seg, static_cast<char*>(B.ck) + (size_t)seg * sbytes, sbytes, cudaMemcpyDeviceToDevice, st));
+      for (int s_ = c0 + 1; s_ <= c1 && !rc; ++s_) {
+        void* xs[3];
+        state_ptrs(B.seg, s_ - c0, xs);
+        SC_CU(cudaMemcpyAsync(xs[0], static_cast<char*>(B.seg) + (size_t)(s_ - c0 - 1) * sbytes, sbytes,
+                              cudaMemcpyDeviceToDevice, st));
+        rc = step(xs);
+      }
+      for (int s_ = c1; s_ > c0 && !rc; --s_) {
+        void* us[3];
+        state_ptrs(B.seg, s_ - c0, us);
+        const void* t3[3];
+        traj_ptrs(s_, t3);
+        // lam += dL/du_s = coef (u_s - u*_s)
+        sc::launch_mse<R>((const void* const*)us, t3, B.mu, coef, D, p->kc, B.dloss + 1, st);
+        sc::launch_axpby<R>(B.lam, (const void* const*)B.mu, 1.0, 1.0, D, (long long)p->csz, st);
+        // step adjoint at u_{s-1}: recompute the stage inputs, then transpose stages 4..1
+        void* un[3];
+        state_ptrs(B.seg, s_ - c0 - 1, un);
+        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[0][c], un[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        static const double cst[3] = {0.5, 0.5, 1.0};
+        for (int q = 0; q < 3 && !rc; ++q) {
+          rc = stage_F<R>(p, cl, B.u[q], B.k, visc, st);
+          for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[q + 1][c], B.u[0][c], cbytes, cudaMemcpyDeviceToDevice, st));
+          sc::launch_axpby<R>(B.u[q + 1], (const void* const*)B.k, cst[q] * dt, 1.0, D, (long long)p->csz, st);
+        }
+        // lam_n accumulates in B.lam (identity part already there)
+        static const double wq[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+        // lk = w4 dt lam
+        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.lk[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        sc::launch_axpby<R>(B.lk, nullptr, 0.0, wq[3] * dt, D, (long long)p->csz, st);
+        // keep a copy of lam (dL/du_{n+1}) in B.k for the stage combinations
+        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.k[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        for (int q = 3; q >= 0 && !rc; --q) {
+          rc = stage_adjoint<R>(p, cl, B.u[q], B.lk, B.mu, visc, st);
+          if (rc) break;
+          sc::launch_axpby<R>(B.lam, (const void* const*)B.mu, 1.0, 1.0, D, (long long)p->csz, st);  // lam_n += mu
+          if (q > 0) {
+            // lk_{q-1} = w_{q-1} dt lam_{n+1} + c_{q-1} dt mu
+            for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.lk[c], B.k[c], cbytes, cudaMemcpyDeviceToDevice, st));
+            sc::launch_axpby<R>(B.lk, (const void* const*)B.mu, cst[q - 1] * dt, wq[q - 1] * dt, D,
+                                (long long)p->csz, st);
+          }
+        }
+      }
+    }
+  }
+  double h = 0;
+  if (!rc) {
+    SC_CU(cudaMemcpyAsync(&h, B.dloss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (adj && cl && cl->gw) SC_CU(cudaMemcpyAsync(grad, cl->gw, cl->nparam * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  freeall();
+  SC_CU(cudaStreamSynchronize(st));
+  if (loss) *loss = traj ? h / nsteps : 0.0;
+  return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int sc_rollout_record(sc_plan* p, sc_closure* cl, const void* const* u0, double dt, double visc, int nsteps,
+                      void* traj, void* stream) {
+  if (!p || !traj || nsteps < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  int rc = check_ptrs(u0, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, rollout_impl, p, cl, u0, nullptr, dt, visc, nsteps, 1, nullptr, nullptr, traj,
+                           as_stream(stream));
+}
+
+int sc_rollout_loss(sc_plan* p, sc_closure* cl, const void* const* u0, const void* traj, double dt, double visc,
+                    int nsteps, double* loss, void* stream) {
+  if (!p || !traj || !loss || nsteps < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  int rc = check_ptrs(u0, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, rollout_impl, p, cl, u0, traj, dt, visc, nsteps, 1, loss, nullptr, nullptr,
+                           as_stream(stream));
+}
+
+int sc_rollout_adjoint(sc_plan* p, sc_closure* cl, const void* const* u0, const void* traj, double dt, double visc,
+                       int nsteps, int ckpt_every, double* loss, double* grad, void* stream) {
+  if (!p || !traj || !grad || nsteps < 1 || ckpt_every < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (!cl || cl->p != p || cl->kind != sc::kCnnFp)
+    return fail(SC_ERR_INVALID, "the adjoint needs the FP32/FP64 CNN closure of this plan");
+  int rc = check_ptrs(u0, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  return SC_DTYPE_DISPATCH(p, rollout_impl, p, cl, u0, traj, dt, visc, nsteps, ckpt_every, loss, grad, nullptr,
+                           as_stream(stream));
 }
 
 int sc_plan_set_option(sc_plan* p, int option, long long value) {

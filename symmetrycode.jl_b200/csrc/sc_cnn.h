@@ -27,5 +27,7 @@ struct CnnArgs {
 bool cnn_supported(int n, int D);
 void cnn_init();
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st);
+// *z = (log(delta^2 sqrt(*a2) / nu) - mu) / sigma
+void launch_redelta(const double* a2, double* z, double delta, double nu, double mu, double sigma, cudaStream_t st);
 
 }  // namespace sc

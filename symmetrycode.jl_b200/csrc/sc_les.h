@@ -5,7 +5,8 @@
 namespace sc {
 
 // closure kinds (values match include/symcode.h SC_CLOSURE_*)
-enum { kNoClosure = 0, kClark = 1, kSmagorinsky = 2, kVerstappen = 3, kDynSmagorinsky = 4, kBardina = 5, kCnn = 6 };
+enum { kNoClosure = 0, kClark = 1, kSmagorinsky = 2, kVerstappen = 3, kDynSmagorinsky = 4, kBardina = 5, kCnn = 6,
+       kCnnFp = 7 };
 
 struct LesSpecArgs {
   const void* in[9];

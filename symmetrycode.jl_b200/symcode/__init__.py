@@ -27,7 +27,9 @@ __all__ = [
     "wray3_", "rk4_", "energy", "get_dissipation", "lib", "header_functions", "sfs_", "filter_reynolds",
     "State", "LesBatch", "propose_timestep", "energy_shells", "maintain_shell_energy_", "spectrum",
     "turbulence_statistics", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
-    "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights", "les_", "les_wray3_", "les_rk4_",
+    "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights",
+    "create_cnn_fp_closure", "closure_num_params", "closure_set_params", "pack_cnn_params", "rollout_record",
+    "rollout_loss", "rollout_adjoint", "les_", "les_wray3_", "les_rk4_",
 ]
 
 
@@ -351,6 +353,72 @@ def create_cnn_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0)
                                           float(sigma)))
     cl._ptr = ptr
     return cl
+
+
+def create_cnn_fp_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0):
+    """The CNN closure on CUDA cores in the grid's precision (``sc_cnn_fp_closure_create``)."""
+    import numpy as np
+    ws = [np.ascontiguousarray(w, dtype=np.float32) for w in weights]
+    bs = [np.ascontiguousarray(b, dtype=np.float32) for b in biases]
+    FP = ct.POINTER(ct.c_float)
+    wa = (FP * 4)(*[w.ctypes.data_as(FP) for w in ws])
+    ba = (FP * 4)(*[b.ctypes.data_as(FP) for b in bs])
+    cl = Closure.__new__(Closure)
+    cl.g, cl.kind, cl.delta = g, 7, float(delta)
+    ptr = ct.c_void_p()
+    with torch.cuda.device(g.device):
+        check(lib().sc_cnn_fp_closure_create(ct.byref(ptr), g.plan, float(delta), float(visc), wa, ba, float(mu),
+                                             float(sigma)))
+    cl._ptr = ptr
+    return cl
+
+
+def closure_num_params(cl):
+    n = ct.c_longlong()
+    check(lib().sc_closure_num_params(cl.ptr, ct.byref(n)))
+    return n.value
+
+
+def closure_set_params(cl, theta):
+    import numpy as np
+    th = np.ascontiguousarray(theta, dtype=np.float64)
+    check(lib().sc_closure_set_params(cl.ptr, th.ctypes.data_as(ct.POINTER(ct.c_double))))
+
+
+def pack_cnn_params(weights, biases):
+    """Flat parameter vector [w1, b1, ..., w4, b4] of ``sc_closure_set_params``."""
+    import numpy as np
+    return np.concatenate([np.concatenate([np.ravel(w), np.ravel(b)]) for w, b in zip(weights, biases)]).astype(np.float64)
+
+
+def rollout_record(g: Grid, cl, u0, dt, visc, nsteps, stream=None):
+    """Trajectory of ``nsteps`` RK4 steps (compact states on the device)."""
+    nb = lib().sc_rollout_traj_bytes(g.plan, int(nsteps))
+    traj = torch.empty(nb, dtype=torch.uint8, device=g.device)
+    pu, _k = ptr_array([g._check_spec(c) for c in u0])
+    check(lib().sc_rollout_record(g.plan, _cl(cl), pu, float(dt), float(visc), int(nsteps),
+                                  ct.c_void_p(traj.data_ptr()), _stream_ptr(stream)))
+    return traj
+
+
+def rollout_loss(g: Grid, cl, u0, traj, dt, visc, nsteps, stream=None):
+    pu, _k = ptr_array([g._check_spec(c) for c in u0])
+    out = ct.c_double()
+    check(lib().sc_rollout_loss(g.plan, _cl(cl), pu, ct.c_void_p(traj.data_ptr()), float(dt), float(visc),
+                                int(nsteps), ct.byref(out), _stream_ptr(stream)))
+    return out.value
+
+
+def rollout_adjoint(g: Grid, cl, u0, traj, dt, visc, nsteps, ckpt_every=5, stream=None):
+    """(loss, dloss/dtheta) of the trajectory MSE by the hand-written adjoint."""
+    import numpy as np
+    pu, _k = ptr_array([g._check_spec(c) for c in u0])
+    grad = np.zeros(closure_num_params(cl), dtype=np.float64)
+    out = ct.c_double()
+    check(lib().sc_rollout_adjoint(g.plan, _cl(cl), pu, ct.c_void_p(traj.data_ptr()), float(dt), float(visc),
+                                   int(nsteps), int(ckpt_every), ct.byref(out),
+                                   grad.ctypes.data_as(ct.POINTER(ct.c_double)), _stream_ptr(stream)))
+    return out.value, grad
 
 
 def _cl(model):

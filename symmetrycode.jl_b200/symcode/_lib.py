@@ -66,6 +66,15 @@ _SIGS = {
     "sc_cnn_closure_create": ([ct.POINTER(_vp), _vp, ct.c_double, ct.c_double, ct.POINTER(ct.POINTER(ct.c_float)),
                                ct.POINTER(ct.POINTER(ct.c_float)), ct.c_double, ct.c_double], ct.c_int),
     "sc_closure_status": ([_vp, ct.POINTER(ct.c_int)], ct.c_int),
+    "sc_cnn_fp_closure_create": ([ct.POINTER(_vp), _vp, ct.c_double, ct.c_double, ct.POINTER(ct.POINTER(ct.c_float)),
+                                  ct.POINTER(ct.POINTER(ct.c_float)), ct.c_double, ct.c_double], ct.c_int),
+    "sc_closure_num_params": ([_vp, ct.POINTER(ct.c_longlong)], ct.c_int),
+    "sc_closure_set_params": ([_vp, ct.POINTER(ct.c_double)], ct.c_int),
+    "sc_rollout_traj_bytes": ([_vp, ct.c_int], ct.c_size_t),
+    "sc_rollout_record": ([_vp, _vp, _pp, ct.c_double, ct.c_double, ct.c_int, _vp, _vp], ct.c_int),
+    "sc_rollout_loss": ([_vp, _vp, _pp, _vp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
+    "sc_rollout_adjoint": ([_vp, _vp, _pp, _vp, ct.c_double, ct.c_double, ct.c_int, ct.c_int, ct.POINTER(ct.c_double),
+                            ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_closure_eval": ([_vp, _pp, _pp, _pp, _vp], ct.c_int),
     "sc_les_rhs": ([_vp, _vp, _pp, _pp, ct.c_double, _vp], ct.c_int),
     "sc_les_wray3_step": ([_vp, _vp, _pp, ct.c_double, ct.c_double, _vp], ct.c_int),
