@@ -1732,7 +1732,8 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
     if (!rc) rc = A(&B.mu[c], cbytes);
   }
   if (!rc && adj) rc = A(&B.ck, nck * sbytes);
-  if (!rc && adj) rc = A(&B.seg, (ck + 1) * sbytes);
+  // the working state lives in segment slot 0 in every mode
+  if (!rc) rc = A(&B.seg, (adj ? ck + 1 : 1) * sbytes);
   if (!rc) rc = A((void**)&B.dloss, 2 * sizeof(double));  // [loss, scratch]
   if (rc) { freeall(); return rc; }
   auto state_ptrs = [&](void* base, long long idx, void** out3) {
