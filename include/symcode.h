@@ -303,6 +303,23 @@ SC_API int sc_energy(sc_plan* plan, const void* const* u_hat, double* energy, vo
 /* get_dissipation! (src/solver.jl:808-811): visc sum k^2 |u|^2 (RFFT double count). */
 SC_API int sc_dissipation(sc_plan* plan, const void* const* u_hat, double visc, double* diss, void* stream);
 
+/* ---- allocation-free spectrum (no counterpart in the reference) ----------- */
+/* The spectrum of sc_spectrum (shells 1..nshell, 1 <= nshell <= n/3) read
+ * straight from the full RFFT layout u_hat[c] (n/2+1, n[, n]), with no plan and
+ * no device allocation: the shell sums go to a fixed device array of
+ * SC_SPECTRUM_STATIC_MAX_SHELLS doubles (4 KiB) inside the library, zeroed by
+ * each call; a larger nshell returns SC_ERR_SIZE.  For callers that may not
+ * allocate, such as a monitor between the time steps of a run whose device
+ * memory is taken by the solver: sc_spectrum there would set up a plan's work
+ * buffers and take a stream-ordered shell buffer per call.  The first call on
+ * each device looks up the array's address with that device current; make it
+ * before any stream capture begins.  Calls on one device share the array, so
+ * calls that overlap in time (other streams or host threads) race.
+ * Synchronous on stream. */
+#define SC_SPECTRUM_STATIC_MAX_SHELLS 512
+SC_API int sc_spectrum_static(const void* const* u_hat, int n, int D, int dtype, int nshell, double* s,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,12 @@ int check_launch(const char* what) {
 
 }  // namespace
 
+namespace sc {
+int api_fail(int code, const char* what, const char* detail) {
+  return detail && *detail ? fail(code, "%s: %s", what, detail) : fail(code, "%s", what);
+}
+}  // namespace sc
+
 struct sc_plan {
   int D = 0, n = 0, dtype = 0, dev = 0;
   double l = 0;

@@ -131,4 +131,7 @@ template <typename R> bool init_kernels(int N);
 template <typename R> void launch_twothirds_full(const PackArgs& a, cudaStream_t st);  // in place on a.dst
 template <typename R> void launch_project_full(const PackArgs& a, double kfac, cudaStream_t st);
 
+// Records "what: detail" (or "what") as the thread's last error string and returns code.
+int api_fail(int code, const char* what, const char* detail);
+
 }  // namespace sc

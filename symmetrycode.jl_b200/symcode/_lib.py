@@ -90,6 +90,7 @@ _SIGS = {
     "sc_maintain_shell_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_state_maintain_shell_energy": ([_vp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_spectrum": ([_vp, _pp, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
+    "sc_spectrum_static": ([_pp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
 }
