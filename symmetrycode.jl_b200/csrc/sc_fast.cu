@@ -288,6 +288,10 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
   {
     constexpr int TOT = D * TR * K1M;
     constexpr int LPT = (TOT + NT - 1) / NT;
+    // select the component pointer instead of indexing the parameter array at run time
+    const C* in0 = static_cast<const C*>(a.in[0]);
+    const C* in1 = static_cast<const C*>(a.in[1]);
+    const C* in2 = static_cast<const C*>(a.in[D == 3 ? 2 : 1]);
     C v[LPT];
 #pragma unroll
     for (int i = 0; i < LPT; ++i) {
@@ -295,7 +299,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
       v[i] = make_float2(0.f, 0.f);
       const int cmp = idx / (TR * K1M), r = (idx / K1M) % TR, kx = idx % K1M;
       if (idx < TOT && kx < K1 && row0 + r < a.nrows)
-        v[i] = __ldg(static_cast<const C*>(a.in[cmp]) + (row0 + r) * K1 + kx);
+        v[i] = __ldg((cmp == 0 ? in0 : cmp == 1 ? in1 : in2) + (row0 + r) * K1 + kx);
     }
 #pragma unroll
     for (int i = 0; i < LPT; ++i) {
@@ -469,6 +473,10 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
   {
     constexpr int TOT = 3 * TR * K1M;
     constexpr int LPT = (TOT + NT - 1) / NT;
+    // select the component pointer instead of indexing the parameter array at run time
+    const C* in0 = static_cast<const C*>(a.in[0]);
+    const C* in1 = static_cast<const C*>(a.in[1]);
+    const C* in2 = static_cast<const C*>(a.in[2]);
     C v[LPT];
 #pragma unroll
     for (int i = 0; i < LPT; ++i) {
@@ -476,7 +484,7 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
       v[i] = make_float2(0.f, 0.f);
       const int cmp = idx / (TR * K1M), r = (idx / K1M) % TR, kx = idx % K1M;
       if (idx < TOT && kx < K1 && row0 + r < a.nrows)
-        v[i] = __ldg(static_cast<const C*>(a.in[cmp]) + (row0 + r) * K1 + kx);
+        v[i] = __ldg((cmp == 0 ? in0 : cmp == 1 ? in1 : in2) + (row0 + r) * K1 + kx);
     }
 #pragma unroll
     for (int i = 0; i < LPT; ++i) {
@@ -589,6 +597,292 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
+// 3D x sweep for N = 810 = 9 * 9 * 10, one row pair per 96-thread block.
+//
+// Inverse (c2r of the Hermitian-extended rows, k = 9 m1 + m2):
+//   Ia  thread t = 9 q + m2 (81): radix-10 over p of Z[81 p + t] (straight
+//       from global memory), twiddle exp(+2 pi i q s_a / 90)         -> X
+//   Ib  thread 9 s_a + m2 (90): radix-9 over q, twiddle exp(+2 pi i m2 s1 / 810),
+//       s1 = s_a + 10 s_b                                            -> Y
+//   Ic  thread s1 (90): radix-9 over m2 -> physical x = s1 + 90 s2 in registers.
+// Forward (x = 90 m1 + m2, k = s1' + 9 s_a + 81 s_b):
+//   F1  the same thread (m2 = s1) forms the products at its 9 points and runs
+//       the first radix-9 over m1 in registers, twiddle exp(-2 pi i m2 s1' / 810)
+//                                                                     -> W
+//   F2  thread 10 s1' + q (90): radix-9 over p (m2 = 10 p + q), twiddle
+//       exp(-2 pi i q s_a / 90)                                       -> V
+//   F3  thread 9 s1' + s_a (81): radix-10 over q, retained k only      -> Z
+//   S   split the paired spectra and store the six product rows.
+// Because the last inverse pass leaves every thread holding exactly the points
+// its first forward pass needs, the products never go through shared memory.
+// Pencils: A = u1 + i u2 (row r), A' = u1 + i u2 (row r'), B = u3(r) + i u3(r');
+// forward pencils per row: (u1 u1, u2 u2), (u3 u3, u1 u2), (u2 u3, u3 u1).
+// Shared memory: two regions of three pencil slots; the layouts below keep
+// every exchange free of bank conflicts except the F2 stores (two-way).
+// ---------------------------------------------------------------------------
+struct X4Cfg {
+  static constexpr int N = 810, NT = 96;
+  static constexpr int PS = 882;  // pencil slot (X uses 89 s_a + 9 q + m2 < 882)
+  static constexpr size_t SMEM = size_t(6) * PS * sizeof(float2);
+};
+
+// Z[k] = Ua[k] + i Ub[k], k = 81 p + t, of two real rows given by their staged
+// half spectra (ra, rb: kmax + 1 modes).  FULL: kmax = 270, so the range of k
+// for each p is known and 324 <= k <= 485 (p = 4, 5) never holds a mode.
+template <bool FULL>
+__device__ __forceinline__ float2 x4_gather(const float2* ra, const float2* rb, int p, int t, int kmax) {
+  constexpr int N = 810;
+  const int k = 81 * p + t;
+  bool direct, mirror;
+  if (FULL) {
+    direct = p <= 2 || (p == 3 && t <= 27);
+    mirror = p >= 7 || (p == 6 && t >= 54);
+  } else {
+    direct = k <= kmax;
+    mirror = k >= N - kmax;
+  }
+  if (direct) {
+    float2 x = ra[k], y = rb[k];
+    if (k == 0) { x.y = 0.f; y.y = 0.f; }  // a real row's mean: imaginary part dropped
+    return make_float2(x.x - y.y, x.y + y.x);
+  }
+  if (mirror) {
+    const float2 x = ra[N - k], y = rb[N - k];
+    return make_float2(x.x + y.y, y.x - x.y);
+  }
+  return make_float2(0.f, 0.f);
+}
+
+// products of one row at this thread's 9 points, first forward radix-9, twiddle
+__device__ __forceinline__ void x4_f1_row(const float* u1, const float* u2, const float* u3, float sc,
+                                          const float2* wf, float2* region, int t) {
+  using C = float2;
+#pragma unroll 1
+  for (int kind = 0; kind < 3; ++kind) {
+    C v[9];
+#pragma unroll
+    for (int m1 = 0; m1 < 9; ++m1) {
+      const float a1 = u1[m1], a2 = u2[m1], a3 = u3[m1];
+      const float pa = kind == 0 ? a1 * a1 : kind == 1 ? a3 * a3 : a2 * a3;
+      const float pb = kind == 0 ? a2 * a2 : kind == 1 ? a1 * a2 : a3 * a1;
+      v[m1] = make_float2(pa * sc, pb * sc);
+    }
+    DFT<9, false, C>::run(v);
+    C* ws = region + kind * X4Cfg::PS + t;
+    ws[0] = v[0];
+#pragma unroll
+    for (int s = 1; s < 9; ++s) ws[90 * s] = cmul(v[s], wf[s]);
+  }
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(X4Cfg::NT, 5)
+k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
+  using C = float2;
+  constexpr int N = 810, PS = X4Cfg::PS;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sm = reinterpret_cast<C*>(smem_raw);
+  C* reg0 = sm;           // slots 0..2
+  C* reg1 = sm + 3 * PS;  // slots 3..5
+  const int t = threadIdx.x;
+  const long long r0 = (long long)blockIdx.x * 2;
+  const bool has1 = r0 + 1 < a.nrows;
+  const int K1 = FULL ? 271 : a.K1in, kmax = K1 - 1;
+  const int K1o = FULL ? 271 : a.K1out, ko = K1o - 1;
+
+  // L: stage the six input rows (u1, u2, u3 of rows r, r') in region 1 with one
+  // round of asynchronous copies; region 1 is not written before Ib.
+  C* rin = reg1;  // [3][2][K1]
+  {
+    const C* in0 = static_cast<const C*>(a.in[0]);
+    const C* in1 = static_cast<const C*>(a.in[1]);
+    const C* in2 = static_cast<const C*>(a.in[2]);
+    for (int i = t; i < 6 * K1; i += X4Cfg::NT) {
+      const int cr = i / K1, kx = i - cr * K1;
+      const C* src = cr < 2 ? in0 : cr < 4 ? in1 : in2;  // no dynamic index into the parameter array
+      C* dst = rin + i;
+      if ((cr & 1) == 0 || has1) cp_async8(dst, src + (r0 + (cr & 1)) * K1 + kx);
+      else *dst = make_float2(0.f, 0.f);
+    }
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  // Ia
+  if (t < 81) {
+    const int q = t / 9;
+    C w[10];
+#pragma unroll
+    for (int sa = 1; sa < 10; ++sa) { const C v = __ldg(&tw[9 * q * sa]); w[sa] = make_float2(v.x, -v.y); }
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+      // A: u1, u2 of row r; A': u1, u2 of row r'; B: u3 of rows r and r'
+      const C* ra = rin + (j < 2 ? j : 4) * K1;
+      const C* rb = rin + (j < 2 ? 2 + j : 5) * K1;
+      C v[10];
+#pragma unroll
+      for (int p = 0; p < 10; ++p) {
+        if (p == 4 || p == 5) v[p] = make_float2(0.f, 0.f);  // 324 <= k <= 485 is never retained
+        else v[p] = x4_gather<FULL>(ra, rb, p, t, kmax);
+      }
+      DFT<10, true, C>::run(v);
+      C* xs = reg0 + j * PS;
+      xs[t] = v[0];
+#pragma unroll
+      for (int sa = 1; sa < 10; ++sa) xs[89 * sa + t] = cmul(v[sa], w[sa]);
+    }
+  }
+  __syncthreads();
+  // Ib
+  if (t < 90) {
+    const int sa = t / 9, m2 = t - 9 * sa;
+    C w[9];
+#pragma unroll
+    for (int sb = 0; sb < 9; ++sb) { const C v = __ldg(&tw[m2 * (sa + 10 * sb)]); w[sb] = make_float2(v.x, -v.y); }
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+      const C* xs = reg0 + j * PS + 89 * sa + m2;
+      C v[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) v[q] = xs[9 * q];
+      DFT<9, true, C>::run(v);
+      C* ys = reg1 + j * PS + t;
+#pragma unroll
+      for (int sb = 0; sb < 9; ++sb) ys[90 * sb] = cmul(v[sb], w[sb]);
+    }
+  }
+  __syncthreads();
+  // Ic + F1
+  const float sc = float(a.scale);
+  float u1[9], u2[9], u3[9], u3b[9];
+  C wf[9];
+  if (t < 90) {
+#pragma unroll
+    for (int s = 1; s < 9; ++s) wf[s] = __ldg(&tw[t * s]);
+    C v[9];
+    const C* ya = reg1 + 9 * t;
+#pragma unroll
+    for (int m2 = 0; m2 < 9; ++m2) v[m2] = ya[m2];
+    DFT<9, true, C>::run(v);
+#pragma unroll
+    for (int s = 0; s < 9; ++s) { u1[s] = v[s].x; u2[s] = v[s].y; }
+    const C* yb = reg1 + 2 * PS + 9 * t;
+#pragma unroll
+    for (int m2 = 0; m2 < 9; ++m2) v[m2] = yb[m2];
+    DFT<9, true, C>::run(v);
+#pragma unroll
+    for (int s = 0; s < 9; ++s) { u3[s] = v[s].x; u3b[s] = v[s].y; }
+    x4_f1_row(u1, u2, u3, sc, wf, reg0, t);
+    const C* yc = reg1 + PS + 9 * t;
+#pragma unroll
+    for (int m2 = 0; m2 < 9; ++m2) v[m2] = yc[m2];
+    DFT<9, true, C>::run(v);
+#pragma unroll
+    for (int s = 0; s < 9; ++s) { u1[s] = v[s].x; u2[s] = v[s].y; }
+  }
+  __syncthreads();
+  if (t < 90) x4_f1_row(u1, u2, u3b, sc, wf, reg1, t);
+  __syncthreads();
+  // F2, in place per region: read all three pencils, barrier, write
+  {
+    const int s1 = t / 10, q = t - 10 * s1;
+    C w2[9];
+    if (t < 90) {
+#pragma unroll
+      for (int s = 1; s < 9; ++s) w2[s] = __ldg(&tw[9 * q * s]);
+    }
+#pragma unroll 1
+    for (int g = 0; g < 2; ++g) {
+      C* rg = g ? reg1 : reg0;
+      C v[3][9];
+      if (t < 90) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const C* ws = rg + j * PS + 90 * s1 + q;
+#pragma unroll
+          for (int p = 0; p < 9; ++p) v[j][p] = ws[10 * p];
+          DFT<9, false, C>::run(v[j]);
+#pragma unroll
+          for (int s = 1; s < 9; ++s) v[j][s] = cmul(v[j][s], w2[s]);
+        }
+      }
+      __syncthreads();
+      if (t < 90) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          C* vs = rg + j * PS + 90 * s1 + 9 * q;
+#pragma unroll
+          for (int s = 0; s < 9; ++s) vs[s] = v[j][s];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // F3, in place per region, pruned to the retained modes (outputs s_b = 4, 5,
+  // k in [324, 485], are never retained and are not formed)
+  {
+    const int s1 = t / 9, sa = t - 9 * s1;
+    const int kb = s1 + 9 * sa;
+#pragma unroll 1
+    for (int g = 0; g < 2; ++g) {
+      C* rg = g ? reg1 : reg0;
+      C v[3][10];
+      if (t < 81) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const C* vs = rg + j * PS + 90 * s1 + sa;
+#pragma unroll
+          for (int q = 0; q < 10; ++q) v[j][q] = vs[9 * q];
+          DFT<10, false, C>::run(v[j]);
+        }
+      }
+      __syncthreads();
+      if (t < 81) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          C* zs = rg + j * PS;
+#pragma unroll
+          for (int sb = 0; sb < 10; ++sb) {
+            if (sb == 4 || sb == 5) continue;
+            const int k = kb + 81 * sb;
+            if (FULL) {
+              if (sb <= 2 || (sb == 3 && k <= 270)) zs[k] = v[j][sb];
+              else if (sb >= 7 || (sb == 6 && k >= 540)) zs[270 + (N - k)] = v[j][sb];
+            } else {
+              if (k <= ko) zs[k] = v[j][sb];
+              else if (k >= N - ko) zs[ko + (N - k)] = v[j][sb];
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // S
+  C* o0 = static_cast<C*>(a.out[0]);
+  C* o1 = static_cast<C*>(a.out[1]);
+  C* o2 = static_cast<C*>(a.out[2]);
+  C* o3 = static_cast<C*>(a.out[3]);
+  C* o4 = static_cast<C*>(a.out[4]);
+  C* o5 = static_cast<C*>(a.out[5]);
+  for (int it = t; it < 2 * K1o; it += X4Cfg::NT) {
+    const int rr = it >= K1o, kx = it - rr * K1o;
+    if (rr == 1 && !has1) continue;
+    const long long o = (r0 + rr) * K1o + kx;
+    const C* zs = rr ? reg1 : reg0;
+    const int kc = kx == 0 ? 0 : ko + kx;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const C z = zs[b * PS + kx], zc = zs[b * PS + kc];
+      C* oa = b == 0 ? o0 : b == 1 ? o2 : o4;
+      C* ob = b == 0 ? o1 : b == 1 ? o3 : o5;
+      oa[o] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+      ob[o] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
@@ -669,17 +963,25 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
   }
 }
 
-static bool x3_enabled() {
-  static const bool on = [] {
+// SC_X_KERNEL=2 / =3 select the older x sweeps (for comparison); the default
+// is the three-level kernel where it exists (N = 810), else k_xsweep3.
+static int x_variant() {
+  static const int v = [] {
     const char* e = getenv("SC_X_KERNEL");
-    return !(e && e[0] == '2');
+    return e && (e[0] == '2' || e[0] == '3') ? e[0] - '0' : 4;
   }();
-  return on;
+  return v;
 }
 
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
-  if (a.D == 3 && x3_enabled()) {
+  if (N == 810 && a.D == 3 && x_variant() == 4) {
+    const unsigned nb4 = unsigned((a.nrows + 1) / 2);
+    if (a.K1in == 271 && a.K1out == 271)
+      k_xsweep4<true><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+    else
+      k_xsweep4<false><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  } else if (a.D == 3 && x_variant() != 2) {
     const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
     k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, static_cast<const float2*>(tw));
   } else if (a.D == 3) k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, static_cast<const float2*>(tw));
