@@ -40,7 +40,7 @@ template <int N, int T> struct Col2Cfg {
   static constexpr int NT = T * NJ;
   static constexpr int SR = N2 * T + 8;  // exchange row stride (+8: half-bank shift between rows)
   static constexpr size_t SMEM = size_t(N1) * SR * sizeof(float2);
-  static constexpr int MINB = 1;
+  static constexpr int MINB = N == 810 ? 3 : 1;  // 80 registers at 810: three CTAs per SM
 };
 
 template <int N, int T, bool INV>
@@ -915,13 +915,13 @@ bool init_fast(int N) {
   return cudaGetLastError() == cudaSuccess;
 }
 
-// Inverse sweeps (zero-padded input, 2/3 of the loads) run the persistent
-// prefetching kernel; forward sweeps run one tile per CTA, which measured
-// faster for them.  SC_COL_KERNEL=2 selects the one-tile kernel for both.
+// Both directions run one tile per CTA (three CTAs per SM at 810), which
+// measured faster over a whole step than the persistent prefetching kernel;
+// SC_COL_KERNEL=3 selects the persistent kernel for the inverse sweeps.
 static int col_variant() {
   static const int v = [] {
     const char* e = getenv("SC_COL_KERNEL");
-    return (e && e[0] == '2') ? 2 : 3;
+    return (e && e[0] == '3') ? 3 : 2;
   }();
   return v;
 }
