@@ -5,7 +5,9 @@ kernels.  Test infrastructure only (see ``oracle/__init__.py``).
 The network: input channels (u_x, u_y, u_z, z) with z = (log Re_Delta - mu)/sigma,
 Re_Delta = Delta^2 sqrt(<|grad u|^2>)/nu (the ``fullchain`` convention,
 src/nets.jl:311-331); four 3x3x3 periodic cross-correlations
-4->32->32->32->6 with exact GELU between them.
+4->32->32->32->6 with GELU between them.  GELU is the activation the
+reference's networks use (``gelu`` in src/nets.jl:187, 191, 549-551, from
+NNlib through Lux), the tanh form 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
 """
 
 from __future__ import annotations
@@ -13,11 +15,26 @@ from __future__ import annotations
 import math
 
 import numpy as np
-from scipy.special import erf
 
 from .spectral import Grid, getenergy, twothirds, vectorgradient
 
-__all__ = ["bf16", "cnn_redelta_channel", "cnn_rows"]
+__all__ = ["bf16", "gelu", "gelu_grad", "cnn_redelta_channel", "cnn_rows"]
+
+_GELU_C = math.sqrt(2.0 / math.pi)
+_GELU_A = 0.044715
+
+
+def gelu(x):
+    """NNlib ``gelu`` (tanh form), used by the reference's convolutional nets."""
+    x = np.asarray(x, dtype=np.float64)
+    return 0.5 * x * (1.0 + np.tanh(_GELU_C * (x + _GELU_A * x ** 3)))
+
+
+def gelu_grad(x):
+    """d gelu / dx of the tanh form."""
+    x = np.asarray(x, dtype=np.float64)
+    t = np.tanh(_GELU_C * (x + _GELU_A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _GELU_C * (1.0 + 3.0 * _GELU_A * x * x)
 
 
 def bf16(x):
@@ -71,6 +88,6 @@ def cnn_rows(uphys, zval, weights, biases, rows, round_bf16=True):
             h = 4 - li  # input window half-width
             act = _conv(act, ws[li], biases[li].astype(np.float64), 1, 2 * h - 1, 1, 2 * h - 1)
             if li < 3:
-                act = rnd(0.5 * act * (1.0 + erf(act / math.sqrt(2.0))))
+                act = rnd(gelu(act))
         out.append(act[:, 0, 0, :])
     return np.stack(out, 1)

@@ -133,13 +133,16 @@ __global__ void k_bias_grad(const ConvArgs a, double* gb) {
   }
 }
 
-// exact GELU and its derivative: gelu(x) = x Phi(x), gelu'(x) = Phi(x) + x phi(x)
+// GELU in the tanh form of NNlib's gelu (the activation of the reference's nets)
+// and its derivative: u = c (x + a x^3), gelu = x (1 + tanh u) / 2,
+// gelu' = (1 + tanh u) / 2 + x (1 - tanh^2 u) c (1 + 3 a x^2) / 2
 template <typename R>
 __global__ void k_gelu(const R* pre, R* post, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const R x = pre[i];
-  post[i] = R(0.5) * x * (R(1) + erf(x * R(0.70710678118654752440)));
+  const R u = R(0.79788456080286535588) * (x + R(0.044715) * x * x * x);
+  post[i] = R(0.5) * x * (R(1) + tanh(u));
 }
 
 template <typename R>
@@ -147,9 +150,9 @@ __global__ void k_gelu_bwd(const R* pre, R* g, long long n) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const R x = pre[i];
-  const R Phi = R(0.5) * (R(1) + erf(x * R(0.70710678118654752440)));
-  const R phi = R(0.39894228040143267794) * exp(R(-0.5) * x * x);
-  g[i] *= Phi + x * phi;
+  const R c = R(0.79788456080286535588), a = R(0.044715);
+  const R t = tanh(c * (x + a * x * x * x));
+  g[i] *= R(0.5) * (R(1) + t) + R(0.5) * x * (R(1) - t * t) * c * (R(1) + R(3) * a * x * x);
 }
 
 // a0 = [v_x, v_y, v_z, z] (planar, 4 channels)

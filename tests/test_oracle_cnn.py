@@ -33,7 +33,6 @@ def test_cnn_rows_window_matches_full_grid():
                     out += np.einsum("oc,czyx->ozyx", wb[:, :, kz, ky, kx], sh)
         act = out + b[:, None, None, None]
         if li < 3:
-            from scipy.special import erf
-            act = O.bf16(0.5 * act * (1 + erf(act / np.sqrt(2))))
+            act = O.bf16(0.5 * act * (1 + np.tanh(np.sqrt(2 / np.pi) * (act + 0.044715 * act ** 3))))
     ref = np.stack([act[:, z, y, :] for (y, z) in rows], 1)
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
