@@ -883,6 +883,195 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
+// Persistent column sweep for N = 810 = 9 * 9 * 10 (FP32), both directions.
+// A tile is T = 8 consecutive kx of one column c of one component q.  The
+// tile's stored rows are copied asynchronously (cp.async, 8 B per element)
+// into one of two shared stages while the previous tile is transformed, so
+// the copies of tile i+1 overlap the three radix passes of tile i.  The passes
+// follow the four-step mapping of the 810 x sweep (k = 9 m1 + m2 inverse,
+// x = 90 m1 + m2 forward) with 90 threads per column; shared arrays are
+// [index][kx], so a warp touches 4 indices x 8 kx and global rows stay
+// 64-byte coalesced.  TRUNC: the transform axis is 2/3-truncated (kpos,
+// kneg <= 324), so inputs 324 <= k <= 485 (inverse) are zero and those
+// outputs (forward) are never stored.
+// ---------------------------------------------------------------------------
+struct Col4Cfg {
+  static constexpr int N = 810, T = 8, NT = 720;
+  static constexpr int XR = 882, YR = 810;  // rows of the two exchange arrays
+  static size_t smem(int nin) { return size_t(XR + YR + 2 * nin) * T * sizeof(float2); }
+};
+
+template <bool INV, bool TRUNC>
+__global__ void __launch_bounds__(Col4Cfg::NT, 1)
+k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles, int nin) {
+  using C = float2;
+  constexpr int N = 810, T = Col4Cfg::T, NT = Col4Cfg::NT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* xs = reinterpret_cast<C*>(smem_raw);  // [XR][T]
+  C* ys = xs + Col4Cfg::XR * T;           // [YR][T]
+  C* stg = ys + Col4Cfg::YR * T;          // [2][nin][T]
+  __shared__ const C* s_src[kMaxComp];
+  __shared__ C* s_dst[kMaxComp];
+  const int tid = threadIdx.x, col = tid % T, w = tid / T;  // w = 0 .. 89
+  const int nq = a.ncomp + (INV ? a.ndrv : 0);
+  if (tid < kMaxComp) {
+    // the component pointers by compile-time indices only (no local copy of the parameters)
+    const int src = tid < a.ncomp ? tid : (tid < nq ? a.drv_src[tid - a.ncomp] : 0);
+    const void* ps = nullptr;
+    void* pd = nullptr;
+#pragma unroll
+    for (int j = 0; j < kMaxComp; ++j) {
+      if (j == src) ps = a.in[j];
+      if (j == tid) pd = a.out[j];
+    }
+    s_src[tid] = static_cast<const C*>(ps);
+    s_dst[tid] = static_cast<C*>(pd);
+  }
+  __syncthreads();
+  const int Kc = a.kpos + a.kneg;
+  auto decode = [&](long long tile, int& tx, int& c, int& q) {
+    tx = int(tile % ntx);
+    const long long r = tile / ntx;
+    c = int(r % a.ncols);
+    q = int(r / a.ncols);
+  };
+  auto issue = [&](long long tile, int b) {
+    int tx, c, q;
+    decode(tile, tx, c, q);
+    const C* src = s_src[q] + (long long)c * a.in_cs + tx * T;
+    C* dst = stg + size_t(b) * nin * T;
+    const int live = min(T, a.K1 - tx * T);
+    for (int i = tid; i < nin * T; i += NT) {
+      const int row = i / T, t = i - row * T;
+      if (t < live) cp_async8(dst + i, src + row * a.in_es + t);
+    }
+  };
+  auto compact = [&](int k) { return k < a.kpos ? k : (k >= N - a.kneg ? k - N + Kc : -1); };
+
+  long long tile = blockIdx.x;
+  int b = 0;
+  if (tile < ntiles) issue(tile, 0);
+  cp_async_commit();
+  for (; tile < ntiles; tile += gridDim.x, b ^= 1) {
+    if (tile + gridDim.x < ntiles) issue(tile + gridDim.x, b ^ 1);  // its stage was last read before a barrier
+    cp_async_commit();
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    __syncthreads();
+    int tx, c, q;
+    decode(tile, tx, c, q);
+    const int kx = tx * T + col;
+    const bool live = kx < a.K1;
+    const C* sg = stg + size_t(b) * nin * T + col;
+    if (INV) {
+      // A: radix-10 over p of Z[81 p + t], twiddle exp(+2 pi i qq s_a / 90)
+      if (w < 81) {
+        const int t = w, qq = t / 9;
+        const bool drv = q >= a.ncomp;
+        const bool zo = a.zero_origin && kx == 0 && c == 0;
+        C v[10];
+#pragma unroll
+        for (int p = 0; p < 10; ++p) {
+          v[p] = make_float2(0.f, 0.f);
+          if (TRUNC && (p == 4 || p == 5)) continue;
+          const int pc = compact(81 * p + t);
+          if (pc < 0 || (zo && pc == 0)) continue;
+          C x = sg[pc * T];
+          if (drv) {
+            const float kk = float(a.kfac * double(pc < a.kpos ? pc : pc - Kc));
+            x = make_float2(-kk * x.y, kk * x.x);
+          }
+          v[p] = x;
+        }
+        DFT<10, true, C>::run(v);
+        C* xo = xs + t * T + col;
+        xo[0] = v[0];
+#pragma unroll
+        for (int sa = 1; sa < 10; ++sa) {
+          const C wv = __ldg(&tw[9 * qq * sa]);
+          xo[89 * sa * T] = cmul(v[sa], make_float2(wv.x, -wv.y));
+        }
+      }
+      __syncthreads();
+      // B: radix-9 over qq, twiddle exp(+2 pi i m2 s1 / 810), s1 = s_a + 10 s_b
+      if (w < 90) {
+        const int sa = w / 9, m2 = w - 9 * sa;
+        C v[9];
+        const C* xi = xs + (89 * sa + m2) * T + col;
+#pragma unroll
+        for (int qq = 0; qq < 9; ++qq) v[qq] = xi[9 * qq * T];
+        DFT<9, true, C>::run(v);
+        C* yo = ys + w * T + col;
+#pragma unroll
+        for (int sb = 0; sb < 9; ++sb) {
+          const C wv = __ldg(&tw[m2 * (sa + 10 * sb)]);
+          yo[90 * sb * T] = cmul(v[sb], make_float2(wv.x, -wv.y));
+        }
+      }
+      __syncthreads();
+      // C: radix-9 over m2 -> x = s1 + 90 s2, straight to global memory
+      if (w < 90 && live) {
+        const int s1 = w;
+        C v[9];
+        const C* yi = ys + 9 * s1 * T + col;
+#pragma unroll
+        for (int m2 = 0; m2 < 9; ++m2) v[m2] = yi[m2 * T];
+        DFT<9, true, C>::run(v);
+        C* dst = s_dst[q] + (long long)c * a.out_cs + kx;
+#pragma unroll
+        for (int s2 = 0; s2 < 9; ++s2) dst[(long long)(s1 + 90 * s2) * a.out_es] = v[s2];
+      }
+    } else {
+      // A: radix-9 over m1 of x = 90 m1 + m2, twiddle exp(-2 pi i m2 s1' / 810)
+      if (w < 90) {
+        const int m2 = w;
+        C v[9];
+#pragma unroll
+        for (int m1 = 0; m1 < 9; ++m1) v[m1] = sg[(90 * m1 + m2) * T];
+        DFT<9, false, C>::run(v);
+        C* xo = xs + m2 * T + col;
+        xo[0] = v[0];
+#pragma unroll
+        for (int s = 1; s < 9; ++s) xo[90 * s * T] = cmul(v[s], __ldg(&tw[m2 * s]));
+      }
+      __syncthreads();
+      // B: radix-9 over p (m2 = 10 p + qq), twiddle exp(-2 pi i qq s_a / 90)
+      if (w < 90) {
+        const int s1 = w / 10, qq = w - 10 * s1;
+        C v[9];
+        const C* xi = xs + (90 * s1 + qq) * T + col;
+#pragma unroll
+        for (int p = 0; p < 9; ++p) v[p] = xi[10 * p * T];
+        DFT<9, false, C>::run(v);
+        C* yo = ys + (90 * s1 + 9 * qq) * T + col;
+        yo[0] = v[0];
+#pragma unroll
+        for (int sa = 1; sa < 9; ++sa) yo[sa * T] = cmul(v[sa], __ldg(&tw[9 * qq * sa]));
+      }
+      __syncthreads();
+      // C: radix-10 over qq -> k = s1' + 9 s_a + 81 s_b, retained modes only
+      if (w < 81 && live) {
+        const int s1 = w / 9, sa = w - 9 * s1;
+        C v[10];
+        const C* yi = ys + (90 * s1 + sa) * T + col;
+#pragma unroll
+        for (int qq = 0; qq < 10; ++qq) v[qq] = yi[9 * qq * T];
+        DFT<10, false, C>::run(v);
+        C* dst = s_dst[q] + (long long)c * a.out_cs + kx;
+#pragma unroll
+        for (int sb = 0; sb < 10; ++sb) {
+          if (TRUNC && (sb == 4 || sb == 5)) continue;
+          const int pc = compact(s1 + 9 * sa + 81 * sb);
+          if (pc >= 0) dst[(long long)pc * a.out_es] = v[sb];
+        }
+      }
+    }
+    // the next tile's pass A writes xs only after this barrier; pass C here reads ys
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
@@ -890,6 +1079,14 @@ template <typename F> static void set_smem2(F* f, size_t bytes) {
 }
 
 template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
+
+static void init_col4() {
+  const int mx = int(Col4Cfg::smem(810));
+  cudaFuncSetAttribute(k_col4<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+}
 
 template <int N> static void init_fast_n() {
   constexpr int T = col_tile<N>();
@@ -906,7 +1103,7 @@ bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64;
 
 bool init_fast(int N) {
   switch (N) {
-    case 810: init_fast_n<810>(); break;
+    case 810: init_fast_n<810>(); init_col4(); break;
     case 256: init_fast_n<256>(); break;
     case 128: init_fast_n<128>(); break;
     case 64: init_fast_n<64>(); break;
@@ -915,13 +1112,16 @@ bool init_fast(int N) {
   return cudaGetLastError() == cudaSuccess;
 }
 
-// Both directions run one tile per CTA (three CTAs per SM at 810), which
-// measured faster over a whole step than the persistent prefetching kernel;
-// SC_COL_KERNEL=3 selects the persistent kernel for the inverse sweeps.
+// At 810 the inverse sweeps run the persistent three-level kernel (k_col4: the
+// zero-padded input is staged while the previous tile computes); the forward
+// sweeps, and every other size, run one two-level tile per CTA (k_col2), which
+// keeps shared-memory traffic at one exchange per element.  SC_COL_KERNEL=2
+// selects k_col2 for the 810 inverse sweeps too, SC_COL_KERNEL=3 the older
+// persistent two-level kernel.
 static int col_variant() {
   static const int v = [] {
     const char* e = getenv("SC_COL_KERNEL");
-    return (e && e[0] == '3') ? 3 : 2;
+    return (e && (e[0] == '2' || e[0] == '3')) ? e[0] - '0' : 4;
   }();
   return v;
 }
@@ -937,8 +1137,26 @@ static int num_sms() {
   return n;
 }
 
+template <bool INV> static void col4_launch(const ColArgs& a, const void* tw, cudaStream_t st) {
+  constexpr int T = Col4Cfg::T;
+  const int ntx = (a.K1 + T - 1) / T;
+  const long long ntiles = (long long)ntx * a.ncols * (a.ncomp + (INV ? a.ndrv : 0));
+  const int nin = INV ? a.kpos + a.kneg : 810;
+  const bool trunc = a.kpos <= 324 && a.kneg <= 324;
+  long long grid = num_sms();
+  if (grid > ntiles) grid = ntiles;
+  const size_t sm = Col4Cfg::smem(nin);
+  const float2* t2 = static_cast<const float2*>(tw);
+  if (trunc) k_col4<INV, true><<<unsigned(grid), Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+  else k_col4<INV, false><<<unsigned(grid), Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+}
+
 template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
   constexpr int T = col_tile<N>();
+  if (N == 810 && INV && col_variant() == 4 && a.kpos + a.kneg <= 810) {
+    col4_launch<INV>(a, tw, st);
+    return;
+  }
   if (col_variant() == 3 && INV) {
     using Cfg = Col3Cfg<N, T>;
     const int ntx = (a.K1 + T - 1) / T;
