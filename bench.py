@@ -311,6 +311,92 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
     }
 
 
+ADJ_N, ADJ_NU, ADJ_DH, ADJ_DT, ADJ_SEED = 64, (1e-3, 5e-4), 4, 5e-3, 5
+
+
+def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
+    """A-posteriori training step: 8 LES instances at 64^3 (nu in {1e-3, 5e-4},
+    Delta/h = 4), CNN closure, nsteps-step RK4 rollout checkpointed every ck
+    steps, trajectory-MSE loss against a target rollout of the perturbed closure
+    (weights x (1 + 0.01 N(0,1))), gradient by the hand-written adjoint.
+    Batched: FP32, the 8 jobs concurrently (sc_rollout_adjoint_batch).  Plain:
+    the per-instance FP64 path, one instance after another (plain_instances of
+    them timed, per-instance time reported)."""
+    import numpy as np
+    import torch
+    import symcode as S
+
+    gd = S.Grid(3, 2 * ADJ_N, dtype=torch.float64, device=dev)
+    ws, bs = S.kaiming_cnn_weights(ADJ_SEED)
+    theta = S.pack_cnn_params(ws, bs)
+    fields = []
+    for i in range(4):
+        uc = initial_compact(2 * ADJ_N, ADJ_SEED + i)
+        u_dns = [c.to(dev) for c in to_full(uc, 2 * ADJ_N, torch.float64)]
+        gl = S.Grid(3, ADJ_N, dtype=torch.float64, device=dev)
+        ub, ta = S.vectorfield(gl), S.tensorfield(gl)
+        S.sfs_(ub, ta, u_dns, gd, gl, ADJ_DH * gl.l / ADJ_N)
+        fields.append([c.clone() for c in ub])
+        gl.close()
+    gd.close()
+
+    def make(dtype, idx):
+        jobs = []
+        for i in idx:
+            nu = ADJ_NU[i % 2]
+            g = S.Grid(3, ADJ_N, dtype=dtype, device=dev)
+            u0 = [c.to(g.cdtype).contiguous() for c in fields[i // 2]]
+            cl = S.create_cnn_fp_closure(ADJ_DH * g.l / ADJ_N, nu, g, ws, bs, mu=5.0, sigma=2.0)
+            rng = np.random.default_rng(ADJ_SEED * 100 + i)
+            S.closure_set_params(cl, theta * (1 + 0.01 * rng.standard_normal(theta.size)))
+            traj = S.rollout_record(g, cl, u0, ADJ_DT, nu, nsteps)
+            S.closure_set_params(cl, theta)
+            jobs.append(dict(grid=g, closure=cl, u0=u0, traj=traj, dt=ADJ_DT, visc=nu, nsteps=nsteps, ckpt_every=ck))
+        return jobs
+
+    jobs32 = make(torch.float32, range(8))
+    S.rollout_adjoint_batch(jobs32)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res32 = S.rollout_adjoint_batch(jobs32)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    for j in jobs32:
+        j["closure"].close()
+        j["grid"].close()
+    del jobs32
+    torch.cuda.empty_cache()
+
+    jobs64 = make(torch.float64, range(plain_instances))
+    S.rollout_adjoint(jobs64[0]["grid"], jobs64[0]["closure"], jobs64[0]["u0"], jobs64[0]["traj"], ADJ_DT,
+                      jobs64[0]["visc"], nsteps, ck)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res64 = [S.rollout_adjoint(j["grid"], j["closure"], j["u0"], j["traj"], ADJ_DT, j["visc"], nsteps, ck)
+             for j in jobs64]
+    torch.cuda.synchronize()
+    t_plain = (time.perf_counter() - t0) / plain_instances
+    errs = [float(np.linalg.norm(res32[i][1] - res64[i][1]) / np.linalg.norm(res64[i][1]))
+            for i in range(plain_instances)]
+    for j in jobs64:
+        j["closure"].close()
+        j["grid"].close()
+    torch.cuda.empty_cache()
+    return {
+        "metric": "batched LES+adjoint steps/s (8 x 64^3 training rollouts: forward, loss and adjoint per step)",
+        "value": 8 * nsteps / t_batch, "unit": "steps/s", "s_per_training_step": t_batch,
+        "plain_fp64_steps_per_s": nsteps / t_plain, "plain_fp64_s_per_instance": t_plain,
+        "speedup_vs_plain": (8 * t_plain) / t_batch,
+        "grad_rel_err_fp32_vs_fp64": errs,
+        "losses": [r[0] for r in res32],
+        "config": f"64^3, nu in {list(ADJ_NU)}, Delta/h={ADJ_DH}, RK4 dt={ADJ_DT}, {nsteps} steps, checkpoint every "
+                  f"{ck}; CNN closure (4 layers 3x3x3, 32 channels, GELU, seeded Kaiming weights) on CUDA cores "
+                  "(FP32 batched / FP64 plain: the adjoint differentiates the unrounded network); target rollout "
+                  "of the closure with weights x (1 + 0.01 N(0,1)); initial fields sfs! of seeded 128^3 fields; "
+                  "host wall clock around the synchronous calls",
+    }
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -383,6 +469,9 @@ def run_gpu(args):
     alg = {"z_inverse": per["z_inverse"], "y_inverse": per["y_inverse"], "x_sweep": per["x_sweep"],
            "y_forward": per["y_forward"], "z_forward": 6 * b + 6 * a, "epilogue": 12 * a}
     dom = max(kms, key=lambda kk: kms[kk])
+    # DRAM traffic of the x sweep from one ncu capture (profiles/k_xsweep4_810_x_sweep_65610_rows.md:
+    # 426.8 MB read + 798.3 MB written for 65610 rows), scaled to the launch's n^2 rows
+    traffic = (426.822656e6 + 798.346752e6) / 65610 * n * n if (dom == "x_sweep" and n == 810) else None
     hbm, src = peaks()
     achieved = alg[dom] / (kms[dom] / 1e3) / 1e9
     step_bytes = 4 * b_rhs
@@ -420,6 +509,10 @@ def run_gpu(args):
     if rank == 0 and not args.skip_les:
         les = les_batch_measure(dev, args.les_steps, 3)
 
+    adj = None
+    if rank == 0 and not args.skip_adj:
+        adj = les_adjoint_measure(dev, args.adj_steps, 5)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.skip_cpu:
         sec = cpu_sample_steps(args.cpu_sample_n, 1)
@@ -441,13 +534,14 @@ def run_gpu(args):
             "step_hbm": {"algorithmic_bytes_per_step": step_bytes, "achieved_gbs": step_gbs,
                          "frac": step_gbs / hbm},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": src,
+                         "frac": achieved / hbm, "traffic": traffic, "peak_source": src,
                          "kernel_ms": kms, "kernel_algorithmic_bytes": alg},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
             "les_batch": les,
+            "les_adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -469,6 +563,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-les", action="store_true")
     ap.add_argument("--les-steps", type=int, default=10)
+    ap.add_argument("--skip-adj", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=8)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

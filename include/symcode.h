@@ -262,6 +262,23 @@ SC_API int sc_rollout_loss(sc_plan* plan, sc_closure* closure, const void* const
 SC_API int sc_rollout_adjoint(sc_plan* plan, sc_closure* closure, const void* const* u0, const void* traj,
                               double dt, double visc, int nsteps, int ckpt_every, double* loss, double* grad,
                               void* stream);
+/* A batch of training rollouts (the a-posteriori training step over several
+ * LES instances): job i is sc_rollout_adjoint(plan, closure, u0, traj, dt,
+ * visc, nsteps, ckpt_every, loss, grad).  The jobs run concurrently, each from
+ * its own host thread on its own stream, after the work already queued on
+ * `stream`; every job needs its own plan and closure.  status[i] receives each
+ * job's sc_status; the call returns the first non-zero one.  Synchronous. */
+typedef struct sc_rollout_job {
+  sc_plan* plan;
+  sc_closure* closure;
+  const void* u0[3];
+  const void* traj;
+  double dt, visc;
+  int nsteps, ckpt_every;
+  double* loss; /* host, 1 */
+  double* grad; /* host, sc_closure_num_params */
+} sc_rollout_job;
+SC_API int sc_rollout_adjoint_batch(int njobs, const sc_rollout_job* jobs, int* status, void* stream);
 
 /* ---- DNS -> LES filter ------------------------------------------------------
  * sfs!(; tau, ubar, u, g_dns, g_les, Delta) (src/data.jl:625-642) for `ndelta`

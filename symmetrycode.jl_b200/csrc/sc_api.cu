@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sc_fft.cuh"
@@ -1886,6 +1887,42 @@ int sc_rollout_adjoint(sc_plan* p, sc_closure* cl, const void* const* u0, const 
   if (rc) return rc;
   return SC_DTYPE_DISPATCH(p, rollout_impl, p, cl, u0, traj, dt, visc, nsteps, ckpt_every, loss, grad, nullptr,
                            as_stream(stream));
+}
+
+int sc_rollout_adjoint_batch(int njobs, const sc_rollout_job* jobs, int* status, void* stream) {
+  if (njobs < 1 || !jobs || !status) return fail(SC_ERR_INVALID, "bad argument");
+  for (int i = 0; i < njobs; ++i)
+    for (int j = 0; j < i; ++j)
+      if (jobs[i].plan == jobs[j].plan || jobs[i].closure == jobs[j].closure)
+        return fail(SC_ERR_INVALID, "jobs %d and %d share a plan or closure", j, i);
+  // jobs start after the work already on the caller's stream
+  cudaEvent_t ready;
+  SC_CU(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  SC_CU(cudaEventRecord(ready, as_stream(stream)));
+  std::vector<std::string> errs(njobs);
+  auto run = [&](int i) {
+    const sc_rollout_job& J = jobs[i];
+    cudaStream_t js = nullptr;
+    int rc = J.plan ? ensure_device(J.plan) : fail(SC_ERR_INVALID, "null plan");
+    if (!rc && cudaStreamCreateWithFlags(&js, cudaStreamNonBlocking) != cudaSuccess)
+      rc = fail(SC_ERR_CUDA, "cudaStreamCreateWithFlags failed");
+    if (!rc && cudaStreamWaitEvent(js, ready, 0) != cudaSuccess) rc = fail(SC_ERR_CUDA, "cudaStreamWaitEvent failed");
+    if (!rc)
+      rc = sc_rollout_adjoint(J.plan, J.closure, J.u0, J.traj, J.dt, J.visc, J.nsteps, J.ckpt_every, J.loss, J.grad,
+                              js);
+    if (js) cudaStreamDestroy(js);
+    status[i] = rc;
+    if (rc) errs[i] = g_err;  // the error text is per host thread
+  };
+  std::vector<std::thread> th;
+  th.reserve(njobs - 1);
+  for (int i = 1; i < njobs; ++i) th.emplace_back(run, i);
+  run(0);
+  for (auto& t : th) t.join();
+  cudaEventDestroy(ready);
+  for (int i = 0; i < njobs; ++i)
+    if (status[i]) return fail(status[i], "job %d: %s", i, errs[i].c_str());
+  return SC_OK;
 }
 
 int sc_plan_set_option(sc_plan* p, int option, long long value) {

@@ -421,6 +421,37 @@ def rollout_adjoint(g: Grid, cl, u0, traj, dt, visc, nsteps, ckpt_every=5, strea
     return out.value, grad
 
 
+def rollout_adjoint_batch(jobs, stream=None):
+    """Several training rollouts at once (``sc_rollout_adjoint_batch``): each job is a
+    dict(grid, closure, u0, traj, dt, visc, nsteps, ckpt_every); returns a list of
+    (loss, dloss/dtheta).  Jobs run concurrently, one stream each; every job needs
+    its own grid (plan) and closure."""
+    import numpy as np
+    from ._lib import sc_rollout_job
+    n = len(jobs)
+    arr = (sc_rollout_job * n)()
+    keep, outs = [], []
+    for i, j in enumerate(jobs):
+        g = j["grid"]
+        u0 = [g._check_spec(c) for c in j["u0"]]  # device addresses (validated)
+        keep.append(j["u0"])
+        grad = np.zeros(closure_num_params(j["closure"]), dtype=np.float64)
+        loss = ct.c_double()
+        outs.append((loss, grad))
+        J = arr[i]
+        J.plan, J.closure = g.plan, _cl(j["closure"])
+        for c in range(3):
+            J.u0[c] = u0[c] if c < len(u0) else None
+        J.traj = j["traj"].data_ptr()
+        J.dt, J.visc = float(j["dt"]), float(j["visc"])
+        J.nsteps, J.ckpt_every = int(j["nsteps"]), int(j.get("ckpt_every", 5))
+        J.loss = ct.pointer(loss)
+        J.grad = grad.ctypes.data_as(ct.POINTER(ct.c_double))
+    status = (ct.c_int * n)()
+    check(lib().sc_rollout_adjoint_batch(n, arr, status, _stream_ptr(stream)))
+    return [(l.value, g) for l, g in outs]
+
+
 def _cl(model):
     return model.ptr if model is not None else None
 

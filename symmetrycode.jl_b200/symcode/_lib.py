@@ -35,6 +35,12 @@ class sc_les_instance(ct.Structure):
                 ("forced", ct.c_int), ("eps", ct.c_double)]
 
 
+class sc_rollout_job(ct.Structure):
+    _fields_ = [("plan", ct.c_void_p), ("closure", ct.c_void_p), ("u0", ct.c_void_p * 3), ("traj", ct.c_void_p),
+                ("dt", ct.c_double), ("visc", ct.c_double), ("nsteps", ct.c_int), ("ckpt_every", ct.c_int),
+                ("loss", ct.POINTER(ct.c_double)), ("grad", ct.POINTER(ct.c_double))]
+
+
 _vp = ct.c_void_p
 _pp = ct.POINTER(ct.c_void_p)
 
@@ -90,6 +96,7 @@ _SIGS = {
     "sc_maintain_shell_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_state_maintain_shell_energy": ([_vp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_spectrum": ([_vp, _pp, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
+    "sc_rollout_adjoint_batch": ([ct.c_int, ct.POINTER(sc_rollout_job), ct.POINTER(ct.c_int), _vp], ct.c_int),
     "sc_spectrum_static": ([_pp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),

@@ -56,7 +56,7 @@ def test_rollout_adjoint_matches_finite_differences():
     loss, grad = S.rollout_adjoint(g, cl, u0, traj, dt, nu, nsteps, ckpt_every=ck)
     assert loss > 0 and np.isfinite(grad).all() and np.abs(grad).max() > 0
     assert math.isclose(loss, S.rollout_loss(g, cl, u0, traj, dt, nu, nsteps), rel_tol=1e-12)
-    for k in range(4):
+    for k in range(16):
         d = rng.standard_normal(theta.size)
         d /= np.linalg.norm(d)
         h = 1e-4 * np.linalg.norm(theta) / math.sqrt(theta.size)
@@ -68,3 +68,38 @@ def test_rollout_adjoint_matches_finite_differences():
         ad = float(grad @ d)
         assert abs(fd - ad) <= 1e-6 * abs(ad) + 1e-14, (k, fd, ad)
     S.closure_set_params(cl, theta)
+
+
+def test_rollout_adjoint_batch_matches_single_jobs():
+    """Concurrent jobs (own plan, closure and stream each) give the single-job results."""
+    n, nsteps, ck, dt = 16, 3, 2, 2e-3
+    go = O.Grid(3, n)
+    ws, bs = _weights(11, scale_last=0.3)
+    theta = S.pack_cnn_params(ws, bs)
+    jobs, ref = [], []
+    for i, nu in enumerate((2e-3, 1e-3, 5e-4)):
+        g = S.Grid(3, n, dtype=torch.float64, device="cuda:0")
+        u0 = [to_dev(c, g) for c in O.random_field(go, seed=70 + i, kpeak=2)]
+        cl = S.create_cnn_fp_closure(4 * go.l / n, nu, g, ws, bs, mu=1.0, sigma=2.0)
+        S.closure_set_params(cl, theta * (1 + 0.01 * np.random.default_rng(80 + i).standard_normal(theta.size)))
+        traj = S.rollout_record(g, cl, u0, dt, nu, nsteps)
+        S.closure_set_params(cl, theta)
+        ref.append(S.rollout_adjoint(g, cl, u0, traj, dt, nu, nsteps, ckpt_every=ck))
+        jobs.append(dict(grid=g, closure=cl, u0=u0, traj=traj, dt=dt, visc=nu, nsteps=nsteps, ckpt_every=ck))
+    for _ in range(2):
+        got = S.rollout_adjoint_batch(jobs)
+        for (l, gr), (lr, grr) in zip(got, ref):
+            assert math.isclose(l, lr, rel_tol=1e-12)
+            assert np.linalg.norm(gr - grr) <= 1e-12 * np.linalg.norm(grr)
+
+
+def test_rollout_adjoint_batch_rejects_shared_plans():
+    n = 16
+    g = S.Grid(3, n, dtype=torch.float64, device="cuda:0")
+    ws, bs = _weights(12)
+    cl = S.create_cnn_fp_closure(4 * g.l / n, 1e-3, g, ws, bs)
+    u0 = [to_dev(c, g) for c in O.random_field(O.Grid(3, n), seed=90, kpeak=2)]
+    traj = S.rollout_record(g, cl, u0, 2e-3, 1e-3, 2)
+    job = dict(grid=g, closure=cl, u0=u0, traj=traj, dt=2e-3, visc=1e-3, nsteps=2)
+    with pytest.raises(S.SymcodeError):
+        S.rollout_adjoint_batch([job, job])
