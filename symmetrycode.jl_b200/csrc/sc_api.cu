@@ -103,6 +103,11 @@ struct sc_closure {
   void* cw[4] = {};   // packed BF16 weights per layer
   void* cbias[4] = {};
   void* act[3] = {};  // BF16 activations
+  void* cwt[4] = {};  // packed BF16 transposed, flipped weights (input-gradient convolutions)
+  void* tact3 = nullptr;        // adjoint: BF16 input of layer 4
+  void* tpre[3] = {};           // adjoint: FP32 pre-activations
+  void* tgbf = nullptr;         // adjoint: BF16 gradient scratch
+  void* tgf = nullptr;          // adjoint: FP32 gradient scratch
   int* err = nullptr;
   double nu = 0, mu = 0, sigma = 1;
   // CUDA-core CNN (FP32/FP64): weights, activations a0 h1 a1 h2 a2 h3 a3, tau, gradients
@@ -340,6 +345,13 @@ sc::LesPhysArgs phys_args(sc_plan* p) {
 // ---------------------------------------------------------------------------
 static const int kCcCin[4] = {4, 32, 32, 32}, kCcCout[4] = {32, 32, 32, 6};
 
+int num_sms_api() {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  return nsm > 0 ? nsm : 148;
+}
+
 long long cc_layer_offset(int l) {  // offset of layer l in the flat parameter vector [w, b]
   long long o = 0;
   for (int i = 0; i < l; ++i) o += (long long)kCcCout[i] * kCcCin[i] * 27 + kCcCout[i];
@@ -403,6 +415,63 @@ int cc_backward(sc_closure* cl, const R* gtau, cudaStream_t st) {
   SC_CU(cudaMemsetAsync(cl->dsum + 1, 0, sizeof(double), st));
   sc::launch_sum<R>(static_cast<const R*>(cl->ccg0) + 3 * np, np, cl->dsum + 1, st);
   return check_launch("cnn backward (CUDA cores)");
+}
+
+// Tensor-core CNN for the adjoint: forward at u keeping every layer input and
+// the pre-activations (v in gp[0..2], tau in tp), and backward from dL/dtau
+// (planar FP32 in cctau) to dL/dv (ccg0[0..2]), dL/dz (dsum[1]) and the
+// parameter gradient (cl->gw).  The backward differentiates the network with
+// the BF16 roundings of weights and activations taken as identities.
+int tc_forward(sc_closure* cl, void* const* u, cudaStream_t st) {
+  sc_plan* p = cl->p;
+  int rc = c2p_batch<float>(p, cl->bb, cl->cb, u, cl->gp, 3, st);
+  if (rc) return rc;
+  SC_CU(cudaMemsetAsync(cl->dsum, 0, sizeof(double), st));
+  sc::launch_spectral_energy<float>(u, 3, 3, p->n, p->K1, p->K2, 1, p->kc, 2.0 * M_PI / p->l, 1, cl->dsum, st);
+  sc::CnnArgs a{};
+  a.n = p->n;
+  for (int c = 0; c < 3; ++c) a.u[c] = cl->gp[c];
+  for (int l = 0; l < 4; ++l) {
+    a.w[l] = static_cast<const __nv_bfloat16*>(cl->cw[l]);
+    a.b[l] = static_cast<const float*>(cl->cbias[l]);
+  }
+  a.act0 = static_cast<__nv_bfloat16*>(cl->act[0]);
+  a.act1 = static_cast<__nv_bfloat16*>(cl->act[1]);
+  a.act2 = static_cast<__nv_bfloat16*>(cl->act[2]);
+  a.act3 = static_cast<__nv_bfloat16*>(cl->tact3);
+  for (int l = 0; l < 3; ++l) a.pre[l] = static_cast<float*>(cl->tpre[l]);
+  for (int c = 0; c < 6; ++c) a.tau.p[c] = static_cast<float*>(cl->tp[c]);
+  a.a2 = cl->dsum; a.z = cl->dsum + 3;
+  a.delta = cl->delta; a.nu = cl->nu; a.mu = cl->mu; a.sigma = cl->sigma;
+  a.err = cl->err;
+  a.nsm = num_sms_api();
+  sc::launch_cnn_forward(a, st);
+  return check_launch("cnn forward (tensor cores, adjoint)");
+}
+
+int tc_backward(sc_closure* cl, cudaStream_t st) {
+  sc_plan* p = cl->p;
+  const long long np = phys_args(p).npts;
+  sc::CnnBwdArgs b{};
+  b.n = p->n;
+  for (int c = 0; c < 6; ++c) b.gtau.p[c] = static_cast<float*>(cl->cctau) + (size_t)c * np;
+  for (int l = 0; l < 4; ++l) b.wt[l] = static_cast<const __nv_bfloat16*>(cl->cwt[l]);
+  b.act[0] = static_cast<const __nv_bfloat16*>(cl->act[0]);
+  b.act[1] = static_cast<const __nv_bfloat16*>(cl->act[1]);
+  b.act[2] = static_cast<const __nv_bfloat16*>(cl->act[2]);
+  b.act[3] = static_cast<const __nv_bfloat16*>(cl->tact3);
+  for (int l = 0; l < 3; ++l) b.pre[l] = static_cast<const float*>(cl->tpre[l]);
+  b.gbf = static_cast<__nv_bfloat16*>(cl->tgbf);
+  b.gf = static_cast<float*>(cl->tgf);
+  for (int c = 0; c < 4; ++c) b.gin_planar.p[c] = static_cast<float*>(cl->ccg0) + (size_t)c * np;
+  b.gw = cl->gw;
+  for (int l = 0; l < 4; ++l) b.woff[l] = cc_layer_offset(l);
+  b.err = cl->err;
+  b.nsm = num_sms_api();
+  sc::launch_cnn_backward(b, st);
+  SC_CU(cudaMemsetAsync(cl->dsum + 1, 0, sizeof(double), st));
+  sc::launch_sum<float>(static_cast<const float*>(cl->ccg0) + 3 * np, np, cl->dsum + 1, st);
+  return check_launch("cnn backward (tensor cores)");
 }
 
 // Closure stress of the compact state u into cl->th (compact), i.e. the
@@ -494,6 +563,7 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
     SC_CU(cudaMemsetAsync(cl->dsum, 0, sizeof(double), st));
     sc::launch_spectral_energy<R>(u, D, D, p->n, p->K1, p->K2, 1, p->kc, 2.0 * M_PI / p->l, 1, cl->dsum, st);
     sc::CnnArgs a{};
+    a.n = p->n;
     for (int c = 0; c < 3; ++c) a.u[c] = cl->gp[c];
     for (int l = 0; l < 4; ++l) {
       a.w[l] = static_cast<const __nv_bfloat16*>(cl->cw[l]);
@@ -1231,12 +1301,75 @@ static uint16_t host_bf16(float f) {
   return uint16_t(x >> 16);
 }
 
+}  // extern "C"
+
+namespace {
+// Upload theta (PyTorch order per layer: w[Cout][Cin][27] then b[Cout]) to the
+// tensor-core CNN: BF16 forward weights in the UMMA K-major layout
+// [27][CP/8][COP][8], FP32 biases, and the input-gradient convolution's
+// weights W'[ci][co][t'] = W[co][ci][26 - t'] (transposed and flipped) in the
+// same layout with the roles of CP and COP exchanged.
+int tc_upload_params(sc_closure* cl, const double* theta) {
+  static const int cin[4] = {4, 32, 32, 32}, cout[4] = {32, 32, 32, 6}, cp[4] = {16, 32, 32, 32},
+                   cop[4] = {32, 32, 32, 16};
+  for (int l = 0; l < 4; ++l) {
+    const long long o = cc_layer_offset(l), nw = (long long)cout[l] * cin[l] * 27;
+    const int cpc = cp[l] / 8;
+    std::vector<uint16_t> wp((size_t)27 * cp[l] * cop[l], 0), wt((size_t)27 * cp[l] * cop[l], 0);
+    for (int t = 0; t < 27; ++t)
+      for (int kc = 0; kc < cpc; ++kc)
+        for (int nn = 0; nn < cout[l]; ++nn)
+          for (int j = 0; j < 8; ++j) {
+            const int ci = 8 * kc + j;
+            if (ci < cin[l]) wp[(((size_t)t * cpc + kc) * cop[l] + nn) * 8 + j] = host_bf16(float(theta[o + ((long long)nn * cin[l] + ci) * 27 + t]));
+          }
+    const int cpc2 = cop[l] / 8;  // input-gradient convolution: CP' = cop, COP' = cp
+    for (int t2 = 0; t2 < 27; ++t2)
+      for (int kc = 0; kc < cpc2; ++kc)
+        for (int nn = 0; nn < cin[l]; ++nn)
+          for (int j = 0; j < 8; ++j) {
+            const int k = 8 * kc + j;  // a forward output channel
+            if (k < cout[l])
+              wt[(((size_t)t2 * cpc2 + kc) * cp[l] + nn) * 8 + j] =
+                  host_bf16(float(theta[o + ((long long)k * cin[l] + nn) * 27 + (26 - t2)]));
+          }
+    std::vector<float> bp(cop[l], 0.f);
+    for (int nn = 0; nn < cout[l]; ++nn) bp[nn] = float(theta[o + nw + nn]);
+    SC_CU(cudaMemcpy(cl->cw[l], wp.data(), wp.size() * 2, cudaMemcpyHostToDevice));
+    SC_CU(cudaMemcpy(cl->cwt[l], wt.data(), wt.size() * 2, cudaMemcpyHostToDevice));
+    SC_CU(cudaMemcpy(cl->cbias[l], bp.data(), bp.size() * 4, cudaMemcpyHostToDevice));
+  }
+  return SC_OK;
+}
+
+// the tensor-core CNN's adjoint buffers, on first use
+int tc_adjoint_buffers(sc_closure* cl) {
+  if (cl->tgf) return SC_OK;
+  const size_t np = (size_t)cl->p->n * cl->p->n * cl->p->n;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  int rc = A(&cl->tact3, np * 32 * 2);
+  for (int l = 0; l < 3 && !rc; ++l) rc = A(&cl->tpre[l], np * 32 * 4);
+  if (!rc) rc = A(&cl->tgbf, np * 32 * 2);
+  if (!rc) rc = A(&cl->cctau, np * 6 * 4);
+  if (!rc) rc = A(&cl->ccg0, np * 4 * 4);
+  if (!rc) rc = A(&cl->tgf, np * 32 * 4);  // last: marks the set complete
+  return rc;
+}
+}  // namespace
+
+extern "C" {
+
 int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, const float* const* weights,
                           const float* const* biases, double mu, double sigma) {
   if (!out || !p || !weights || !biases) return fail(SC_ERR_INVALID, "null argument");
   *out = nullptr;
   if (p->dtype != SC_FLOAT32 || !sc::cnn_supported(p->n, p->D))
-    return fail(SC_ERR_UNSUPPORTED, "the CNN closure runs on FP32 3D plans with n = 128");
+    return fail(SC_ERR_UNSUPPORTED, "the tensor-core CNN closure runs on FP32 3D plans with n = 64 or 128");
   if (!(delta > 0) || !(visc > 0) || !(sigma > 0)) return fail(SC_ERR_INVALID, "delta, visc and sigma must be positive");
   for (int l = 0; l < 4; ++l)
     if (!weights[l] || !biases[l]) return fail(SC_ERR_INVALID, "missing weights of layer %d", l);
@@ -1245,8 +1378,8 @@ int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
   if (rc) return rc;
   cl->kind = sc::kCnn;
   cl->nu = visc; cl->mu = mu; cl->sigma = sigma;
-  static const int cin[4] = {4, 32, 32, 32}, cout[4] = {32, 32, 32, 6}, cp[4] = {16, 32, 32, 32},
-                   cop[4] = {32, 32, 32, 16};
+  cl->nparam = cc_layer_offset(4);
+  static const int cp[4] = {16, 32, 32, 32}, cop[4] = {32, 32, 32, 16};
   const size_t npts = (size_t)p->n * p->n * p->n;
   auto A = [&](void** ptr, size_t bytes) -> int {
     cudaError_t e = cudaMalloc(ptr, bytes);
@@ -1255,31 +1388,26 @@ int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
     return SC_OK;
   };
   for (int l = 0; l < 4 && !rc; ++l) {
-    const int cpc = cp[l] / 8;
-    std::vector<uint16_t> wp((size_t)27 * cpc * cop[l] * 8, 0);
-    for (int t = 0; t < 27; ++t)
-      for (int kc = 0; kc < cpc; ++kc)
-        for (int nn = 0; nn < cout[l]; ++nn)
-          for (int j = 0; j < 8; ++j) {
-            const int ci = 8 * kc + j;
-            if (ci >= cin[l]) continue;
-            // PyTorch conv3d layout (Cout, Cin, kz, ky, kx); tap t = kz*9 + ky*3 + kx
-            const float w = weights[l][((size_t)nn * cin[l] + ci) * 27 + t];
-            wp[(((size_t)t * cpc + kc) * cop[l] + nn) * 8 + j] = host_bf16(w);
-          }
-    std::vector<float> bp(cop[l], 0.f);
-    for (int nn = 0; nn < cout[l]; ++nn) bp[nn] = biases[l][nn];
-    if (!rc) rc = A(&cl->cw[l], wp.size() * 2);
-    if (!rc) rc = A(&cl->cbias[l], bp.size() * 4);
-    if (!rc && (cudaMemcpy(cl->cw[l], wp.data(), wp.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-                cudaMemcpy(cl->cbias[l], bp.data(), bp.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
-      rc = fail(SC_ERR_CUDA, "weight upload");
+    const size_t nwp = (size_t)27 * cp[l] * cop[l];
+    rc = A(&cl->cw[l], nwp * 2);
+    if (!rc) rc = A(&cl->cwt[l], nwp * 2);
+    if (!rc) rc = A(&cl->cbias[l], cop[l] * 4);
   }
   if (!rc) rc = A(&cl->act[0], npts * 16 * 2);
   if (!rc) rc = A(&cl->act[1], npts * 32 * 2);
   if (!rc) rc = A(&cl->act[2], npts * 32 * 2);
   if (!rc) rc = A((void**)&cl->err, sizeof(int));
+  if (!rc) rc = A((void**)&cl->gw, cl->nparam * sizeof(double));
   if (!rc && cudaMemset(cl->err, 0, sizeof(int)) != cudaSuccess) rc = fail(SC_ERR_CUDA, "memset");
+  if (!rc) {
+    std::vector<double> theta(cl->nparam);
+    for (int l = 0; l < 4; ++l) {
+      const long long o = cc_layer_offset(l), nw = (long long)kCcCout[l] * kCcCin[l] * 27;
+      for (long long i = 0; i < nw; ++i) theta[o + i] = weights[l][i];
+      for (int i = 0; i < kCcCout[l]; ++i) theta[o + nw + i] = biases[l][i];
+    }
+    rc = tc_upload_params(cl, theta.data());
+  }
   if (!rc) {
     sc::cnn_init();
     if (cudaGetLastError() != cudaSuccess) rc = fail(SC_ERR_CUDA, "CNN kernel setup");
@@ -1337,13 +1465,14 @@ int sc_cnn_fp_closure_create(sc_closure** out, sc_plan* p, double delta, double 
 
 int sc_closure_num_params(const sc_closure* cl, long long* n) {
   if (!cl || !n) return fail(SC_ERR_INVALID, "null argument");
-  *n = cl->kind == sc::kCnnFp ? cl->nparam : 0;
+  *n = (cl->kind == sc::kCnnFp || cl->kind == sc::kCnn) ? cl->nparam : 0;
   return SC_OK;
 }
 
 int sc_closure_set_params(sc_closure* cl, const double* theta) {
   if (!cl || !theta) return fail(SC_ERR_INVALID, "null argument");
-  if (cl->kind != sc::kCnnFp) return fail(SC_ERR_UNSUPPORTED, "only the FP32/FP64 CNN closure has a parameter vector");
+  if (cl->kind == sc::kCnn) return tc_upload_params(cl, theta);
+  if (cl->kind != sc::kCnnFp) return fail(SC_ERR_UNSUPPORTED, "only the CNN closures have a parameter vector");
   const bool f64 = cl->p->dtype == SC_FLOAT64;
   for (int l = 0; l < 4; ++l) {
     const long long o = cc_layer_offset(l), nw = (long long)kCcCout[l] * kCcCin[l] * 27, nb_ = kCcCout[l];
@@ -1650,10 +1779,12 @@ int stage_adjoint(sc_plan* p, sc_closure* cl, void* const* u, void* const* lam, 
   for (int c = 0; c < NP; ++c) as.lsig[c] = lsig[c];
   as.D = D; as.kc = p->kc; as.kfac = 2.0 * M_PI / p->l; as.visc = visc;
   sc::launch_adj_spec<R>(as, st);
-  const bool cnn = cl && cl->kind == sc::kCnnFp;
+  const bool tc = cl && cl->kind == sc::kCnn;
+  const bool cnn = cl && (cl->kind == sc::kCnnFp || tc);
   int rc = SC_OK;
   // physical velocity of the stage (and the CNN activations) at u
-  if (cnn) rc = cc_forward<R>(cl, u, st);  // v in gp[0..2]
+  if (tc) rc = tc_forward(cl, u, st);  // v in gp[0..2]
+  else if (cnn) rc = cc_forward<R>(cl, u, st);
   else rc = c2p_batch<R>(p, cl->bb, cl->cb, u, cl->gp, D, st);
   if (rc) return rc;
   // m = T(lsig) / N, physical: into the CNN tau buffer (as dL/dtau) or gp[3..]
@@ -1682,7 +1813,8 @@ int stage_adjoint(sc_plan* p, sc_closure* cl, void* const* u, void* const* lam, 
     }
     if ((rc = check_launch("adjoint stress to physical"))) return rc;
   }
-  if (cnn && (rc = cc_backward<R>(cl, static_cast<const R*>(cl->cctau), st))) return rc;
+  if (tc && (rc = tc_backward(cl, st))) return rc;
+  if (cnn && !tc && (rc = cc_backward<R>(cl, static_cast<const R*>(cl->cctau), st))) return rc;
   sc::AdjPhysArgs ap{};
   for (int c = 0; c < D; ++c) {
     ap.v[c] = cl->gp[c];
@@ -1880,10 +2012,11 @@ int sc_rollout_loss(sc_plan* p, sc_closure* cl, const void* const* u0, const voi
 int sc_rollout_adjoint(sc_plan* p, sc_closure* cl, const void* const* u0, const void* traj, double dt, double visc,
                        int nsteps, int ckpt_every, double* loss, double* grad, void* stream) {
   if (!p || !traj || !grad || nsteps < 1 || ckpt_every < 1) return fail(SC_ERR_INVALID, "bad argument");
-  if (!cl || cl->p != p || cl->kind != sc::kCnnFp)
-    return fail(SC_ERR_INVALID, "the adjoint needs the FP32/FP64 CNN closure of this plan");
+  if (!cl || cl->p != p || (cl->kind != sc::kCnnFp && cl->kind != sc::kCnn))
+    return fail(SC_ERR_INVALID, "the adjoint needs a CNN closure of this plan");
   int rc = check_ptrs(u0, p->D);
   if (!rc) rc = ensure_device(p);
+  if (!rc && cl->kind == sc::kCnn) rc = tc_adjoint_buffers(cl);
   if (rc) return rc;
   return SC_DTYPE_DISPATCH(p, rollout_impl, p, cl, u0, traj, dt, visc, nsteps, ckpt_every, loss, grad, nullptr,
                            as_stream(stream));

@@ -6,7 +6,10 @@
 // standardised log Re_Delta as a constant 4th channel, conv 4->32, GELU,
 // conv 32->32, GELU, conv 32->32, GELU, conv 32->6 -> tau (pair order).
 //
-// One CTA computes one output x-row (128 voxels = the MMA's M) at a time.  The
+// Grids of n = 64 and n = 128 points per axis.  One CTA computes one output
+// x-row at a time with M = 128 MMAs: at n = 128 the row is the tile; at n = 64
+// rows 64..127 of the tile read staged data past the row (in bounds, never
+// stored) and only TMEM lanes 0..63 are read back.  The
 // nine input rows (y-1..y+1, z-1..z+1) are staged once in shared memory in the
 // UMMA K-major no-swizzle layout [row][k-chunk][x+1][8 channels] with a one-voxel
 // periodic halo in x, so the 27 taps are 27 descriptors into the same slab:
@@ -25,8 +28,6 @@ namespace sc {
 
 namespace {
 
-constexpr int kN = 128;        // grid size handled (one x-row = one MMA tile)
-constexpr int kRowPlane = (kN + 2) * 16;  // bytes of one k-chunk plane of one staged row
 constexpr long long kSpinLimit = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -110,15 +111,34 @@ __device__ __forceinline__ float gelu(float x) {
   return 0.5f * x * (1.f + tanh_hw(u));
 }
 
+
+__device__ __forceinline__ float gelu_grad(float x) {
+  const float c = 0.7978845608028654f, a = 0.044715f;
+  const float t = tanhf(c * x * (1.f + a * x * x));
+  return 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * c * (1.f + 3.f * a * x * x);
+}
+
 }  // namespace
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
+template <int KN> constexpr int row_plane() { return (KN + 2) * 16; }  // bytes of one k-chunk plane of a staged row
+
+// Epilogue modes: BF16 GELU activations; the same plus the FP32
+// pre-activations (kept for the adjoint); FP32 planar tau (last layer);
+// FP32 channels-last without bias or activation (the input-gradient convolution).
+enum { kGelu = 0, kGeluSave = 1, kTau = 2, kLinear = 3 };
+
+struct ConvOut {
+  __nv_bfloat16* act;  // kGelu, kGeluSave: BF16 channels-last [n^3][COP]
+  float* pre;          // kGeluSave: FP32 channels-last pre-activations; kLinear: FP32 channels-last output
+  TauPtrs tau;         // kTau
+};
+
 // One convolution layer.  act_in: BF16 channels-last [n^3][CP]; weights:
-// BF16 [27][CP/8][COP][8] (UMMA K-major planes per tap); out: BF16 channels-last
-// [n^3][COP] with GELU (LAST = false) or FP32 planar tau (LAST = true).
+// BF16 [27][CP/8][COP][8] (UMMA K-major planes per tap); output per MODE.
 // Each CTA walks a contiguous run of x-rows (y fastest), software-pipelined
 // with one CTA barrier per row and three warp roles:
 //  - warp 0, one thread: issues the 27 x CP/16 MMAs of row y into one of two
@@ -126,17 +146,17 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 //  - warps 1-3: once the MMAs of row y-1 are done, fetch row y+3 with cp.async
 //    into the ring slot that row y-2 left (kSlots y-slots per z-offset; row
 //    y+2 is already resident, so each fetch has two rows of time to land);
-//  - warps 4-11 (two per tensor-memory lane quadrant): the bias + GELU
-//    epilogue of row y-1 from the other accumulator, while row y computes.
+//  - warps 4-11 (two per tensor-memory lane quadrant): the epilogue of row
+//    y-1 from the other accumulator, while row y computes.
 // A change of z-plane drains the pipeline and restages the new plane.
 constexpr int kSlots = 5;
 constexpr int kConvThreads = 384;
 
-template <int CP, int COP, bool LAST>
+template <int KN, int CP, int COP, int MODE>
 __global__ void __launch_bounds__(kConvThreads, 1)
 k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restrict__ wgt,
-        const float* __restrict__ bias, __nv_bfloat16* __restrict__ act_out, const TauPtrs tau_out,
-        int* __restrict__ err) {
+        const float* __restrict__ bias, const ConvOut out, int* __restrict__ err) {
+  constexpr int kRowPlane = row_plane<KN>();
   constexpr int CPC = CP / 8;              // 16-byte channel chunks
   constexpr int PLANE_ROW = CPC * kRowPlane;
   constexpr int SIN = 3 * kSlots * PLANE_ROW;  // [zr][slot] staged rows
@@ -150,16 +170,17 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SIN + SW + 16);
   const int tid = threadIdx.x, warp = tid / 32;
   const bool is_stage = warp >= 1 && warp < 4;
-  // epilogue warps: lane quadrant warp % 4, columns ecol0 .. ecol0 + 15
+  // epilogue warps: lane quadrant warp % 4 (rows 32 (warp % 4) ..), columns ecol0 .. ecol0 + 15
   const int lane_base = 32 * (warp % 4);
   const int ecol0 = warp >= 8 ? COP / 2 : 0;
-  const bool is_epi = warp >= 4 && (COP / 2 == 16 || warp < 8);
+  const bool is_epi = warp >= 4 && (COP / 2 == 16 || warp < 8) && lane_base < KN;
 
   for (int i = tid; i < SW / 16; i += blockDim.x)
     reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(wgt) + i);
   float bia[16];
 #pragma unroll
-  for (int c = 0; c < 16; ++c) bia[c] = (is_epi && (!LAST || c < 6)) ? __ldg(bias + ecol0 + c) : 0.f;
+  for (int c = 0; c < 16; ++c)
+    bia[c] = (is_epi && MODE != kLinear && (MODE != kTau || c < 6)) ? __ldg(bias + ecol0 + c) : 0.f;
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + 1)));
@@ -181,16 +202,16 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   // copy x-rows ylo..yhi of the three z-offsets of plane z into their ring slots
   auto stage = [&](int z, int ylo, int yhi, int t0, int tstride) {
     const int nyr = yhi - ylo + 1;
-    const int chunks = 3 * nyr * (kN + 2) * CPC;
+    const int chunks = 3 * nyr * (KN + 2) * CPC;
     for (int i = t0; i < chunks; i += tstride) {
       const int kc = i % CPC;
-      const int xi = (i / CPC) % (kN + 2);
-      const int q = i / (CPC * (kN + 2));
+      const int xi = (i / CPC) % (KN + 2);
+      const int q = i / (CPC * (KN + 2));
       const int zr = q / nyr, yv = ylo + q % nyr;
-      const int zz = (z + zr - 1 + kN) % kN, yy = (yv + kN) % kN;
-      const int x = (xi - 1 + kN) % kN;
-      const long long vox = ((long long)zz * kN + yy) * kN + x;
-      unsigned char* dst = s_in + (zr * kSlots + (yv + kN) % kSlots) * PLANE_ROW + kc * kRowPlane + xi * 16;
+      const int zz = (z + zr - 1 + KN) % KN, yy = (yv + KN) % KN;
+      const int x = (xi - 1 + KN) % KN;
+      const long long vox = ((long long)zz * KN + yy) * KN + x;
+      unsigned char* dst = s_in + (zr * kSlots + (yv + KN) % kSlots) * PLANE_ROW + kc * kRowPlane + xi * 16;
       cp_async16(dst, reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
     }
   };
@@ -201,22 +222,35 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     asm volatile("tcgen05.fence::after_thread_sync;");
     return r;
   };
-  // bias + activation of row prow from accumulator buffer b (epilogue warps)
+  // epilogue of row prow from accumulator buffer b (epilogue warps)
   auto epilogue = [&](int prow, int b) {
     if (!is_epi) return;
     float v[16];
     tmem_ld<16>(tmem + (uint32_t(lane_base) << 16) + uint32_t(b * 32 + ecol0), v);
-    const long long vox = (long long)prow * kN + lane_base + tid % 32;
-    if (!LAST) {
+    const long long vox = (long long)prow * KN + lane_base + tid % 32;
+    if (MODE == kGelu || MODE == kGeluSave) {
       __align__(16) __nv_bfloat16 o[16];
+      __align__(16) float h[16];
 #pragma unroll
-      for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16_rn(gelu(v[c] + bia[c]));
-      uint4* dst = reinterpret_cast<uint4*>(act_out + vox * COP + ecol0);
+      for (int c = 0; c < 16; ++c) {
+        h[c] = v[c] + bia[c];
+        o[c] = __float2bfloat16_rn(gelu(h[c]));
+      }
+      uint4* dst = reinterpret_cast<uint4*>(out.act + vox * COP + ecol0);
       dst[0] = reinterpret_cast<uint4*>(o)[0];
       dst[1] = reinterpret_cast<uint4*>(o)[1];
-    } else {
+      if (MODE == kGeluSave) {
+        float4* ph = reinterpret_cast<float4*>(out.pre + vox * COP + ecol0);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) tau_out.p[c][vox] = v[c] + bia[c];
+        for (int j = 0; j < 4; ++j) ph[j] = reinterpret_cast<float4*>(h)[j];
+      }
+    } else if (MODE == kTau) {
+#pragma unroll
+      for (int c = 0; c < 6; ++c) out.tau.p[c][vox] = v[c] + bia[c];
+    } else {
+      float4* pl = reinterpret_cast<float4*>(out.pre + vox * COP + ecol0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pl[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
   };
   // wait for buffer b everywhere, run its epilogue, barrier; false on a timeout
@@ -230,14 +264,14 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     return all;
   };
 
-  const int nrows = kN * kN;
+  const int nrows = KN * KN;
   const int per = (nrows + gridDim.x - 1) / gridDim.x;
   const int rbeg = blockIdx.x * per;
   const int rend = min(rbeg + per, nrows);
   int cur_z = -1;
   int pending = -1;  // row whose accumulator still needs its epilogue
   for (int row = rbeg; row < rend; ++row) {
-    const int y = row % kN, z = row / kN;
+    const int y = row % KN, z = row / KN;
     if (z != cur_z) {
       // new plane: drain, then stage rows y-1 .. y+2 as one group (all threads)
       if (pending >= 0) {
@@ -245,7 +279,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
         pending = -1;
         if (!ok) break;
       }
-      stage(z, y - 1, min(y + 2, kN), tid, kConvThreads);
+      stage(z, y - 1, min(y + 2, KN), tid, kConvThreads);
       commit();
       cur_z = z;
       asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -264,7 +298,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
       const uint32_t dcol = tmem + uint32_t(b * 32);
       uint32_t sl[3];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) sl[d] = uint32_t((y + d - 1 + kN) % kSlots) * (PLANE_ROW >> 4);
+      for (int d = 0; d < 3; ++d) sl[d] = uint32_t((y + d - 1 + KN) % kSlots) * (PLANE_ROW >> 4);
 #pragma unroll
       for (int t = 0; t < 27; ++t) {
         const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
@@ -283,7 +317,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     if (pending >= 0 && warp != 0) mine = wait_buf(pending & 1);  // the last readers of row y-2's slot
     // prefetch row y+3 (read first by the MMAs of row y+2, when this CTA runs
     // that row in this plane); every thread commits a group, empty or not
-    if (is_stage && mine && y + 2 < kN && row + 2 < rend) stage(z, y + 3, y + 3, tid - 32, 96);
+    if (is_stage && mine && y + 2 < KN && row + 2 < rend) stage(z, y + 3, y + 3, tid - 32, 96);
     commit();
     if (pending >= 0 && mine) epilogue(pending, pending & 1);
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -330,38 +364,240 @@ __global__ void k_cnn_redelta(const double* a2, double* z, double delta, double 
   *z = (log(re) - mu) / sigma;
 }
 
-template <int CP, int COP, bool LAST> static size_t conv_smem() {
-  return size_t(3 * kSlots) * (CP / 8) * kRowPlane + size_t(27) * (CP / 8) * COP * 16 + 32;
+// ---------------------------------------------------------------------------
+// backward pass helpers
+// ---------------------------------------------------------------------------
+// dL/dtau (6 planar FP32) -> BF16 channels-last [n^3][16] (channels 6..15 zero)
+__global__ void k_gtau_cl(TauPtrs g, __nv_bfloat16* __restrict__ out, long long npts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  __align__(16) __nv_bfloat16 o[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) o[c] = __float2bfloat16_rn(c < 6 ? g.p[c][i] : 0.f);
+  uint4* dst = reinterpret_cast<uint4*>(out + i * 16);
+  dst[0] = reinterpret_cast<uint4*>(o)[0];
+  dst[1] = reinterpret_cast<uint4*>(o)[1];
 }
 
-template <int CP, int COP, bool LAST> static void conv_attr() {
-  cudaFuncSetAttribute(k_conv3<CP, COP, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(conv_smem<CP, COP, LAST>()));
+// g_pre = BF16(g_post * gelu'(h)), channels-last [n^3][32]
+__global__ void k_gelu_bwd_cl(const float* __restrict__ gpost, const float* __restrict__ h,
+                              __nv_bfloat16* __restrict__ out, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = __float2bfloat16_rn(gpost[i] * gelu_grad(h[i]));
 }
 
-bool cnn_supported(int n, int D) { return n == kN && D == 3; }
+// FP32 channels-last [n^3][16] -> planar channels 0..3 (dL/dv and the z channel)
+__global__ void k_gin_planar(const float* __restrict__ gin, const GinPtrs o, long long npts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const float4 v = *reinterpret_cast<const float4*>(gin + i * 16);
+  o.p[0][i] = v.x; o.p[1][i] = v.y; o.p[2][i] = v.z; o.p[3][i] = v.w;
+}
+
+// Weight and bias gradients of one layer (CUDA cores, FP32 accumulation,
+// FP64 atomics into the flat parameter gradient):
+//   gw[co][ci][t] += sum_v g[v][co] a[v + off(t)][ci],  gb[co] += sum_v g[v][co]
+// for co < cout, ci < cin.  Block (tap t, chunk of voxels); a group of
+// (COP/4)(CP/4) threads holds a 4 x 4 (co, ci) register tile; the chunk's g
+// rows and shifted a rows are staged in shared memory 64 voxels at a time.
+template <int KN, int CP, int COP>
+__global__ void __launch_bounds__(256)
+k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ a, int cin, int cout,
+             int vchunk, double* __restrict__ gw, double* __restrict__ gb) {
+  constexpr int TG = (COP / 4) * (CP / 4);  // threads per group
+  constexpr int NG = 256 / TG;              // groups (split the voxels of a stage)
+  constexpr int VS = 64;                    // voxels per stage
+  constexpr long long NPTS = (long long)KN * KN * KN;
+  __shared__ __align__(16) float sg[VS][COP + 4];
+  __shared__ __align__(16) float sa[VS][CP + 4];
+  __shared__ float red[256][17];
+  const int t = blockIdx.x;  // tap
+  const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+  const int tid = threadIdx.x, grp = tid / TG, lt = tid % TG;
+  const int co0 = 4 * (lt / (CP / 4)), ci0 = 4 * (lt % (CP / 4));
+  float acc[4][4] = {};
+  float accb[4] = {};
+  const long long v0 = (long long)blockIdx.y * vchunk;
+  const long long v1 = min(v0 + vchunk, NPTS);
+  for (long long vb = v0; vb < v1; vb += VS) {
+    // stage g rows and shifted a rows (BF16 -> FP32)
+    for (int i = tid; i < VS * (COP + CP) / 2; i += 256) {
+      const int pairs_g = VS * COP / 2;
+      if (i < pairs_g) {
+        const int vv = i / (COP / 2), c = 2 * (i % (COP / 2));
+        const long long v = vb + vv;
+        float2 f = make_float2(0.f, 0.f);
+        if (v < v1) f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(g + v * COP + c));
+        sg[vv][c] = f.x; sg[vv][c + 1] = f.y;
+      } else {
+        const int j = i - pairs_g;
+        const int vv = j / (CP / 2), c = 2 * (j % (CP / 2));
+        const long long v = vb + vv;
+        float2 f = make_float2(0.f, 0.f);
+        if (v < v1) {
+          const int x = int(v % KN), y = int((v / KN) % KN), z = int(v / ((long long)KN * KN));
+          const long long q = ((long long)((z + dz + KN) % KN) * KN + (y + dy + KN) % KN) * KN + (x + dx + KN) % KN;
+          f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(a + q * CP + c));
+        }
+        sa[vv][c] = f.x; sa[vv][c + 1] = f.y;
+      }
+    }
+    __syncthreads();
+    for (int vv = grp; vv < VS; vv += NG) {
+      const float4 gg = *reinterpret_cast<const float4*>(&sg[vv][co0]);
+      const float4 aa = *reinterpret_cast<const float4*>(&sa[vv][ci0]);
+      const float gv[4] = {gg.x, gg.y, gg.z, gg.w}, av[4] = {aa.x, aa.y, aa.z, aa.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += gv[i] * av[j];
+        accb[i] += gv[i];
+      }
+    }
+    __syncthreads();
+  }
+  // reduce the groups, then one FP64 atomic per gradient entry
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) red[tid][4 * i + j] = acc[i][j];
+    red[tid][16] = 0.f;
+  }
+  __syncthreads();
+  if (grp == 0) {
+    for (int k = 1; k < NG; ++k)
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc[e / 4][e % 4] += red[k * TG + lt][e];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int co = co0 + i, ci = ci0 + j;
+        if (co < cout && ci < cin) atomicAdd(&gw[((long long)co * cin + ci) * 27 + t], double(acc[i][j]));
+      }
+  }
+  __syncthreads();
+  if (t == 13 && ci0 == 0) {  // bias gradient once (centre tap), from the same g rows
+#pragma unroll
+    for (int i = 0; i < 4; ++i) red[tid][i] = accb[i];
+  }
+  __syncthreads();
+  if (t == 13 && grp == 0 && ci0 == 0) {
+    for (int k = 1; k < NG; ++k)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) accb[i] += red[k * TG + lt][i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (co0 + i < cout) atomicAdd(&gb[co0 + i], double(accb[i]));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <int KN, int CP, int COP, int MODE> static size_t conv_smem() {
+  return size_t(3 * kSlots) * (CP / 8) * row_plane<KN>() + size_t(27) * (CP / 8) * COP * 16 + 32;
+}
+
+template <int KN, int CP, int COP, int MODE> static void conv_attr() {
+  cudaFuncSetAttribute(k_conv3<KN, CP, COP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       int(conv_smem<KN, CP, COP, MODE>()));
+}
+
+template <int KN, int CP, int COP, int MODE>
+static void conv_launch(int grid, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* b, const ConvOut& o,
+                        int* err, cudaStream_t st) {
+  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(in, w, b, o, err);
+}
+
+bool cnn_supported(int n, int D) { return (n == 64 || n == 128) && D == 3; }
 
 void launch_redelta(const double* a2, double* z, double delta, double nu, double mu, double sigma, cudaStream_t st) {
   k_cnn_redelta<<<1, 1, 0, st>>>(a2, z, delta, nu, mu, sigma);
 }
 
+template <int KN> static void cnn_init_n() {
+  conv_attr<KN, 16, 32, kGelu>();
+  conv_attr<KN, 32, 32, kGelu>();
+  conv_attr<KN, 32, 16, kTau>();
+  conv_attr<KN, 16, 32, kGeluSave>();
+  conv_attr<KN, 32, 32, kGeluSave>();
+  conv_attr<KN, 16, 32, kLinear>();
+  conv_attr<KN, 32, 32, kLinear>();
+  conv_attr<KN, 32, 16, kLinear>();
+}
+
 void cnn_init() {
-  conv_attr<16, 32, false>();
-  conv_attr<32, 32, false>();
-  conv_attr<32, 16, true>();
+  cnn_init_n<64>();
+  cnn_init_n<128>();
+}
+
+static unsigned nblk(long long n) { return unsigned((n + 255) / 256); }
+
+template <int KN> static void cnn_forward_n(const CnnArgs& a, cudaStream_t st) {
+  const long long npts = (long long)KN * KN * KN;
+  k_cnn_redelta<<<1, 1, 0, st>>>(a.a2, a.z, a.delta, a.nu, a.mu, a.sigma);
+  k_cnn_input<<<nblk(npts), 256, 0, st>>>(static_cast<const float*>(a.u[0]), static_cast<const float*>(a.u[1]),
+                                          static_cast<const float*>(a.u[2]), a.z, a.act0, npts);
+  const int grid = a.nsm > 0 ? a.nsm : 148;
+  ConvOut o1{}, o2{}, o3{}, o4{};
+  o1.act = a.act1; o1.pre = a.pre[0];
+  o2.act = a.act2; o2.pre = a.pre[1];
+  __nv_bfloat16* a3 = a.act3 ? a.act3 : a.act1;
+  o3.act = a3; o3.pre = a.pre[2];
+  o4.tau = a.tau;
+  if (a.pre[0]) {
+    conv_launch<KN, 16, 32, kGeluSave>(grid, a.act0, a.w[0], a.b[0], o1, a.err, st);
+    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act1, a.w[1], a.b[1], o2, a.err, st);
+    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act2, a.w[2], a.b[2], o3, a.err, st);
+  } else {
+    conv_launch<KN, 16, 32, kGelu>(grid, a.act0, a.w[0], a.b[0], o1, a.err, st);
+    conv_launch<KN, 32, 32, kGelu>(grid, a.act1, a.w[1], a.b[1], o2, a.err, st);
+    conv_launch<KN, 32, 32, kGelu>(grid, a.act2, a.w[2], a.b[2], o3, a.err, st);
+  }
+  conv_launch<KN, 32, 16, kTau>(grid, a3, a.w[3], a.b[3], o4, a.err, st);
 }
 
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st) {
-  const long long npts = (long long)kN * kN * kN;
-  k_cnn_redelta<<<1, 1, 0, st>>>(a.a2, a.z, a.delta, a.nu, a.mu, a.sigma);
-  k_cnn_input<<<unsigned((npts + 255) / 256), 256, 0, st>>>(
-      static_cast<const float*>(a.u[0]), static_cast<const float*>(a.u[1]), static_cast<const float*>(a.u[2]), a.z,
-      a.act0, npts);
+  if (a.n == 64) cnn_forward_n<64>(a, st);
+  else cnn_forward_n<128>(a, st);
+}
+
+template <int KN, int CP, int COP>
+static void wgrad_launch(const __nv_bfloat16* g, const __nv_bfloat16* act, int cin, int cout, double* gw, double* gb,
+                         cudaStream_t st) {
+  constexpr long long npts = (long long)KN * KN * KN;
+  const int vchunk = 4096;
+  dim3 grid(27, unsigned((npts + vchunk - 1) / vchunk));
+  k_conv_wgrad<KN, CP, COP><<<grid, 256, 0, st>>>(g, act, cin, cout, vchunk, gw, gb);
+}
+
+template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t st) {
+  const long long npts = (long long)KN * KN * KN;
   const int grid = a.nsm > 0 ? a.nsm : 148;
-  const TauPtrs none{};
-  k_conv3<16, 32, false><<<grid, kConvThreads, conv_smem<16, 32, false>(), st>>>(a.act0, a.w[0], a.b[0], a.act1, none, a.err);
-  k_conv3<32, 32, false><<<grid, kConvThreads, conv_smem<32, 32, false>(), st>>>(a.act1, a.w[1], a.b[1], a.act2, none, a.err);
-  k_conv3<32, 32, false><<<grid, kConvThreads, conv_smem<32, 32, false>(), st>>>(a.act2, a.w[2], a.b[2], a.act1, none, a.err);
-  k_conv3<32, 16, true><<<grid, kConvThreads, conv_smem<32, 16, true>(), st>>>(a.act1, a.w[3], a.b[3], nullptr, a.tau, a.err);
+  // layer 4: g4 = dL/dtau (BF16 [v][16]); input gradient through W4^T; weight gradient against act3
+  k_gtau_cl<<<nblk(npts), 256, 0, st>>>(a.gtau, a.gbf, npts);
+  wgrad_launch<KN, 32, 16>(a.gbf, a.act[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st);
+  ConvOut o{};
+  o.pre = a.gf;
+  conv_launch<KN, 16, 32, kLinear>(grid, a.gbf, a.wt[3], nullptr, o, a.err, st);
+  // layers 3, 2: g_pre = g_post * gelu'(h); input and weight gradients
+  for (int l = 2; l >= 1; --l) {
+    k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[l], a.gbf, npts * 32);
+    wgrad_launch<KN, 32, 32>(a.gbf, a.act[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st);
+    conv_launch<KN, 32, 32, kLinear>(grid, a.gbf, a.wt[l], nullptr, o, a.err, st);
+  }
+  // layer 1: input gradient into 16 channels (4 used), then planar
+  k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[0], a.gbf, npts * 32);
+  wgrad_launch<KN, 16, 32>(a.gbf, a.act[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st);
+  conv_launch<KN, 32, 16, kLinear>(grid, a.gbf, a.wt[0], nullptr, o, a.err, st);
+  k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);
+}
+
+void launch_cnn_backward(const CnnBwdArgs& a, cudaStream_t st) {
+  if (a.n == 64) cnn_backward_n<64>(a, st);
+  else cnn_backward_n<128>(a, st);
 }
 
 }  // namespace sc

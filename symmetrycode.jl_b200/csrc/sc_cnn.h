@@ -9,13 +9,20 @@ struct TauPtrs {
   float* p[6];
 };
 
+struct GinPtrs {
+  float* p[4];
+};
+
 struct CnnArgs {
-  const void* u[3];            // physical velocity (FP32, 128^3)
+  int n;                       // 64 or 128
+  const void* u[3];            // physical velocity (FP32, n^3)
   const __nv_bfloat16* w[4];   // packed weights per layer
   const float* b[4];           // biases per layer (padded)
   __nv_bfloat16* act0;         // [n^3][16]
   __nv_bfloat16* act1;         // [n^3][32]
   __nv_bfloat16* act2;         // [n^3][32]
+  __nv_bfloat16* act3;         // [n^3][32] input of layer 4; null: act1 is reused
+  float* pre[3];               // FP32 [n^3][32] pre-activations of layers 1-3 (kept for the adjoint), or null
   TauPtrs tau;                 // 6 physical FP32 outputs
   const double* a2;            // <|grad u|^2> (device, FP64)
   double* z;                   // device scalar for the Re_Delta channel
@@ -24,9 +31,29 @@ struct CnnArgs {
   int nsm;
 };
 
+// Backward pass of the network after a forward pass that kept act0..act3 and
+// the pre-activations: from dL/dtau to dL/d(input channels) and the weight and
+// bias gradients (accumulated in FP64 into gw at the flat offsets woff[l]:
+// [Cout][Cin][27] weights, then [Cout] biases, PyTorch order).
+struct CnnBwdArgs {
+  int n;
+  TauPtrs gtau;                       // dL/dtau, 6 planar FP32
+  const __nv_bfloat16* wt[4];         // packed transposed, flipped weights per layer
+  const __nv_bfloat16* act[4];        // layer inputs (BF16 channels-last)
+  const float* pre[3];                // pre-activations h1..h3
+  __nv_bfloat16* gbf;                 // scratch BF16 [n^3][32]
+  float* gf;                          // scratch FP32 [n^3][32]
+  GinPtrs gin_planar;                 // out: dL/d(u_x, u_y, u_z, z channel), planar FP32
+  double* gw;
+  long long woff[4];
+  int* err;
+  int nsm;
+};
+
 bool cnn_supported(int n, int D);
 void cnn_init();
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st);
+void launch_cnn_backward(const CnnBwdArgs& a, cudaStream_t st);
 // *z = (log(delta^2 sqrt(*a2) / nu) - mu) / sigma
 void launch_redelta(const double* a2, double* z, double delta, double nu, double mu, double sigma, cudaStream_t st);
 

@@ -63,3 +63,57 @@ def test_les_rhs_with_cnn_adds_divergence_of_tau(setup):
     extra = O.tensordivergence(sig, go)
     diff = [to_np(a) - to_np(b) for a, b in zip(du_c, du_0)]
     assert rel_l2(diff, [O.twothirds(e, go) for e in extra]) < 1e-4
+
+
+def test_cnn_closure_64_matches_oracle():
+    """n = 64: M = 128 tiles of which rows 0..63 are the x-row."""
+    n = 64
+    g, go = S.Grid(3, n, dtype=torch.float32, device="cuda:0"), O.Grid(3, n)
+    u = O.random_field(go, seed=41, kpeak=3)
+    delta, nu = 4 * go.l / n, 1e-3
+    ws, bs = S.kaiming_cnn_weights(8)
+    bs = [b + 0.05 * np.arange(b.size, dtype=np.float32) for b in bs]
+    cl = S.create_cnn_closure(delta, nu, g, ws, bs, mu=1.0, sigma=2.0)
+    ut = [to_dev(c, g) for c in u]
+    tau = to_np(cl(ut, None))
+    uphys = np.stack([to_np(S.to_phys_(S.spacescalarfield(g), c, g)) for c in ut], 0)
+    zval = O.cnn_redelta_channel(u, go, delta, nu, mu=1.0, sigma=2.0)
+    rows = [(0, 0), (17, 5), (63, 63), (31, 40)]
+    ref = O.cnn_rows(uphys, zval, ws, bs, rows)
+    got = np.stack([tau[:, z, y, :] for (y, z) in rows], 1)
+    assert np.isfinite(got).all()
+    assert rel_l2(got, ref) < 5e-3
+    # the parameter vector round-trips: setting the same weights gives the same stress
+    S.closure_set_params(cl, S.pack_cnn_params(ws, bs))
+    assert rel_l2(to_np(cl(ut, None)), tau) < 1e-7
+
+
+@pytest.mark.parametrize("target_scale", [1.3])
+def test_tensor_core_adjoint_matches_fp64_gradient(target_scale):
+    """The BF16 tensor-core adjoint (roundings taken as identities) against the
+    FP64 CUDA-core adjoint of the same network on the same rollout.  The target
+    closure has weights x target_scale, so the trajectory residual, which the
+    gradient is proportional to, is large against the BF16 rounding of weights
+    and activations (with a 1 % perturbation the two residuals, and hence the
+    gradients, differ by tens of percent through the rounding alone)."""
+    n, nsteps, ck, dt, nu = 64, 3, 2, 5e-3, 1e-3
+    go = O.Grid(3, n)
+    u0n = O.random_field(go, seed=42, kpeak=3)
+    ws, bs = S.kaiming_cnn_weights(9)
+    theta = S.pack_cnn_params(ws, bs)
+    theta_t = theta * target_scale
+    out = {}
+    for kind, dtype in (("tc", torch.float32), ("fp64", torch.float64)):
+        g = S.Grid(3, n, dtype=dtype, device="cuda:0")
+        u0 = [to_dev(c, g) for c in u0n]
+        make = S.create_cnn_closure if kind == "tc" else S.create_cnn_fp_closure
+        cl = make(4 * go.l / n, nu, g, ws, bs, mu=5.0, sigma=2.0)
+        S.closure_set_params(cl, theta_t)
+        traj = S.rollout_record(g, cl, u0, dt, nu, nsteps)
+        S.closure_set_params(cl, theta)
+        out[kind] = S.rollout_adjoint(g, cl, u0, traj, dt, nu, nsteps, ckpt_every=ck)
+    (l_tc, g_tc), (l_64, g_64) = out["tc"], out["fp64"]
+    assert np.isfinite(g_tc).all()
+    err = np.linalg.norm(g_tc - g_64) / np.linalg.norm(g_64)
+    assert err < 5e-2, err
+    assert abs(l_tc - l_64) <= 5e-2 * abs(l_64)
