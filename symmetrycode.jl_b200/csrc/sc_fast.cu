@@ -60,25 +60,31 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
   C* __restrict__ out = static_cast<C*>(a.out[q]);
   const bool live = kx < a.K1;
   const int Kc = a.kpos + a.kneg;
+  // element offsets fit in 32 bits for every sweep (at most ~3.5e8 elements
+  // per component), so the per-element address arithmetic stays 32-bit
+  const int ies = int(a.in_es), oes = int(a.out_es);
   if (j < N2) {
     C v[N1];
     const C* base = in + kx + (long long)c * a.in_cs;
+    if (INV) {
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) {
-      const int e = N2 * n1 + j;
-      v[n1] = mk<C>(0.f, 0.f);
-      if (INV) {
+      for (int n1 = 0; n1 < N1; ++n1) {
+        const int e = N2 * n1 + j;
+        v[n1] = mk<C>(0.f, 0.f);
         const int p = cpos(e, N, a.kpos, a.kneg);
         if (live && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
-          v[n1] = __ldg(base + (long long)p * a.in_es);
+          v[n1] = __ldg(base + p * ies);
           if (drv) {
             const float kk = float(a.kfac * double(p < a.kpos ? p : p - Kc));
             v[n1] = mk<C>(-kk * v[n1].y, kk * v[n1].x);
           }
         }
-      } else if (live) {
-        v[n1] = __ldg(base + (long long)e * a.in_es);
       }
+    } else {
+      const C* bj = base + j * ies;
+      const int st = N2 * ies;
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) v[n1] = live ? __ldg(bj + n1 * st) : mk<C>(0.f, 0.f);
     }
     DFT<N1, INV, C>::run(v);
 #pragma unroll
@@ -97,14 +103,19 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
     for (int n2 = 0; n2 < N2; ++n2) w[n2] = ys[j * SR + n2 * T + t];
     DFT<N2, INV, C>::run(w);
     C* obase = out + kx + (long long)c * a.out_cs;
+    if (INV) {
+      C* oj = obase + j * oes;
+      const int st = N1 * oes;
 #pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) {
-      const int e = j + N1 * k2;
-      if (INV) {
-        obase[(long long)e * a.out_es] = w[k2];
-      } else {
-        const int p = cpos(e, N, a.kpos, a.kneg);
-        if (p >= 0) obase[(long long)p * a.out_es] = w[k2];
+      for (int k2 = 0; k2 < N2; ++k2) oj[k2 * st] = w[k2];
+    } else {
+      // retained e = j + N1 k2: e < kpos keeps its index, e >= N - kneg moves down by N - Kc
+      const int shift = N - Kc;
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) {
+        const int e = j + N1 * k2;
+        if (e < a.kpos) obase[e * oes] = w[k2];
+        else if (e >= N - a.kneg) obase[(e - shift) * oes] = w[k2];
       }
     }
   }
