@@ -311,6 +311,63 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
     }
 
 
+def filter_measure(dev, g, st_state, reps=3):
+    """configs[2]'s filter call: sfs! of the 810^3 FP32 state to 128^3 at
+    Delta/h in {2, 4, 8} (ubar 3 + tau 6 per Delta, FP32), device-timed."""
+    import torch
+    import symcode as S
+    gl = S.Grid(3, 128, dtype=torch.float32, device=dev)
+    u = [S.scalarfield(g) for _ in range(3)]
+    st_state.store(u)
+    deltas = [dh * gl.l / 128 for dh in (2, 4, 8)]
+    ubar = [[S.scalarfield(gl) for _ in range(3)] for _ in deltas]
+    tau = [[S.scalarfield(gl) for _ in range(6)] for _ in deltas]
+    S.sfs_(ubar, tau, u, g, gl, deltas)  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        S.sfs_(ubar, tau, u, g, gl, deltas)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ok = all(bool(torch.isfinite(t).all()) for grp in tau for t in grp)
+    del u, ubar, tau
+    gl.close()
+    torch.cuda.empty_cache()
+    return {"metric": "sfs! 810^3 -> 128^3, Delta/h in {2,4,8} (one call, all three filters)", "ms": ms,
+            "calls_per_s": 1e3 / ms, "finite": ok}
+
+
+def fp32_vs_fp64_measure(dev, n=256, nsteps=100, every=10):
+    """256^3 forced DNS (nu=2e-3, dt=2e-3, eps=0.1, k_p=4, seed 1) run
+    in FP32 and FP64 side by side; relative L2 error of the FP32 state every
+    `every` steps."""
+    import torch
+    import symcode as S
+    uc = initial_compact(n, 1)
+    g32 = S.Grid(3, n, dtype=torch.float32, device=dev)
+    g64 = S.Grid(3, n, dtype=torch.float64, device=dev)
+    s32, s64 = S.State(g32), S.State(g64)
+    s32.load([c.to(dev) for c in to_full(uc, n, torch.float32)])
+    s64.load([c.to(dev) for c in to_full(uc, n, torch.float64)])
+    u32, u64 = [S.scalarfield(g32) for _ in range(3)], [S.scalarfield(g64) for _ in range(3)]
+    errs = []
+    for k in range(nsteps // every):
+        s32.rk4(2e-3, 2e-3, every, 0.1)
+        s64.rk4(2e-3, 2e-3, every, 0.1)
+        s32.store(u32)
+        s64.store(u64)
+        num = sum(float((a.to(torch.complex128) - b).abs().pow(2).sum()) for a, b in zip(u32, u64))
+        den = sum(float(b.abs().pow(2).sum()) for b in u64)
+        errs.append(math.sqrt(num / den))
+    g32.close()
+    g64.close()
+    torch.cuda.empty_cache()
+    return {"config": f"{n}^3 forced DNS, nu=2e-3, dt=2e-3, eps=0.1, k_p=4, seed 1, {nsteps} RK4 steps",
+            "every_steps": every, "rel_l2_fp32_vs_fp64": errs}
+
+
 ADJ_N, ADJ_NU, ADJ_DH, ADJ_DT, ADJ_SEED = 64, (1e-3, 5e-4), 4, 5e-3, 5
 
 
@@ -512,6 +569,11 @@ def run_gpu(args):
     if rank == 0 and not args.skip_les:
         les = les_batch_measure(dev, args.les_steps, 3)
 
+    filt = c1 = None
+    if rank == 0 and not args.skip_extra:
+        filt = filter_measure(dev, g, st)
+        c1 = fp32_vs_fp64_measure(dev)
+
     adj = None
     if rank == 0 and not args.skip_adj:
         adj = les_adjoint_measure(dev, args.adj_steps, 5)
@@ -545,6 +607,8 @@ def run_gpu(args):
             "clocks": clocks,
             "les_batch": les,
             "les_adjoint": adj,
+            "filter": filt,
+            "fp32_vs_fp64_256": c1,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -567,6 +631,7 @@ def main():
     ap.add_argument("--skip-les", action="store_true")
     ap.add_argument("--les-steps", type=int, default=10)
     ap.add_argument("--skip-adj", action="store_true")
+    ap.add_argument("--skip-extra", action="store_true", help="skip the filter and 256^3 FP32-vs-FP64 legs")
     ap.add_argument("--adj-steps", type=int, default=40)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
