@@ -117,4 +117,73 @@ function energy(u, p::Plan)
     return e[]
 end
 
+"`propose_timestep(u, grid, visc, cache)` (src/solver.jl:931-947), without the `cfl` factor."
+function propose_timestep(u, p::Plan, visc)
+    dt = Ref{Cdouble}(0)
+    check(ccall((:sc_propose_timestep, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cdouble, Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, ptrs(u), visc, dt, stream()))
+    return dt[]
+end
+
+"`spectrum(u, grid)` (src/solver.jl:693-699) on shells 1..nshell."
+function spectrum(u, p::Plan, nshell::Integer)
+    s = zeros(Cdouble, nshell)
+    check(ccall((:sc_spectrum, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cint, Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, ptrs(u), nshell, s, stream()))
+    return s
+end
+
+"""
+CNN closure (new): `ws[l]`, `bs[l]` in PyTorch conv3d order (Cout, Cin, 3, 3, 3),
+flattened column-major as Julia stores `permutedims(w, (5, 4, 3, 2, 1))`.
+`tensorcores = true` selects the tcgen05 BF16 network (FP32 plans, n = 64 or 128).
+"""
+function create_cnn(Δ, visc, p::Plan, ws::Vector{Vector{Float32}}, bs::Vector{Vector{Float32}};
+                    mu = 0.0, sigma = 1.0, tensorcores = true)
+    ref = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve ws bs begin
+        wp = [pointer(w) for w in ws]
+        bp = [pointer(b) for b in bs]
+        f = tensorcores ? :sc_cnn_closure_create : :sc_cnn_fp_closure_create
+        check(ccall((f, LIB), Cint,
+            (Ptr{Ptr{Cvoid}}, Ptr{Cvoid}, Cdouble, Cdouble, Ptr{Ptr{Float32}}, Ptr{Ptr{Float32}}, Cdouble, Cdouble),
+            ref, p.ptr, Δ, visc, wp, bp, mu, sigma))
+    end
+    c = Closure(ref[], p)
+    finalizer(c -> ccall((:sc_closure_destroy, LIB), Cint, (Ptr{Cvoid},), c.ptr), c)
+    return c
+end
+
+"The CNN's flat parameter vector θ (weights then biases per layer)."
+function set_params!(c::Closure, θ::Vector{Float64})
+    check(ccall((:sc_closure_set_params, LIB), Cint, (Ptr{Cvoid}, Ptr{Cdouble}), c.ptr, θ))
+    return c
+end
+function num_params(c::Closure)
+    n = Ref{Clonglong}(0)
+    check(ccall((:sc_closure_num_params, LIB), Cint, (Ptr{Cvoid}, Ptr{Clonglong}), c.ptr, n))
+    return Int(n[])
+end
+
+"Trajectory of `nsteps` RK4 steps with closure `c` (device bytes, compact states)."
+function rollout_record(c::Closure, u0, p::Plan; Δt, visc, nsteps)
+    nb = ccall((:sc_rollout_traj_bytes, LIB), Csize_t, (Ptr{Cvoid}, Cint), p.ptr, nsteps)
+    traj = CuArray{UInt8}(undef, nb)
+    check(ccall((:sc_rollout_record, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cdouble, Cdouble, Cint, CuPtr{Cvoid}, Ptr{Cvoid}),
+        p.ptr, c.ptr, ptrs(u0), Δt, visc, nsteps, pointer(traj), stream()))
+    return traj
+end
+
+"(loss, dloss/dθ) of the trajectory MSE against `traj` by the hand-written adjoint."
+function rollout_adjoint(c::Closure, u0, traj, p::Plan; Δt, visc, nsteps, ckpt_every = 5)
+    loss = Ref{Cdouble}(0)
+    grad = zeros(Cdouble, num_params(c))
+    check(ccall((:sc_rollout_adjoint, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, CuPtr{Cvoid}, Cdouble, Cdouble, Cint, Cint, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, c.ptr, ptrs(u0), pointer(traj), Δt, visc, nsteps, ckpt_every, loss, grad, stream()))
+    return loss[], grad
+end
+
 end # module
