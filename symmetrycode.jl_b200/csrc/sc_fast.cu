@@ -1076,8 +1076,11 @@ k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles
         }
       }
     }
-    // the next tile's pass A writes xs only after this barrier; pass C here reads ys
-    __syncthreads();
+    // No barrier here: the next tile's stage copies go to the buffer whose
+    // readers (pass A of the previous tile) finished before the A->B barrier
+    // of this tile; its pass A writes xs after its top barrier, which every
+    // thread reaches only after this tile's pass C; its pass B writes ys after
+    // two more barriers.
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
