@@ -314,6 +314,17 @@ SC_API int sc_state_maintain_shell_energy(sc_plan* plan, const double* eref, voi
  * s[i-1] = 1/2 sum_{i <= |k| < i+1} |u_hat|^2 with the RFFT double count.  Synchronous. */
 SC_API int sc_spectrum(sc_plan* plan, const void* const* u_hat, int nshell, double* s, void* stream);
 
+/* The a-posteriori reductions of one LES state in solve_les!'s reduce!
+ * (src/les.jl:94-148): out[0] = e_post = ||u - twothirds(u_ref)|| / ||twothirds(u_ref)||
+ * (0 when u_ref is null), out[1] = kinetic energy, out[2] = viscous
+ * dissipation (get_dissipation!), out[3] = eps_sfs = -mean(tau_dev : S) with
+ * the closure re-evaluated on u (0 without a closure); spec[0..nshell-1] =
+ * spectrum(u); transfer[i-1] = sum over shell i of Re(conj(u) . (-i k_j tau_dev_ij))
+ * (zeros without a closure).  1 <= nshell <= n/3.  Synchronous. */
+SC_API int sc_les_diagnostics(sc_plan* plan, sc_closure* closure, const void* const* u_hat,
+                              const void* const* uref_hat, double visc, int nshell, double* out, double* spec,
+                              double* transfer, void* stream);
+
 /* ---- diagnostics (FP64 on the device; synchronous, result to host) ------- */
 /* energy(u) (src/solver.jl:643-646): 1/2 sum_i getenergy(u_i). */
 SC_API int sc_energy(sc_plan* plan, const void* const* u_hat, double* energy, void* stream);

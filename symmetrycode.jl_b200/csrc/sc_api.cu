@@ -1742,6 +1742,60 @@ int sc_spectrum(sc_plan* p, const void* const* u, int nshell, double* s, void* s
   return SC_DTYPE_DISPATCH(p, spectrum_impl, p, p->S, nshell, s, st);
 }
 
+int sc_les_diagnostics(sc_plan* p, sc_closure* cl, const void* const* u, const void* const* uref, double visc,
+                       int nshell, double* out, double* spec, double* transfer, void* stream) {
+  if (!p || !out || !spec || !transfer || nshell < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (nshell > p->kc) return fail(SC_ERR_INVALID, "shells beyond n/3 are not retained (nshell <= %d)", p->kc);
+  if (cl && cl->p != p) return fail(SC_ERR_INVALID, "closure belongs to another plan");
+  if (cl && cl->kind == sc::kNoClosure) cl = nullptr;
+  int rc = check_ptrs(u, p->D);
+  if (!rc && uref) rc = check_ptrs(uref, p->D);
+  if (!rc) rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  auto body = [&](auto tag) -> int {
+    using R = decltype(tag);
+    double s = 0;
+    int r = energy_impl<R>(p, u, 0, 0, &s, st);
+    if (r) return r;
+    out[1] = 0.5 * s;
+    if ((r = energy_impl<R>(p, u, 0, 1, &s, st))) return r;
+    out[2] = visc * s;
+    if ((r = pack_state<R>(p, u, p->S, st))) return r;
+    if ((r = spectrum_impl<R>(p, p->S, nshell, spec, st))) return r;
+    // e_post and the closure terms accumulate into dscal[1..2] and a shell buffer
+    double* d = nullptr;
+    SC_CU(cudaMallocAsync((void**)&d, (3 + nshell) * sizeof(double), st));
+    cudaMemsetAsync(d, 0, (3 + nshell) * sizeof(double), st);
+    sc::DiagArgs a{};
+    a.D = p->D; a.n = p->n; a.kc = p->kc; a.kfac = 2.0 * M_PI / p->l;
+    for (int c = 0; c < p->D; ++c) a.u[c] = u[c];
+    if (uref) {
+      for (int c = 0; c < p->D; ++c) a.uref[c] = uref[c];
+      sc::launch_epost<R>(a, d, st);
+    }
+    if (cl) {
+      if ((r = products<R>(p, p->S, st))) { cudaFreeAsync(d, st); return r; }
+      if ((r = closure_tauhat<R>(cl, p->S, st))) { cudaFreeAsync(d, st); return r; }
+      sc::DiagArgs b = a;
+      for (int c = 0; c < p->D; ++c) b.u[c] = p->S[c];
+      for (int c = 0; c < (p->D == 3 ? 6 : 3); ++c) b.th[c] = cl->th[c];
+      sc::launch_sfs_diag<R>(b, nshell, d + 2, d + 3, st);
+    }
+    r = check_launch("les diagnostics");
+    std::vector<double> h(3 + nshell);
+    cudaMemcpyAsync(h.data(), d, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    SC_CU(cudaStreamSynchronize(st));
+    if (r) return r;
+    out[0] = uref ? std::sqrt(h[0]) / std::sqrt(h[1]) : 0.0;
+    out[3] = -h[2];
+    for (int i = 0; i < nshell; ++i) transfer[i] = h[3 + i];
+    return SC_OK;
+  };
+  return p->dtype == SC_FLOAT64 ? body(double()) : body(float());
+}
+
 size_t sc_rollout_traj_bytes(const sc_plan* p, int nsteps) {
   if (!p || nsteps < 1) return 0;
   return (size_t)nsteps * p->D * p->csz * p->esz;

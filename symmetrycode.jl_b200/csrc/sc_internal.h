@@ -134,4 +134,17 @@ template <typename R> void launch_project_full(const PackArgs& a, double kfac, c
 // Records "what: detail" (or "what") as the thread's last error string and returns code.
 int api_fail(int code, const char* what, const char* detail);
 
+// a-posteriori diagnostics of an LES state (sc_diag.cu)
+struct DiagArgs {
+  const void* u[3];     // compact state (sfs) or full layout (epost)
+  const void* uref[3];  // full layout (epost)
+  const void* th[6];    // compact closure stress spectrum (sfs)
+  int D, n, kc;
+  double kfac;
+};
+// sums[0] += ||u - twothirds(uref)||^2, sums[1] += ||twothirds(uref)||^2 (zero them first)
+template <typename R> void launch_epost(const DiagArgs& a, double* sums, cudaStream_t st);
+// *eps += sum w Re(tau_dev : conj S); T[0..nshell-1] += shell transfer (zero them first)
+template <typename R> void launch_sfs_diag(const DiagArgs& a, int nshell, double* eps, double* T, cudaStream_t st);
+
 }  // namespace sc

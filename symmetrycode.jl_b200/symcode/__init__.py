@@ -558,6 +558,20 @@ def spectrum(u, g: Grid, nshell=None, stream=None):
     return list(s)
 
 
+def les_diagnostics(u, g: Grid, model=None, uref=None, visc=0.0, nshell=None, stream=None):
+    """The a-posteriori reductions of ``solve_les!``'s ``reduce!`` (src/les.jl:94-148):
+    dict(e_post, ke, eps_visc, eps_sfs, spectrum, transfer)."""
+    nshell = nshell or g.n // 3
+    pu, _k1 = ptr_array([g._check_spec(c) for c in u])
+    pr, _k2 = ptr_array([g._check_spec(c) for c in uref]) if uref is not None else (None, None)
+    out = (ct.c_double * 4)()
+    spec = (ct.c_double * nshell)()
+    tr = (ct.c_double * nshell)()
+    check(lib().sc_les_diagnostics(g.plan, _cl(model), pu, pr, float(visc), int(nshell), out, spec, tr,
+                                   _stream_ptr(stream)))
+    return dict(e_post=out[0], ke=out[1], eps_visc=out[2], eps_sfs=out[3], spectrum=list(spec), transfer=list(tr))
+
+
 def turbulence_statistics(u, visc, g: Grid):
     """``turbulence_statistics`` (src/solver.jl:836-852) from the device FP64 reductions."""
     e = energy(u, g)

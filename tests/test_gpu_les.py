@@ -146,3 +146,30 @@ def test_les_batch_matches_single_instances_and_guard():
     b.run(2)  # the frozen instance no longer advances; the others keep going
     status2, _ = b.status()
     assert status2[:3] == [0, 0, 0]
+
+
+@pytest.mark.parametrize("kind", [None, "clark", "smagorinsky", "dynsmag"])
+def test_les_diagnostics_match_oracle(kind):
+    """reduce! of solve_les! (src/les.jl:94-148): e_post, ke, eps_visc, spectrum,
+    eps_sfs and the shell transfer, against the physical-space oracle."""
+    D, n, visc = 3, 32, 1e-3
+    g, go = S.Grid(D, n, dtype=torch.float64, device="cuda:0"), O.Grid(D, n)
+    u = [O.twothirds(c, go) for c in O.random_field(go, seed=31, kpeak=3)]
+    uref = O.random_field(go, seed=32, kpeak=3)
+    delta = 2 * go.l / n
+    if kind is None:
+        cl, model = None, None
+    else:
+        cl, m = _models(kind, delta, g, D)
+        model = lambda uu, GG: m(uu, GG, go)  # noqa: E731
+    ref = O.les_aposteriori(u, uref, go, model, visc)
+    got = S.les_diagnostics([to_dev(c, g) for c in u], g, cl, [to_dev(c, g) for c in uref], visc)
+    for k in ("e_post", "ke", "eps_visc"):
+        assert math.isclose(got[k], ref[k], rel_tol=1e-11), k
+    assert np.allclose(got["spectrum"], ref["spectrum"], rtol=1e-11, atol=1e-300)
+    if kind is None:
+        assert got["eps_sfs"] == 0 and not any(got["transfer"])
+    else:
+        assert math.isclose(got["eps_sfs"], ref["eps_sfs"], rel_tol=1e-9), (got["eps_sfs"], ref["eps_sfs"])
+        t, tr = np.array(got["transfer"]), np.array(ref["transfer"])
+        assert np.linalg.norm(t - tr) <= 1e-9 * np.linalg.norm(tr)
