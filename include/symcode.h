@@ -186,6 +186,19 @@ SC_API int sc_cnn_fp_closure_create(sc_closure** closure, sc_plan* plan, double 
                                     const float* const* weights, const float* const* biases, double mu,
                                     double sigma);
 /* Flat parameter vector of the FP32/FP64 CNN closure, layer by layer [w (C_out, C_in, 27), b (C_out)]. */
+/* fullchain(setup, mlp(...)) (src/nets.jl:311-331, 248-296): a pointwise MLP
+ * closure in the plan's precision.  Input: the velocity gradient G normalised
+ * by (|G| + eps) pointwise, channels d_b u_a with a fastest, plus the
+ * standardised log Re_Delta channel when use_redelta (append_redelta,
+ * src/data.jl:689-695, with mu, sigma); layers widths[0] -> ... -> widths[nlayers]
+ * (widths[0] = D^2 (+1), widths[nlayers] = 6 | 3, each <= 128) with GELU (NNlib's
+ * tanh form) on all but the last, which has no bias; trace removed; tau =
+ * output * Delta^2 |G|^2.  theta: per layer W[c_out][c_in] (the memory order of
+ * Lux's (c_in, c_out) PointwiseConv weight), then b[c_out] (not for the last).
+ * Kind SC_CLOSURE_MLP. */
+#define SC_CLOSURE_MLP 8
+SC_API int sc_mlp_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc, int nlayers,
+                                 const int* widths, const double* theta, int use_redelta, double mu, double sigma);
 SC_API int sc_closure_num_params(const sc_closure* closure, long long* nparams);
 SC_API int sc_closure_set_params(sc_closure* closure, const double* theta);
 /* Synchronous: SC_ERR_TIMEOUT if a bounded wait of the closure's kernels ran out. */

@@ -21,7 +21,7 @@ from .filtering import gaussianfilter
 from .spectral import (WORKERS, Grid, nonlinearity, pairs, strainrate, to_phys,
                        twothirds, make_tracefree)
 
-__all__ = ["GRAD_ORDER", "grad_matrix", "store_sym", "clark", "smagorinsky", "verstappen",
+__all__ = ["mlp_fullchain", "GRAD_ORDER", "grad_matrix", "store_sym", "clark", "smagorinsky", "verstappen",
            "bardina", "dynamic_smagorinsky", "smagorinsky_tensor", "smagorinsky_ml_mm",
            "dynsmag_coefficient", "test_filter_phys"]
 
@@ -147,3 +147,40 @@ def dynamic_smagorinsky(u, delta, g: Grid, return_coeff=False):
     if return_coeff:
         return tau, c
     return tau
+
+
+def mlp_fullchain(G, delta, visc, weights, biases, D, use_redelta=False, mu=0.0, sigma=1.0, eps=np.finfo(np.float64).eps):
+    """``fullchain(setup, mlp(...), ...)`` (src/nets.jl:311-331 wrapping
+    src/nets.jl:248-296): a pointwise MLP on the normalised velocity gradient.
+
+    ``G``: dict of physical VGT components ('xy' = d_y u_x).  Input channels are
+    G stacked with the first index fastest (xx, yx, zx, xy, ...), divided by
+    (|G| + eps) pointwise; with ``use_redelta`` the standardised
+    log Re_Delta = (log(Delta^2 sqrt(mean |G|^2) / visc) - mu) / sigma is
+    appended (``append_redelta``, src/data.jl:689-695).  Layers
+    (``PointwiseConv``, src/nets.jl:37-80): y = act(W^T x + b) with W of shape
+    (c_in, c_out); GELU (NNlib, tanh form) on every layer but the last, which
+    has no bias; the output's trace is removed and it is scaled by Delta^2 |G|^2.
+    ``weights[l]``: array (c_out, c_in); ``biases[l]``: (c_out,) or None."""
+    from .cnn import gelu
+    names = "xyz"[:D]
+    x = np.stack([G[names[a] + names[b]] for b in range(D) for a in range(D)], 0)
+    A2 = np.sum(x * x, axis=0)
+    x = x / (np.sqrt(A2) + eps)
+    if use_redelta:
+        re = delta ** 2 * np.sqrt(np.mean(A2)) / visc
+        z = (np.log(re) - mu) / sigma
+        x = np.concatenate([x, np.full((1,) + A2.shape, z)], 0)
+    nl = len(weights)
+    for l, W in enumerate(weights):
+        y = np.einsum("oc,c...->o...", np.asarray(W, dtype=np.float64), x)
+        if biases[l] is not None:
+            y = y + np.asarray(biases[l], dtype=np.float64).reshape((-1,) + (1,) * A2.ndim)
+        x = gelu(y) if l < nl - 1 else y
+    if D == 3:
+        t = (x[0] + x[1] + x[2]) / 3
+        x = np.stack([x[0] - t, x[1] - t, x[2] - t, x[3], x[4], x[5]], 0)
+    else:
+        t = (x[0] + x[1]) / 2
+        x = np.stack([x[0] - t, x[1] - t, x[2]], 0)
+    return x * (delta ** 2 * A2)

@@ -119,6 +119,11 @@ struct sc_closure {
   void* ccg0 = nullptr;    // [4][npts]
   double* gw = nullptr;    // flat parameter gradient (FP64)
   long long nparam = 0;
+  // pointwise MLP closure
+  int mlp_nl = 0;
+  int mlp_w[sc::kMlpMaxLayers + 1] = {};
+  void* mlp_theta = nullptr;
+  double* mlp_z = nullptr;  // [sum |G|^2, z] when the Re_Delta channel is used
   std::vector<void*> allocs;
 };
 
@@ -417,6 +422,20 @@ int cc_backward(sc_closure* cl, const R* gtau, cudaStream_t st) {
   return check_launch("cnn backward (CUDA cores)");
 }
 
+sc::MlpArgs mlp_args(sc_closure* cl, const void* const* G, void* const* tau) {
+  sc_plan* p = cl->p;
+  sc::MlpArgs a{};
+  const int D = p->D;
+  for (int c = 0; c < D * D; ++c) a.G[c] = G[c];
+  for (int c = 0; c < (D == 3 ? 6 : 3); ++c) a.tau[c] = tau[c];
+  a.npts = phys_args(p).npts;
+  a.D = D; a.nl = cl->mlp_nl;
+  for (int l = 0; l <= cl->mlp_nl; ++l) a.w[l] = cl->mlp_w[l];
+  a.theta = cl->mlp_theta;
+  a.delta = cl->delta;
+  return a;
+}
+
 // Tensor-core CNN for the adjoint: forward at u keeping every layer input and
 // the pre-activations (v in gp[0..2], tau in tp), and backward from dL/dtau
 // (planar FP32 in cctau) to dL/dv (ccg0[0..2]), dL/dz (dsum[1]) and the
@@ -483,7 +502,15 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
   sc_plan* p = cl->p;
   const int D = p->D, NP = D == 3 ? 6 : 3;
   int rc = SC_OK;
-  if (cl->kind == sc::kClark || cl->kind == sc::kSmagorinsky || cl->kind == sc::kVerstappen) {
+  if (cl->kind == sc::kMlp) {
+    sc::LesSpecArgs g = spec_args(p);
+    for (int c = 0; c < D; ++c) g.in[c] = u[c];
+    for (int c = 0; c < D * D; ++c) g.out[c] = cl->gc[c];
+    sc::launch_grad<R>(g, D, st);
+    if ((rc = c2p_batch<R>(p, cl->bb, cl->cb, cl->gc, cl->gp, D * D, st))) return rc;
+    sc::launch_mlp<R>(mlp_args(cl, (const void* const*)cl->gp, cl->tp), cl->mlp_z, cl->nu, cl->mu, cl->sigma, st);
+    if ((rc = check_launch("mlp closure"))) return rc;
+  } else if (cl->kind == sc::kClark || cl->kind == sc::kSmagorinsky || cl->kind == sc::kVerstappen) {
     sc::LesSpecArgs g = spec_args(p);
     for (int c = 0; c < D; ++c) g.in[c] = u[c];
     for (int c = 0; c < D * D; ++c) g.out[c] = cl->gc[c];
@@ -1463,15 +1490,64 @@ int sc_cnn_fp_closure_create(sc_closure** out, sc_plan* p, double delta, double 
   return SC_OK;
 }
 
+int sc_mlp_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, int nlayers, const int* widths,
+                          const double* theta, int use_redelta, double mu, double sigma) {
+  if (!out || !p || !widths || !theta) return fail(SC_ERR_INVALID, "null argument");
+  *out = nullptr;
+  const int D = p->D, NP = D == 3 ? 6 : 3;
+  if (nlayers < 1 || nlayers > sc::kMlpMaxLayers) return fail(SC_ERR_INVALID, "1 <= nlayers <= %d", sc::kMlpMaxLayers);
+  if (widths[0] != D * D + (use_redelta ? 1 : 0))
+    return fail(SC_ERR_INVALID, "widths[0] must be D^2 (+1 with the Re_Delta channel)");
+  if (widths[nlayers] != NP) return fail(SC_ERR_INVALID, "the last width must be %d", NP);
+  for (int l = 0; l <= nlayers; ++l)
+    if (widths[l] < 1 || widths[l] > sc::kMlpMaxWidth) return fail(SC_ERR_INVALID, "widths must be 1..%d", sc::kMlpMaxWidth);
+  if (!(delta > 0) || (use_redelta && (!(visc > 0) || !(sigma > 0))))
+    return fail(SC_ERR_INVALID, "delta (and with Re_Delta: visc, sigma) must be positive");
+  sc_closure* cl = nullptr;
+  int rc = sc_closure_create(&cl, p, sc::kClark, delta, nullptr, 0);
+  if (rc) return rc;
+  cl->kind = sc::kMlp;
+  cl->nu = visc; cl->mu = mu; cl->sigma = sigma;
+  cl->mlp_nl = nlayers;
+  long long np_ = 0;
+  for (int l = 0; l < nlayers; ++l) {
+    cl->mlp_w[l] = widths[l];
+    np_ += (long long)widths[l] * widths[l + 1] + (l < nlayers - 1 ? widths[l + 1] : 0);
+  }
+  cl->mlp_w[nlayers] = widths[nlayers];
+  cl->nparam = np_;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  rc = A(&cl->mlp_theta, np_ * (p->esz / 2));
+  if (!rc && use_redelta) rc = A((void**)&cl->mlp_z, 2 * sizeof(double));
+  if (!rc) rc = sc_closure_set_params(cl, theta);
+  if (rc) { sc_closure_destroy(cl); return rc; }
+  *out = cl;
+  return SC_OK;
+}
+
 int sc_closure_num_params(const sc_closure* cl, long long* n) {
   if (!cl || !n) return fail(SC_ERR_INVALID, "null argument");
-  *n = (cl->kind == sc::kCnnFp || cl->kind == sc::kCnn) ? cl->nparam : 0;
+  *n = (cl->kind == sc::kCnnFp || cl->kind == sc::kCnn || cl->kind == sc::kMlp) ? cl->nparam : 0;
   return SC_OK;
 }
 
 int sc_closure_set_params(sc_closure* cl, const double* theta) {
   if (!cl || !theta) return fail(SC_ERR_INVALID, "null argument");
   if (cl->kind == sc::kCnn) return tc_upload_params(cl, theta);
+  if (cl->kind == sc::kMlp) {
+    if (cl->p->dtype == SC_FLOAT64) {
+      SC_CU(cudaMemcpy(cl->mlp_theta, theta, cl->nparam * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(theta, theta + cl->nparam);
+      SC_CU(cudaMemcpy(cl->mlp_theta, f.data(), cl->nparam * 4, cudaMemcpyHostToDevice));
+    }
+    return SC_OK;
+  }
   if (cl->kind != sc::kCnnFp) return fail(SC_ERR_UNSUPPORTED, "only the CNN closures have a parameter vector");
   const bool f64 = cl->p->dtype == SC_FLOAT64;
   for (int l = 0; l < 4; ++l) {
@@ -1524,6 +1600,12 @@ int sc_closure_eval(sc_closure* cl, const void* const* u, const void* const* G, 
   cudaStream_t st = as_stream(stream);
   auto body = [&](auto tag) -> int {
     using R = decltype(tag);
+    if (cl->kind == sc::kMlp) {
+      int r = check_ptrs(G, D * D);
+      if (r) return r;
+      sc::launch_mlp<R>(mlp_args(cl, G, tau), cl->mlp_z, cl->nu, cl->mu, cl->sigma, st);
+      return check_launch("mlp closure");
+    }
     if (cl->kind == sc::kClark || cl->kind == sc::kSmagorinsky || cl->kind == sc::kVerstappen) {
       int r = check_ptrs(G, D * D);
       if (r) return r;

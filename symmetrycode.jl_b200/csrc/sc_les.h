@@ -6,7 +6,7 @@ namespace sc {
 
 // closure kinds (values match include/symcode.h SC_CLOSURE_*)
 enum { kNoClosure = 0, kClark = 1, kSmagorinsky = 2, kVerstappen = 3, kDynSmagorinsky = 4, kBardina = 5, kCnn = 6,
-       kCnnFp = 7 };
+       kCnnFp = 7, kMlp = 8 };
 
 struct LesSpecArgs {
   const void* in[9];
@@ -40,5 +40,22 @@ template <typename R> void launch_smag_tensor(const LesPhysArgs& a, int D, cudaS
 template <typename R> void launch_sub_products(const LesPhysArgs& a, int D, cudaStream_t st);
 // accumulates sum(M:L), sum(M:M) into sums[0..1] (zero them first) and sets sums[2] = c
 template <typename R> void launch_dynsmag_mlmm(const LesPhysArgs& a, int D, double* sums, cudaStream_t st);
+
+// pointwise MLP closure (sc_mlp.cu): fullchain(mlp) of src/nets.jl:311-331
+constexpr int kMlpMaxWidth = 128;
+constexpr int kMlpMaxLayers = 8;
+struct MlpArgs {
+  const void* G[9];   // physical VGT, channel a + D b = d_b u_a
+  void* tau[6];       // physical tau, pair order
+  long long npts;
+  int D, nl;
+  int w[kMlpMaxLayers + 1];  // widths: w[0] = D^2 (+1 with the Re_Delta channel) ... w[nl] = 3 | 6
+  const void* theta;  // per layer W[c_out][c_in], then b[c_out] (all layers but the last)
+  double delta;
+  const double* z;    // set by launch_mlp
+};
+// zbuf: two device doubles when the Re_Delta channel is used, else null
+template <typename R>
+void launch_mlp(const MlpArgs& a, double* zbuf, double nu, double mu, double sigma, cudaStream_t st);
 
 }  // namespace sc

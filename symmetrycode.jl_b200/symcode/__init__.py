@@ -373,6 +373,33 @@ def create_cnn_fp_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1
     return cl
 
 
+CLOSURE_MLP = 8
+
+
+def create_mlp_closure(delta, visc, g: Grid, weights, biases, use_redelta=False, mu=0.0, sigma=1.0):
+    """``fullchain(setup, mlp(...))`` (src/nets.jl:311-331): pointwise MLP closure.
+    ``weights[l]``: (c_out, c_in); ``biases[l]``: (c_out,) for all layers but the last."""
+    import numpy as np
+    nl = len(weights)
+    widths = [int(np.shape(weights[0])[1])] + [int(np.shape(w)[0]) for w in weights]
+    parts = []
+    for l, w in enumerate(weights):
+        parts.append(np.asarray(w, dtype=np.float64).ravel())
+        if l < nl - 1:
+            parts.append(np.asarray(biases[l], dtype=np.float64).ravel())
+    theta = np.ascontiguousarray(np.concatenate(parts))
+    wa = (ct.c_int * (nl + 1))(*widths)
+    cl = Closure.__new__(Closure)
+    cl.g, cl.kind, cl.delta = g, CLOSURE_MLP, float(delta)
+    ptr = ct.c_void_p()
+    with torch.cuda.device(g.device):
+        check(lib().sc_mlp_closure_create(ct.byref(ptr), g.plan, float(delta), float(visc), nl, wa,
+                                          theta.ctypes.data_as(ct.POINTER(ct.c_double)), int(bool(use_redelta)),
+                                          float(mu), float(sigma)))
+    cl._ptr = ptr
+    return cl
+
+
 def closure_num_params(cl):
     n = ct.c_longlong()
     check(lib().sc_closure_num_params(cl.ptr, ct.byref(n)))

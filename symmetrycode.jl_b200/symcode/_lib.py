@@ -99,6 +99,9 @@ _SIGS = {
     "sc_rollout_adjoint_batch": ([ct.c_int, ct.POINTER(sc_rollout_job), ct.POINTER(ct.c_int), _vp], ct.c_int),
     "sc_les_diagnostics": ([_vp, _vp, _pp, _pp, ct.c_double, ct.c_int, ct.POINTER(ct.c_double),
                             ct.POINTER(ct.c_double), ct.POINTER(ct.c_double), _vp], ct.c_int),
+    "sc_mlp_closure_create": ([ct.POINTER(ct.c_void_p), _vp, ct.c_double, ct.c_double, ct.c_int,
+                               ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, ct.c_double, ct.c_double],
+                              ct.c_int),
     "sc_spectrum_static": ([_pp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),

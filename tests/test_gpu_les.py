@@ -173,3 +173,29 @@ def test_les_diagnostics_match_oracle(kind):
         assert math.isclose(got["eps_sfs"], ref["eps_sfs"], rel_tol=1e-9), (got["eps_sfs"], ref["eps_sfs"])
         t, tr = np.array(got["transfer"]), np.array(ref["transfer"])
         assert np.linalg.norm(t - tr) <= 1e-9 * np.linalg.norm(tr)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 2e-5)])
+@pytest.mark.parametrize("widths,redelta", [([9, 16, 12, 6], False), ([10, 8, 6], True)])
+def test_mlp_closure_matches_oracle(dtype, tol, widths, redelta):
+    """fullchain(mlp) (src/nets.jl:311-331): model(u, G) and les! against the oracle."""
+    D, n, visc = 3, 32, 1e-3
+    g, go = S.Grid(D, n, dtype=dtype, device="cuda:0"), O.Grid(D, n)
+    u = O.random_field(go, seed=33, kpeak=3)
+    delta = 2 * go.l / n
+    rng = np.random.default_rng(34)
+    ws = [rng.standard_normal((widths[l + 1], widths[l])) / np.sqrt(widths[l]) for l in range(len(widths) - 1)]
+    bs = [0.1 * rng.standard_normal(widths[l + 1]) for l in range(len(widths) - 2)] + [None]
+    cl = S.create_mlp_closure(delta, visc, g, ws, bs, use_redelta=redelta, mu=2.0, sigma=1.5)
+    eps = np.finfo(np.float32 if dtype == torch.float32 else np.float64).eps
+    model = lambda uu, GG: O.mlp_fullchain(GG, delta, visc, ws, bs, D, redelta, 2.0, 1.5, eps)  # noqa: E731
+    GG = O.physical_gradient(u, go)
+    names = "xyz"[:D]
+    Gt = [to_dev(GG[names[a] + names[b]], g) for b in range(D) for a in range(D)]
+    tau = cl([to_dev(c, g) for c in u], Gt)
+    assert rel_l2(to_np(tau), model(u, GG)) < tol
+    ref = [O.twothirds(c, go) for c in O.les_rhs(u, go, model, visc)]
+    du = S.vectorfield(g)
+    S.les_(du, [to_dev(c, g) for c in u], g, cl, visc)
+    assert rel_l2([to_np(c) for c in du], ref) < tol
+    assert S.closure_num_params(cl) == sum(w.size for w in ws) + sum(b.size for b in bs if b is not None)
