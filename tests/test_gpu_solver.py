@@ -194,6 +194,21 @@ def test_rk4_unforced_2d():
     assert rel_l2([to_np(c) for c in ut], ref) < TOL64
 
 
+def test_config0_2d_decaying_200_steps():
+    """The 2D decaying case: 256^2 FP64, nu = 5e-4, RK4 dt = 1e-3, 200 steps from
+    the seeded k^4 exp(-2 (k/5)^2) field (seed 0), against the oracle on the same
+    field; the tolerance allows 200 steps of round-off growth."""
+    g, go = _grid(2, 256, torch.float64)
+    u = O.random_field(go, seed=0, kpeak=5)
+    ref = u
+    for _ in range(200):
+        ref = O.rk4_step(ref, 1e-3, go, 5e-4)
+    ut = [to_dev(c, g) for c in u]
+    S.rk4_(ut, 1e-3, g, 5e-4, nsteps=200)
+    assert rel_l2([to_np(c) for c in ut], ref) < 1e-11
+    assert math.isclose(S.energy(ut, g), O.energy(ref), rel_tol=1e-12)
+
+
 # -------------------------------------------------------------- diagnostics
 def test_energy_and_dissipation():
     g, go = _grid(3, 32, torch.float64)
