@@ -199,6 +199,16 @@ SC_API int sc_cnn_fp_closure_create(sc_closure** closure, sc_plan* plan, double 
 #define SC_CLOSURE_MLP 8
 SC_API int sc_mlp_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc, int nlayers,
                                  const int* widths, const double* theta, int use_redelta, double mu, double sigma);
+/* tbnn(net, ps, st, Delta, g; use_redelta, redelta_norm, visc) (src/nets.jl:560-588)
+ * with the tensor basis of tb_kernel! (src/nets.jl:393-505): the normalised
+ * gradient's invariants tr(SS), tr(RR) [, tr(SSS), tr(SRR), tr(SSRR)] (+ Re_Delta)
+ * feed the same pointwise MLP (widths[0] = 2 | 5 (+1), widths[nlayers] = 2 | 7
+ * basis coefficients); tau = sum_k w_k B_k * Delta^2 |G|^2 with the deviatoric
+ * basis dev(S), dev(SR - RS) (2D) or dev(S), dev(SS), dev(RR), dev(SR - RS),
+ * dev(RSR), dev(RSS - SSR), dev(RSRR - RRSR) (3D).  Kind SC_CLOSURE_TBNN. */
+#define SC_CLOSURE_TBNN 9
+SC_API int sc_tbnn_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc, int nlayers,
+                                  const int* widths, const double* theta, int use_redelta, double mu, double sigma);
 SC_API int sc_closure_num_params(const sc_closure* closure, long long* nparams);
 SC_API int sc_closure_set_params(sc_closure* closure, const double* theta);
 /* Synchronous: SC_ERR_TIMEOUT if a bounded wait of the closure's kernels ran out. */

@@ -21,7 +21,7 @@ from .filtering import gaussianfilter
 from .spectral import (WORKERS, Grid, nonlinearity, pairs, strainrate, to_phys,
                        twothirds, make_tracefree)
 
-__all__ = ["mlp_fullchain", "GRAD_ORDER", "grad_matrix", "store_sym", "clark", "smagorinsky", "verstappen",
+__all__ = ["mlp_fullchain", "tbnn", "GRAD_ORDER", "grad_matrix", "store_sym", "clark", "smagorinsky", "verstappen",
            "bardina", "dynamic_smagorinsky", "smagorinsky_tensor", "smagorinsky_ml_mm",
            "dynsmag_coefficient", "test_filter_phys"]
 
@@ -184,3 +184,48 @@ def mlp_fullchain(G, delta, visc, weights, biases, D, use_redelta=False, mu=0.0,
         t = (x[0] + x[1]) / 2
         x = np.stack([x[0] - t, x[1] - t, x[2]], 0)
     return x * (delta ** 2 * A2)
+
+
+def _dev(M, D):
+    tr = np.trace(M, axis1=-2, axis2=-1)[..., None, None]
+    return M - tr / D * np.eye(D)
+
+
+def tbnn(G, delta, visc, weights, biases, D, use_redelta=False, mu=0.0, sigma=1.0, eps=np.finfo(np.float64).eps):
+    """``tbnn(net, ps, st, Delta, g; use_redelta, redelta_norm, visc)``
+    (src/nets.jl:560-588) with ``build_tensorbasis`` / ``tb_kernel!``
+    (src/nets.jl:393-505): A = grad u normalised by (|A| + eps), S and R its
+    symmetric and antisymmetric parts; invariants tr(SS), tr(RR) [, tr(SSS),
+    tr(SRR), tr(SSRR)] (+ the standardised log Re_Delta) feed a pointwise MLP
+    (GELU, bias-free last layer) whose outputs weight the deviatoric basis
+    dev(S), dev(SR - RS) (2D) or dev(S), dev(SS), dev(RR), dev(SR - RS), dev(RSR),
+    dev(RSS - SSR), dev(RSRR - RRSR) (3D); tau = sum * Delta^2 |A|^2, packed."""
+    from .cnn import gelu
+    names = "xyz"[:D]
+    A = np.stack([np.stack([G[names[a] + names[b]] for b in range(D)], -1) for a in range(D)], -2)
+    A2 = np.sum(A * A, axis=(-1, -2))
+    A = A / (np.sqrt(A2) + eps)[..., None, None]
+    S = (A + np.swapaxes(A, -1, -2)) / 2
+    R = (A - np.swapaxes(A, -1, -2)) / 2
+    mm = lambda *Ms: __import__("functools").reduce(lambda x, y: x @ y, Ms)  # noqa: E731
+    tr = lambda M: np.trace(M, axis1=-2, axis2=-1)  # noqa: E731
+    if D == 2:
+        inv = [tr(mm(S, S)), tr(mm(R, R))]
+        basis = [_dev(S, D), _dev(mm(S, R) - mm(R, S), D)]
+    else:
+        inv = [tr(mm(S, S)), tr(mm(R, R)), tr(mm(S, S, S)), tr(mm(S, R, R)), tr(mm(S, S, R, R))]
+        basis = [_dev(S, D), _dev(mm(S, S), D), _dev(mm(R, R), D), _dev(mm(S, R) - mm(R, S), D),
+                 _dev(mm(R, S, R), D), _dev(mm(R, S, S) - mm(S, S, R), D),
+                 _dev(mm(R, S, R, R) - mm(R, R, S, R), D)]
+    x = np.stack(inv, 0)
+    if use_redelta:
+        re = delta ** 2 * np.sqrt(np.mean(A2)) / visc
+        x = np.concatenate([x, np.full((1,) + A2.shape, (np.log(re) - mu) / sigma)], 0)
+    nl = len(weights)
+    for l, W in enumerate(weights):
+        y = np.einsum("oc,c...->o...", np.asarray(W, dtype=np.float64), x)
+        if biases[l] is not None:
+            y = y + np.asarray(biases[l], dtype=np.float64).reshape((-1,) + (1,) * A2.ndim)
+        x = gelu(y) if l < nl - 1 else y
+    M = sum(x[k][..., None, None] * basis[k] for k in range(len(basis)))
+    return np.stack([M[..., i, j] for (i, j) in pairs(D)], 0) * (delta ** 2 * A2)

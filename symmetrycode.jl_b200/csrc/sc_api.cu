@@ -433,6 +433,7 @@ sc::MlpArgs mlp_args(sc_closure* cl, const void* const* G, void* const* tau) {
   for (int l = 0; l <= cl->mlp_nl; ++l) a.w[l] = cl->mlp_w[l];
   a.theta = cl->mlp_theta;
   a.delta = cl->delta;
+  a.mode = cl->kind == sc::kTbnn ? 1 : 0;
   return a;
 }
 
@@ -502,7 +503,7 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
   sc_plan* p = cl->p;
   const int D = p->D, NP = D == 3 ? 6 : 3;
   int rc = SC_OK;
-  if (cl->kind == sc::kMlp) {
+  if (cl->kind == sc::kMlp || cl->kind == sc::kTbnn) {
     sc::LesSpecArgs g = spec_args(p);
     for (int c = 0; c < D; ++c) g.in[c] = u[c];
     for (int c = 0; c < D * D; ++c) g.out[c] = cl->gc[c];
@@ -1490,15 +1491,20 @@ int sc_cnn_fp_closure_create(sc_closure** out, sc_plan* p, double delta, double 
   return SC_OK;
 }
 
-int sc_mlp_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, int nlayers, const int* widths,
-                          const double* theta, int use_redelta, double mu, double sigma) {
+}  // extern "C"
+
+namespace {
+int pointwise_net_create(sc_closure** out, sc_plan* p, int kind, double delta, double visc, int nlayers,
+                         const int* widths, const double* theta, int use_redelta, double mu, double sigma) {
   if (!out || !p || !widths || !theta) return fail(SC_ERR_INVALID, "null argument");
   *out = nullptr;
   const int D = p->D, NP = D == 3 ? 6 : 3;
+  const int nin = kind == sc::kTbnn ? (D == 3 ? 5 : 2) : D * D;  // invariants or gradient channels
+  const int nout = kind == sc::kTbnn ? (D == 3 ? 7 : 2) : NP;    // basis coefficients or stress
   if (nlayers < 1 || nlayers > sc::kMlpMaxLayers) return fail(SC_ERR_INVALID, "1 <= nlayers <= %d", sc::kMlpMaxLayers);
-  if (widths[0] != D * D + (use_redelta ? 1 : 0))
-    return fail(SC_ERR_INVALID, "widths[0] must be D^2 (+1 with the Re_Delta channel)");
-  if (widths[nlayers] != NP) return fail(SC_ERR_INVALID, "the last width must be %d", NP);
+  if (widths[0] != nin + (use_redelta ? 1 : 0))
+    return fail(SC_ERR_INVALID, "widths[0] must be %d (+1 with the Re_Delta channel)", nin);
+  if (widths[nlayers] != nout) return fail(SC_ERR_INVALID, "the last width must be %d", nout);
   for (int l = 0; l <= nlayers; ++l)
     if (widths[l] < 1 || widths[l] > sc::kMlpMaxWidth) return fail(SC_ERR_INVALID, "widths must be 1..%d", sc::kMlpMaxWidth);
   if (!(delta > 0) || (use_redelta && (!(visc > 0) || !(sigma > 0))))
@@ -1506,7 +1512,7 @@ int sc_mlp_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
   sc_closure* cl = nullptr;
   int rc = sc_closure_create(&cl, p, sc::kClark, delta, nullptr, 0);
   if (rc) return rc;
-  cl->kind = sc::kMlp;
+  cl->kind = kind;
   cl->nu = visc; cl->mu = mu; cl->sigma = sigma;
   cl->mlp_nl = nlayers;
   long long np_ = 0;
@@ -1529,17 +1535,31 @@ int sc_mlp_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
   *out = cl;
   return SC_OK;
 }
+}  // namespace
+
+extern "C" {
+
+int sc_mlp_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, int nlayers, const int* widths,
+                          const double* theta, int use_redelta, double mu, double sigma) {
+  return pointwise_net_create(out, p, sc::kMlp, delta, visc, nlayers, widths, theta, use_redelta, mu, sigma);
+}
+
+int sc_tbnn_closure_create(sc_closure** out, sc_plan* p, double delta, double visc, int nlayers, const int* widths,
+                           const double* theta, int use_redelta, double mu, double sigma) {
+  return pointwise_net_create(out, p, sc::kTbnn, delta, visc, nlayers, widths, theta, use_redelta, mu, sigma);
+}
 
 int sc_closure_num_params(const sc_closure* cl, long long* n) {
   if (!cl || !n) return fail(SC_ERR_INVALID, "null argument");
-  *n = (cl->kind == sc::kCnnFp || cl->kind == sc::kCnn || cl->kind == sc::kMlp) ? cl->nparam : 0;
+  *n = (cl->kind == sc::kCnnFp || cl->kind == sc::kCnn || cl->kind == sc::kMlp || cl->kind == sc::kTbnn) ? cl->nparam
+                                                                                                         : 0;
   return SC_OK;
 }
 
 int sc_closure_set_params(sc_closure* cl, const double* theta) {
   if (!cl || !theta) return fail(SC_ERR_INVALID, "null argument");
   if (cl->kind == sc::kCnn) return tc_upload_params(cl, theta);
-  if (cl->kind == sc::kMlp) {
+  if (cl->kind == sc::kMlp || cl->kind == sc::kTbnn) {
     if (cl->p->dtype == SC_FLOAT64) {
       SC_CU(cudaMemcpy(cl->mlp_theta, theta, cl->nparam * 8, cudaMemcpyHostToDevice));
     } else {
@@ -1600,7 +1620,7 @@ int sc_closure_eval(sc_closure* cl, const void* const* u, const void* const* G, 
   cudaStream_t st = as_stream(stream);
   auto body = [&](auto tag) -> int {
     using R = decltype(tag);
-    if (cl->kind == sc::kMlp) {
+    if (cl->kind == sc::kMlp || cl->kind == sc::kTbnn) {
       int r = check_ptrs(G, D * D);
       if (r) return r;
       sc::launch_mlp<R>(mlp_args(cl, G, tau), cl->mlp_z, cl->nu, cl->mu, cl->sigma, st);

@@ -6,7 +6,7 @@ namespace sc {
 
 // closure kinds (values match include/symcode.h SC_CLOSURE_*)
 enum { kNoClosure = 0, kClark = 1, kSmagorinsky = 2, kVerstappen = 3, kDynSmagorinsky = 4, kBardina = 5, kCnn = 6,
-       kCnnFp = 7, kMlp = 8 };
+       kCnnFp = 7, kMlp = 8, kTbnn = 9 };
 
 struct LesSpecArgs {
   const void* in[9];
@@ -53,6 +53,7 @@ struct MlpArgs {
   const void* theta;  // per layer W[c_out][c_in], then b[c_out] (all layers but the last)
   double delta;
   const double* z;    // set by launch_mlp
+  int mode;           // 0: fullchain(mlp); 1: tbnn (invariants in, basis coefficients out)
 };
 // zbuf: two device doubles when the Re_Delta channel is used, else null
 template <typename R>

@@ -373,12 +373,23 @@ def create_cnn_fp_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1
     return cl
 
 
-CLOSURE_MLP = 8
+CLOSURE_MLP, CLOSURE_TBNN = 8, 9
 
 
 def create_mlp_closure(delta, visc, g: Grid, weights, biases, use_redelta=False, mu=0.0, sigma=1.0):
     """``fullchain(setup, mlp(...))`` (src/nets.jl:311-331): pointwise MLP closure.
     ``weights[l]``: (c_out, c_in); ``biases[l]``: (c_out,) for all layers but the last."""
+    return _pointwise_net(lib().sc_mlp_closure_create, CLOSURE_MLP, delta, visc, g, weights, biases, use_redelta,
+                          mu, sigma)
+
+
+def create_tbnn_closure(delta, visc, g: Grid, weights, biases, use_redelta=False, mu=0.0, sigma=1.0):
+    """``tbnn`` (src/nets.jl:560-588): invariants -> MLP -> tensor-basis coefficients."""
+    return _pointwise_net(lib().sc_tbnn_closure_create, CLOSURE_TBNN, delta, visc, g, weights, biases, use_redelta,
+                          mu, sigma)
+
+
+def _pointwise_net(fn, kind, delta, visc, g: Grid, weights, biases, use_redelta, mu, sigma):
     import numpy as np
     nl = len(weights)
     widths = [int(np.shape(weights[0])[1])] + [int(np.shape(w)[0]) for w in weights]
@@ -390,12 +401,11 @@ def create_mlp_closure(delta, visc, g: Grid, weights, biases, use_redelta=False,
     theta = np.ascontiguousarray(np.concatenate(parts))
     wa = (ct.c_int * (nl + 1))(*widths)
     cl = Closure.__new__(Closure)
-    cl.g, cl.kind, cl.delta = g, CLOSURE_MLP, float(delta)
+    cl.g, cl.kind, cl.delta = g, kind, float(delta)
     ptr = ct.c_void_p()
     with torch.cuda.device(g.device):
-        check(lib().sc_mlp_closure_create(ct.byref(ptr), g.plan, float(delta), float(visc), nl, wa,
-                                          theta.ctypes.data_as(ct.POINTER(ct.c_double)), int(bool(use_redelta)),
-                                          float(mu), float(sigma)))
+        check(fn(ct.byref(ptr), g.plan, float(delta), float(visc), nl, wa,
+                 theta.ctypes.data_as(ct.POINTER(ct.c_double)), int(bool(use_redelta)), float(mu), float(sigma)))
     cl._ptr = ptr
     return cl
 

@@ -102,6 +102,9 @@ _SIGS = {
     "sc_mlp_closure_create": ([ct.POINTER(ct.c_void_p), _vp, ct.c_double, ct.c_double, ct.c_int,
                                ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, ct.c_double, ct.c_double],
                               ct.c_int),
+    "sc_tbnn_closure_create": ([ct.POINTER(ct.c_void_p), _vp, ct.c_double, ct.c_double, ct.c_int,
+                                ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, ct.c_double, ct.c_double],
+                               ct.c_int),
     "sc_spectrum_static": ([_pp, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_dissipation": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),

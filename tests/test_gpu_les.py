@@ -199,3 +199,30 @@ def test_mlp_closure_matches_oracle(dtype, tol, widths, redelta):
     S.les_(du, [to_dev(c, g) for c in u], g, cl, visc)
     assert rel_l2([to_np(c) for c in du], ref) < tol
     assert S.closure_num_params(cl) == sum(w.size for w in ws) + sum(b.size for b in bs if b is not None)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-11), (torch.float32, 5e-5)])
+@pytest.mark.parametrize("D,redelta", [(3, False), (3, True), (2, False)])
+def test_tbnn_closure_matches_oracle(dtype, tol, D, redelta):
+    """tbnn (src/nets.jl:560-588) with the tensor basis of tb_kernel!: model(u, G) and les!."""
+    n, visc = (32 if D == 3 else 64), 1e-3
+    g, go = S.Grid(D, n, dtype=dtype, device="cuda:0"), O.Grid(D, n)
+    u = O.random_field(go, seed=35, kpeak=3)
+    delta = 2 * go.l / n
+    nin, nb = (5, 7) if D == 3 else (2, 2)
+    widths = [nin + int(redelta), 12, 10, nb]
+    rng = np.random.default_rng(36)
+    ws = [rng.standard_normal((widths[l + 1], widths[l])) / np.sqrt(widths[l]) for l in range(len(widths) - 1)]
+    bs = [0.1 * rng.standard_normal(widths[l + 1]) for l in range(len(widths) - 2)] + [None]
+    cl = S.create_tbnn_closure(delta, visc, g, ws, bs, use_redelta=redelta, mu=2.0, sigma=1.5)
+    eps = np.finfo(np.float32 if dtype == torch.float32 else np.float64).eps
+    model = lambda uu, GG: O.tbnn(GG, delta, visc, ws, bs, D, redelta, 2.0, 1.5, eps)  # noqa: E731
+    GG = O.physical_gradient(u, go)
+    names = "xyz"[:D]
+    Gt = [to_dev(GG[names[a] + names[b]], g) for b in range(D) for a in range(D)]
+    tau = cl([to_dev(c, g) for c in u], Gt)
+    assert rel_l2(to_np(tau), model(u, GG)) < tol
+    ref = [O.twothirds(c, go) for c in O.les_rhs(u, go, model, visc)]
+    du = S.vectorfield(g)
+    S.les_(du, [to_dev(c, g) for c in u], g, cl, visc)
+    assert rel_l2([to_np(c) for c in du], ref) < tol
