@@ -149,23 +149,59 @@ template <int P, int Q, bool INV, typename C> struct DFTPQ {
   }
 };
 
-template <bool INV, typename C> struct DFT<6, INV, C> : DFTPQ<2, 3, INV, C> {};
+// Prime-factor (Good-Thomas) composite for coprime P, Q: input index
+// n = (Q n1 + P n2) mod N, output index k with k = k1 (mod P), k = k2 (mod Q);
+// then X = DFT_P over n1 of DFT_Q over n2, with no twiddle factors.  Both index
+// maps are compile-time, so in registers they cost nothing.
+constexpr int sc_modinv(int a, int m) {
+  for (int x = 1; x < m; ++x)
+    if ((a * x) % m == 1) return x;
+  return 1;
+}
+template <int P, int Q, bool INV, typename C> struct DFTPFA {
+  static __device__ __forceinline__ void run(C* v) {
+    constexpr int N = P * Q;
+    constexpr int EP = Q * sc_modinv(Q % P, P);  // = 1 (mod P), 0 (mod Q)
+    constexpr int EQ = P * sc_modinv(P % Q, Q);  // = 0 (mod P), 1 (mod Q)
+    C y[N];
+#pragma unroll
+    for (int n1 = 0; n1 < P; ++n1) {
+      C t[Q];
+#pragma unroll
+      for (int n2 = 0; n2 < Q; ++n2) t[n2] = v[(Q * n1 + P * n2) % N];
+      DFT<Q, INV, C>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < Q; ++k2) y[n1 * Q + k2] = t[k2];
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < Q; ++k2) {
+      C s[P];
+#pragma unroll
+      for (int n1 = 0; n1 < P; ++n1) s[n1] = y[n1 * Q + k2];
+      DFT<P, INV, C>::run(s);
+#pragma unroll
+      for (int k1 = 0; k1 < P; ++k1) v[(k1 * EP + k2 * EQ) % N] = s[k1];
+    }
+  }
+};
+
+template <bool INV, typename C> struct DFT<6, INV, C> : DFTPFA<2, 3, INV, C> {};
 template <bool INV, typename C> struct DFT<8, INV, C> : DFTPQ<2, 4, INV, C> {};
 template <bool INV, typename C> struct DFT<9, INV, C> : DFTPQ<3, 3, INV, C> {};
-template <bool INV, typename C> struct DFT<10, INV, C> : DFTPQ<2, 5, INV, C> {};
-template <bool INV, typename C> struct DFT<12, INV, C> : DFTPQ<4, 3, INV, C> {};
-template <bool INV, typename C> struct DFT<15, INV, C> : DFTPQ<3, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<10, INV, C> : DFTPFA<2, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<12, INV, C> : DFTPFA<4, 3, INV, C> {};
+template <bool INV, typename C> struct DFT<15, INV, C> : DFTPFA<3, 5, INV, C> {};
 template <bool INV, typename C> struct DFT<16, INV, C> : DFTPQ<4, 4, INV, C> {};
-template <bool INV, typename C> struct DFT<18, INV, C> : DFTPQ<2, 9, INV, C> {};
-template <bool INV, typename C> struct DFT<20, INV, C> : DFTPQ<4, 5, INV, C> {};
-template <bool INV, typename C> struct DFT<24, INV, C> : DFTPQ<8, 3, INV, C> {};
+template <bool INV, typename C> struct DFT<18, INV, C> : DFTPFA<2, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<20, INV, C> : DFTPFA<4, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<24, INV, C> : DFTPFA<8, 3, INV, C> {};
 template <bool INV, typename C> struct DFT<25, INV, C> : DFTPQ<5, 5, INV, C> {};
 template <bool INV, typename C> struct DFT<27, INV, C> : DFTPQ<3, 9, INV, C> {};
-template <bool INV, typename C> struct DFT<30, INV, C> : DFTPQ<3, 10, INV, C> {};
+template <bool INV, typename C> struct DFT<30, INV, C> : DFTPFA<3, 10, INV, C> {};
 template <bool INV, typename C> struct DFT<32, INV, C> : DFTPQ<4, 8, INV, C> {};
-template <bool INV, typename C> struct DFT<36, INV, C> : DFTPQ<4, 9, INV, C> {};
-template <bool INV, typename C> struct DFT<40, INV, C> : DFTPQ<8, 5, INV, C> {};
-template <bool INV, typename C> struct DFT<45, INV, C> : DFTPQ<5, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<36, INV, C> : DFTPFA<4, 9, INV, C> {};
+template <bool INV, typename C> struct DFT<40, INV, C> : DFTPFA<8, 5, INV, C> {};
+template <bool INV, typename C> struct DFT<45, INV, C> : DFTPFA<5, 9, INV, C> {};
 
 // ---------------------------------------------------------------------------
 // radix schedule for N = 2^a 3^b 5^c (compile time)
