@@ -154,6 +154,43 @@ function create_cnn(Δ, visc, p::Plan, ws::Vector{Vector{Float32}}, bs::Vector{V
     return c
 end
 
+"""
+Pointwise learned closures: `fullchain(setup, mlp(...))` (`kind = :mlp`) and `tbnn`
+(`kind = :tbnn`).  `ws[l]` is the layer's `(c_in, c_out)` PointwiseConv weight
+(Julia memory order), `bs[l]` its bias (absent for the last layer).
+"""
+function create_pointwise(kind::Symbol, Δ, visc, p::Plan, ws::Vector{Matrix{Float64}}, bs::Vector{Vector{Float64}};
+                          use_redelta = false, mu = 0.0, sigma = 1.0)
+    widths = Cint[size(ws[1], 1); [size(w, 2) for w in ws]]
+    θ = Float64[]
+    for (l, w) in enumerate(ws)
+        append!(θ, vec(w))
+        l < length(ws) && append!(θ, bs[l])
+    end
+    f = kind === :tbnn ? :sc_tbnn_closure_create : :sc_mlp_closure_create
+    ref = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((f, LIB), Cint,
+        (Ptr{Ptr{Cvoid}}, Ptr{Cvoid}, Cdouble, Cdouble, Cint, Ptr{Cint}, Ptr{Cdouble}, Cint, Cdouble, Cdouble),
+        ref, p.ptr, Δ, visc, length(ws), widths, θ, use_redelta, mu, sigma))
+    c = Closure(ref[], p)
+    finalizer(c -> ccall((:sc_closure_destroy, LIB), Cint, (Ptr{Cvoid},), c.ptr), c)
+    return c
+end
+
+"The a-posteriori reductions of `solve_les!` (src/les.jl:94-148) for one LES state."
+function les_diagnostics(u, p::Plan; model::Union{Nothing, Closure} = nothing, uref = nothing, visc, nshell)
+    out = zeros(Cdouble, 4)
+    spec = zeros(Cdouble, nshell)
+    tr = zeros(Cdouble, nshell)
+    m = isnothing(model) ? C_NULL : model.ptr
+    r = isnothing(uref) ? Ptr{CuPtr{Cvoid}}(C_NULL) : ptrs(uref)
+    check(ccall((:sc_les_diagnostics, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Ptr{CuPtr{Cvoid}}, Cdouble, Cint, Ptr{Cdouble}, Ptr{Cdouble},
+         Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, m, ptrs(u), r, visc, nshell, out, spec, tr, stream()))
+    return (; e_post = out[1], ke = out[2], eps_visc = out[3], eps_sfs = out[4], spectrum = spec, transfer = tr)
+end
+
 "The CNN's flat parameter vector θ (weights then biases per layer)."
 function set_params!(c::Closure, θ::Vector{Float64})
     check(ccall((:sc_closure_set_params, LIB), Cint, (Ptr{Cvoid}, Ptr{Cdouble}), c.ptr, θ))
