@@ -130,7 +130,9 @@ class ClockSampler:
         return out
 
 
-def init_dist():
+def init_dist(backend=None):
+    """One process per GPU (torchrun env).  The replicas exchange nothing but
+    the timing; NCCL on GPUs, gloo when the ranks run on CPU (tests)."""
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -138,8 +140,10 @@ def init_dist():
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return ws, rank, local
 
 
@@ -154,9 +158,17 @@ def max_over_ranks(x, ws):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(ms_local, ws, steps):
+    """Whole-job steps/s of `ws` independent replicas: every rank ran `steps`
+    steps; the job's time is the slowest rank's (max over ranks)."""
+    ms = max_over_ranks(ms_local, ws)
+    return ws * steps / (ms / 1e3), ms
 
 
 def initial_compact(n, seed):
@@ -509,9 +521,7 @@ def run_gpu(args):
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier(ws)
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms, ws)
-    value = ws * args.steps / (ms / 1e3)
+    value, ms = job_throughput(ev0.elapsed_time(ev1), ws, args.steps)
     energy_after = st.energy()
     if not math.isfinite(energy_after):
         raise RuntimeError("state diverged during the benchmark")
