@@ -215,6 +215,24 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
       cp_async16(dst, reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
     }
   };
+  // one row yv of plane z by the 96 staging threads: 96 is a multiple of CPC, so
+  // each thread keeps its channel chunk and walks (z-offset, x) with adds only
+  auto stage_row = [&](int z, int yv, int pt) {
+    const int kc = pt % CPC, step = 96 / CPC;
+    const int yy = (yv + KN) % KN, sl = (yv + KN) % kSlots;
+    const long long zb0 = ((long long)((z - 1 + KN) % KN) * KN + yy) * KN;
+    const long long zb1 = ((long long)z * KN + yy) * KN;
+    const long long zb2 = ((long long)((z + 1) % KN) * KN + yy) * KN;
+    for (int xz = pt / CPC; xz < 3 * (KN + 2); xz += step) {
+      const int zr = xz >= 2 * (KN + 2) ? 2 : (xz >= KN + 2 ? 1 : 0);
+      const int xi = xz - zr * (KN + 2);
+      int x = xi - 1;
+      x = x < 0 ? x + KN : (x >= KN ? x - KN : x);
+      unsigned char* dst = s_in + (zr * kSlots + sl) * PLANE_ROW + kc * kRowPlane + xi * 16;
+      const long long zb = zr == 0 ? zb0 : (zr == 1 ? zb1 : zb2);
+      cp_async16(dst, reinterpret_cast<const uint4*>(act_in + (zb + x) * CP) + kc);
+    }
+  };
   auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
   // bounded wait of this thread for the MMAs of buffer b
   auto wait_buf = [&](int b) -> bool {
@@ -317,7 +335,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     if (pending >= 0 && warp != 0) mine = wait_buf(pending & 1);  // the last readers of row y-2's slot
     // prefetch row y+3 (read first by the MMAs of row y+2, when this CTA runs
     // that row in this plane); every thread commits a group, empty or not
-    if (is_stage && mine && y + 2 < KN && row + 2 < rend) stage(z, y + 3, y + 3, tid - 32, 96);
+    if (is_stage && mine && y + 2 < KN && row + 2 < rend) stage_row(z, y + 3, tid - 32);
     commit();
     if (pending >= 0 && mine) epilogue(pending, pending & 1);
     asm volatile("tcgen05.fence::before_thread_sync;");
