@@ -43,7 +43,11 @@ template <int N, int T> struct Col2Cfg {
   static constexpr int MINB = N == 810 ? 3 : 1;  // 80 registers at 810: three CTAs per SM
 };
 
-template <int N, int T, bool INV>
+// DRV: the launch carries derivative outputs (ColArgs::ndrv > 0).  Without it
+// the wavenumber scaling is compiled out; otherwise the compiler hoists the
+// int -> double -> float conversions of every element out of the `drv` branch
+// and pays for them on the XU pipe even for plain components.
+template <int N, int T, bool INV, bool DRV>
 __global__ void __launch_bounds__(Col2Cfg<N, T>::NT, Col2Cfg<N, T>::MINB)
 k_col2(const ColArgs a, const float2* __restrict__ tw) {
   using C = float2;
@@ -55,7 +59,7 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
   const int kx = blockIdx.x * T + t;
   const int c = blockIdx.y;
   const int q = blockIdx.z;
-  const bool drv = q >= a.ncomp;
+  const bool drv = DRV && q >= a.ncomp;
   const C* __restrict__ in = static_cast<const C*>(a.in[drv ? a.drv_src[q - a.ncomp] : q]);
   C* __restrict__ out = static_cast<C*>(a.out[q]);
   const bool live = kx < a.K1;
@@ -912,9 +916,16 @@ struct Col4Cfg {
   static size_t smem(int nin) { return size_t(XR + YR + 2 * nin) * T * sizeof(float2); }
 };
 
-template <bool INV, bool TRUNC>
+// Tile t = tx + ntx (c + ncols q); every CTA walks t = blockIdx.x + i gridDim.x
+// (ntiles < 2^31).  The walk advances (tx, c, q) incrementally, so the loop
+// runs no division.
+struct TileWalk {
+  int tx, c, q;
+};
+
+template <bool INV, bool TRUNC, bool DRV>
 __global__ void __launch_bounds__(Col4Cfg::NT, 1)
-k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles, int nin) {
+k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, int ntiles, int nin) {
   using C = float2;
   constexpr int N = 810, T = Col4Cfg::T, NT = Col4Cfg::NT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -924,7 +935,7 @@ k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles
   __shared__ const C* s_src[kMaxComp];
   __shared__ C* s_dst[kMaxComp];
   const int tid = threadIdx.x, col = tid % T, w = tid / T;  // w = 0 .. 89
-  const int nq = a.ncomp + (INV ? a.ndrv : 0);
+  const int nq = a.ncomp + (INV && DRV ? a.ndrv : 0);
   if (tid < kMaxComp) {
     // the component pointers by compile-time indices only (no local copy of the parameters)
     const int src = tid < a.ncomp ? tid : (tid < nq ? a.drv_src[tid - a.ncomp] : 0);
@@ -940,44 +951,58 @@ k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles
   }
   __syncthreads();
   const int Kc = a.kpos + a.kneg;
-  auto decode = [&](long long tile, int& tx, int& c, int& q) {
-    tx = int(tile % ntx);
-    const long long r = tile / ntx;
-    c = int(r % a.ncols);
-    q = int(r / a.ncols);
+  // element offsets of one component fit in 32 bits (at most ~3.5e8 elements)
+  const int ies = int(a.in_es), oes = int(a.out_es);
+  const int G = int(gridDim.x);
+  const int dtx = G % ntx, dr = G / ntx, dc = dr % a.ncols, dq = dr / a.ncols;
+  auto advance = [&](TileWalk t) {
+    t.tx += dtx;
+    const int carry = t.tx >= ntx;
+    t.tx -= carry ? ntx : 0;
+    t.c += dc + carry;
+    const int carry2 = t.c >= a.ncols;
+    t.c -= carry2 ? a.ncols : 0;
+    t.q += dq + carry2;
+    return t;
   };
-  auto issue = [&](long long tile, int b) {
-    int tx, c, q;
-    decode(tile, tx, c, q);
-    const C* src = s_src[q] + (long long)c * a.in_cs + tx * T;
-    C* dst = stg + size_t(b) * nin * T;
-    const int live = min(T, a.K1 - tx * T);
+  auto issue = [&](const TileWalk& t, int b) {
+    const C* src = s_src[t.q] + (long long)t.c * a.in_cs + t.tx * T;
+    C* dst = stg + b * nin * T;
+    const int live = min(T, a.K1 - t.tx * T);
     for (int i = tid; i < nin * T; i += NT) {
-      const int row = i / T, t = i - row * T;
-      if (t < live) cp_async8(dst + i, src + row * a.in_es + t);
+      const int row = i / T, tt = i - row * T;
+      if (tt < live) cp_async8(dst + i, src + (row * ies + tt));
     }
   };
   auto compact = [&](int k) { return k < a.kpos ? k : (k >= N - a.kneg ? k - N + Kc : -1); };
 
-  long long tile = blockIdx.x;
+  int tile = blockIdx.x;
+  TileWalk cur;
+  {
+    const int r = tile / ntx;
+    cur.tx = tile - r * ntx;
+    cur.c = r % a.ncols;
+    cur.q = r / a.ncols;
+  }
   int b = 0;
-  if (tile < ntiles) issue(tile, 0);
+  if (tile < ntiles) issue(cur, 0);
   cp_async_commit();
-  for (; tile < ntiles; tile += gridDim.x, b ^= 1) {
-    if (tile + gridDim.x < ntiles) issue(tile + gridDim.x, b ^ 1);  // its stage was last read before a barrier
+  for (; tile < ntiles; tile += G, b ^= 1) {
+    const TileWalk nxt = advance(cur);
+    if (tile + G < ntiles) issue(nxt, b ^ 1);  // its stage was last read before a barrier
     cp_async_commit();
     asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     __syncthreads();
-    int tx, c, q;
-    decode(tile, tx, c, q);
+    const int tx = cur.tx, c = cur.c, q = cur.q;
+    cur = nxt;
     const int kx = tx * T + col;
     const bool live = kx < a.K1;
-    const C* sg = stg + size_t(b) * nin * T + col;
+    const C* sg = stg + b * nin * T + col;
     if (INV) {
       // A: radix-10 over p of Z[81 p + t], twiddle exp(+2 pi i qq s_a / 90)
       if (w < 81) {
         const int t = w, qq = t / 9;
-        const bool drv = q >= a.ncomp;
+        const bool drv = DRV && q >= a.ncomp;
         const bool zo = a.zero_origin && kx == 0 && c == 0;
         C v[10];
 #pragma unroll
@@ -1027,9 +1052,9 @@ k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles
 #pragma unroll
         for (int m2 = 0; m2 < 9; ++m2) v[m2] = yi[m2 * T];
         DFT<9, true, C>::run(v);
-        C* dst = s_dst[q] + (long long)c * a.out_cs + kx;
+        C* dst = s_dst[q] + (long long)c * a.out_cs + kx + s1 * oes;
 #pragma unroll
-        for (int s2 = 0; s2 < 9; ++s2) dst[(long long)(s1 + 90 * s2) * a.out_es] = v[s2];
+        for (int s2 = 0; s2 < 9; ++s2) dst[90 * s2 * oes] = v[s2];
       }
     } else {
       // A: radix-9 over m1 of x = 90 m1 + m2, twiddle exp(-2 pi i m2 s1' / 810)
@@ -1072,7 +1097,7 @@ k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles
         for (int sb = 0; sb < 10; ++sb) {
           if (TRUNC && (sb == 4 || sb == 5)) continue;
           const int pc = compact(s1 + 9 * sa + 81 * sb);
-          if (pc >= 0) dst[(long long)pc * a.out_es] = v[sb];
+          if (pc >= 0) dst[pc * oes] = v[sb];
         }
       }
     }
@@ -1096,18 +1121,21 @@ template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
 
 static void init_col4() {
   const int mx = int(Col4Cfg::smem(810));
-  cudaFuncSetAttribute(k_col4<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  cudaFuncSetAttribute(k_col4<false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
 }
 
 template <int N> static void init_fast_n() {
   constexpr int T = col_tile<N>();
   set_smem2(k_col3<N, T, true>, Col3Cfg<N, T>::SMEM);
   set_smem2(k_col3<N, T, false>, Col3Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, true>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, true>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, false, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
   set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
   set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
@@ -1154,15 +1182,22 @@ static int num_sms() {
 template <bool INV> static void col4_launch(const ColArgs& a, const void* tw, cudaStream_t st) {
   constexpr int T = Col4Cfg::T;
   const int ntx = (a.K1 + T - 1) / T;
-  const long long ntiles = (long long)ntx * a.ncols * (a.ncomp + (INV ? a.ndrv : 0));
+  const bool drv = INV && a.ndrv > 0;
+  const int ntiles = ntx * a.ncols * (a.ncomp + (drv ? a.ndrv : 0));  // <= 51 * 810 * kMaxComp
   const int nin = INV ? a.kpos + a.kneg : 810;
   const bool trunc = a.kpos <= 324 && a.kneg <= 324;
-  long long grid = num_sms();
-  if (grid > ntiles) grid = ntiles;
+  const int grid = num_sms() < ntiles ? num_sms() : ntiles;
   const size_t sm = Col4Cfg::smem(nin);
   const float2* t2 = static_cast<const float2*>(tw);
-  if (trunc) k_col4<INV, true><<<unsigned(grid), Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
-  else k_col4<INV, false><<<unsigned(grid), Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+  if constexpr (INV) {
+    if (drv) {
+      if (trunc) k_col4<true, true, true><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+      else k_col4<true, false, true><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+      return;
+    }
+  }
+  if (trunc) k_col4<INV, true, false><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
+  else k_col4<INV, false, false><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
 }
 
 template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
@@ -1182,7 +1217,13 @@ template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, 
   }
   using Cfg = Col2Cfg<N, T>;
   dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
-  k_col2<N, T, INV><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  if constexpr (INV) {
+    if (a.ndrv > 0) {
+      k_col2<N, T, true, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+      return;
+    }
+  }
+  k_col2<N, T, INV, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
 }
 
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st) {
