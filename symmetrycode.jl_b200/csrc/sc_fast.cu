@@ -43,11 +43,24 @@ template <int N, int T> struct Col2Cfg {
   static constexpr int MINB = N == 810 ? 3 : 1;  // 80 registers at 810: three CTAs per SM
 };
 
+// Where a block of B consecutive transform indices e0 .. e0 + B - 1 falls in
+// the compact layout (kpos modes e < kpos kept in place, kneg modes
+// e >= N - kneg moved down by N - kpos - kneg): 0 every index kept in place,
+// 1 every index moved, 2 none kept, 3 the block straddles a boundary.
+constexpr int crange(int e0, int B, int N, int kpos, int kneg) {
+  return e0 + B - 1 < kpos ? 0 : (e0 >= N - kneg ? 1 : (e0 >= kpos && e0 + B - 1 < N - kneg ? 2 : 3));
+}
+
 // DRV: the launch carries derivative outputs (ColArgs::ndrv > 0).  Without it
 // the wavenumber scaling is compiled out; otherwise the compiler hoists the
 // int -> double -> float conversions of every element out of the `drv` branch
 // and pays for them on the XU pipe even for plain components.
-template <int N, int T, bool INV, bool DRV>
+// FULL: the transform axis has the 2/3-rule compact layout of the solver
+// (kpos = N/3 + 1, kneg = N/3), so which of each thread's N1 gathers (inverse)
+// or N2 stores (forward) touch a retained mode is known at compile time except
+// in the one block that straddles a boundary; the unused forward outputs are
+// then never formed.
+template <int N, int T, bool INV, bool DRV, bool FULL>
 __global__ void __launch_bounds__(Col2Cfg<N, T>::NT, Col2Cfg<N, T>::MINB)
 k_col2(const ColArgs a, const float2* __restrict__ tw) {
   using C = float2;
@@ -63,7 +76,9 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
   const C* __restrict__ in = static_cast<const C*>(a.in[drv ? a.drv_src[q - a.ncomp] : q]);
   C* __restrict__ out = static_cast<C*>(a.out[q]);
   const bool live = kx < a.K1;
-  const int Kc = a.kpos + a.kneg;
+  constexpr int KP = N / 3 + 1, KN = N / 3;
+  const int kpos = FULL ? KP : a.kpos, kneg = FULL ? KN : a.kneg;
+  const int Kc = kpos + kneg;
   // element offsets fit in 32 bits for every sweep (at most ~3.5e8 elements
   // per component), so the per-element address arithmetic stays 32-bit
   const int ies = int(a.in_es), oes = int(a.out_es);
@@ -75,11 +90,13 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
       for (int n1 = 0; n1 < N1; ++n1) {
         const int e = N2 * n1 + j;
         v[n1] = mk<C>(0.f, 0.f);
-        const int p = cpos(e, N, a.kpos, a.kneg);
+        const int rg = FULL ? crange(N2 * n1, N2, N, KP, KN) : 3;
+        if (rg == 2) continue;
+        const int p = rg == 0 ? e : (rg == 1 ? e - N + Kc : cpos(e, N, kpos, kneg));
         if (live && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
           v[n1] = __ldg(base + p * ies);
           if (drv) {
-            const float kk = float(a.kfac * double(p < a.kpos ? p : p - Kc));
+            const float kk = float(a.kfac * double(p < kpos ? p : p - Kc));
             v[n1] = mk<C>(-kk * v[n1].y, kk * v[n1].x);
           }
         }
@@ -118,8 +135,13 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
 #pragma unroll
       for (int k2 = 0; k2 < N2; ++k2) {
         const int e = j + N1 * k2;
-        if (e < a.kpos) obase[e * oes] = w[k2];
-        else if (e >= N - a.kneg) obase[(e - shift) * oes] = w[k2];
+        const int rg = FULL ? crange(N1 * k2, N1, N, KP, KN) : 3;
+        if (rg == 0) obase[e * oes] = w[k2];
+        else if (rg == 1) obase[(e - shift) * oes] = w[k2];
+        else if (rg == 3) {
+          if (e < kpos) obase[e * oes] = w[k2];
+          else if (e >= N - kneg) obase[(e - shift) * oes] = w[k2];
+        }
       }
     }
   }
@@ -1133,9 +1155,12 @@ template <int N> static void init_fast_n() {
   constexpr int T = col_tile<N>();
   set_smem2(k_col3<N, T, true>, Col3Cfg<N, T>::SMEM);
   set_smem2(k_col3<N, T, false>, Col3Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, true, true>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, true, false>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, false, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, true, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, true, true>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, false, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, true, false, true>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, false, false, false>, Col2Cfg<N, T>::SMEM);
+  set_smem2(k_col2<N, T, false, false, true>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
   set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
   set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
@@ -1154,16 +1179,16 @@ bool init_fast(int N) {
   return cudaGetLastError() == cudaSuccess;
 }
 
-// At 810 the inverse sweeps run the persistent three-level kernel (k_col4: the
-// zero-padded input is staged while the previous tile computes); the forward
-// sweeps, and every other size, run one two-level tile per CTA (k_col2), which
-// keeps shared-memory traffic at one exchange per element.  SC_COL_KERNEL=2
-// selects k_col2 for the 810 inverse sweeps too, SC_COL_KERNEL=3 the older
-// persistent two-level kernel.
+// Every column sweep runs one two-level tile per CTA (k_col2), which keeps
+// shared-memory traffic at one exchange per element and, at three CTAs per SM,
+// beats the persistent kernels in both directions (810^3 inverse y sweep, 81
+// planes: 0.166 ms k_col2 against 0.283 ms k_col4).  SC_COL_KERNEL=4 selects
+// the persistent three-level kernel (k_col4) for the 810 inverse sweeps,
+// SC_COL_KERNEL=3 the persistent two-level kernel (k_col3).
 static int col_variant() {
   static const int v = [] {
     const char* e = getenv("SC_COL_KERNEL");
-    return (e && (e[0] == '2' || e[0] == '3')) ? e[0] - '0' : 4;
+    return (e && (e[0] == '3' || e[0] == '4')) ? e[0] - '0' : 2;
   }();
   return v;
 }
@@ -1217,13 +1242,17 @@ template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, 
   }
   using Cfg = Col2Cfg<N, T>;
   dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
+  const float2* t2 = static_cast<const float2*>(tw);
+  const bool full = a.kpos == N / 3 + 1 && a.kneg == N / 3;
   if constexpr (INV) {
     if (a.ndrv > 0) {
-      k_col2<N, T, true, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+      if (full) k_col2<N, T, true, true, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+      else k_col2<N, T, true, true, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
       return;
     }
   }
-  k_col2<N, T, INV, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  if (full) k_col2<N, T, INV, false, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+  else k_col2<N, T, INV, false, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
 }
 
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st) {
