@@ -139,7 +139,8 @@ SC_API int sc_state_profile_rhs(sc_plan* plan, double visc, int reps, double* ms
  * right shape (allocated and freed inside; legacy default stream):
  * kernel 0 = y-inverse sweep (3 comps) over `count` z planes, 1 = y-forward
  * sweep (6 comps) over `count` z planes, 2 = the 3D x sweep with products over
- * `count` rows.  Returns the mean ms per launch over `reps` launches and the
+ * `count` rows, 3 / 4 = z-inverse / z-forward sweep of one component over the
+ * first `count` ky columns of a full-size cube (count <= 2 (n/3) + 1).  Returns the mean ms per launch over `reps` launches and the
  * algorithmic bytes of one launch.  Synchronous; used by the profiles and the
  * tile autotuning, not by the solver. */
 SC_API int sc_microbench(int kernel, int n, int dtype, long long count, int reps, double* ms, double* bytes);

@@ -1162,6 +1162,17 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
     if (kernel == 0) { ca.in_cs = (long long)K1 * K2; ca.in_es = K1; ca.out_cs = (long long)K1 * n; ca.out_es = K1; }
     else { ca.in_cs = (long long)K1 * n; ca.in_es = K1; ca.out_cs = (long long)K1 * K2; ca.out_es = K1; }
     b = (double)nin * esz * (kernel == 0 ? small : big) + (double)nout * esz * (kernel == 0 ? big : small);
+  } else if (kernel == 3 || kernel == 4) {
+    // z-inverse / z-forward geometry, one component, over the first `count` ky
+    // columns of a full-size cube: the lines keep the solver's z stride (one
+    // K1 x K2 plane), so TLB and DRAM-page behaviour match the full sweep.
+    if (count > K2) { cleanup(); return fail(SC_ERR_INVALID, "count exceeds the %d ky columns", K2); }
+    const size_t small = (size_t)K1 * K2 * K2, big = (size_t)K1 * K2 * n;
+    ca.in[0] = alloc(kernel == 3 ? small : big);
+    ca.out[0] = alloc(kernel == 3 ? big : small);
+    ca.ncomp = 1; ca.K1 = K1; ca.ncols = (int)count; ca.kpos = kc + 1; ca.kneg = kc;
+    ca.in_cs = K1; ca.in_es = (long long)K1 * K2; ca.out_cs = K1; ca.out_es = (long long)K1 * K2;
+    b = (double)esz * K1 * count * (K2 + n);
   } else if (kernel == 2) {  // 3D x sweep over `count` rows
     for (int c = 0; c < 3; ++c) xa.in[c] = alloc((size_t)K1 * count);
     for (int c = 0; c < 6; ++c) xa.out[c] = alloc((size_t)K1 * count);
@@ -1175,8 +1186,8 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   auto launch = [&]() {
-    if (kernel == 0) sc::launch_col_inv<R>(n, ca, tw, 0);
-    else if (kernel == 1) sc::launch_col_fwd<R>(n, ca, tw, 0);
+    if (kernel == 0 || kernel == 3) sc::launch_col_inv<R>(n, ca, tw, 0);
+    else if (kernel == 1 || kernel == 4) sc::launch_col_fwd<R>(n, ca, tw, 0);
     else sc::launch_xsweep_ns<R>(n, xa, tw, 0);
   };
   launch();

@@ -3,7 +3,9 @@
     python -m symcode.microbench --kernel x --n 810 --count 65610 [--dtype f32] [--reps 5]
 
 kernel: ``yinv`` (y-inverse sweep over COUNT z planes), ``yfwd`` (y-forward
-sweep over COUNT z planes) or ``x`` (3D x sweep with products over COUNT rows).
+sweep over COUNT z planes), ``x`` (3D x sweep with products over COUNT rows),
+``zinv`` / ``zfwd`` (z sweeps of one component over COUNT ky columns of a
+full-size cube, so the lines keep the solver's plane stride).
 Prints one JSON line with ms per launch, algorithmic bytes and GB/s.  Used to
 make small, self-contained cases of the exact kernels the solver runs (for
 ncu) and to compare tile shapes.
@@ -20,7 +22,7 @@ import sys
 
 from ._lib import check, lib
 
-KERNELS = {"yinv": 0, "yfwd": 1, "x": 2}
+KERNELS = {"yinv": 0, "yfwd": 1, "x": 2, "zinv": 3, "zfwd": 4}
 CNN_LAYERS = ((4, 32), (32, 32), (32, 32), (32, 6))
 
 
