@@ -96,7 +96,7 @@ struct sc_closure {
   void* ph2[6] = {};  // physical M1
   void* ph3[6] = {};  // physical S~ then m2
   void* ph4[3] = {};  // physical test-filtered velocity
-  void* bb[12] = {};  // batched-transform scratch (kx, ky, z)
+  void* bb[12] = {};  // batched-transform scratch (kx, ky, z), stored [ky][z][kx]
   void* cb[12] = {};  // batched-transform scratch (kx, y, z)
   double* dsum = nullptr;  // [<ML>, <MM>, c] (dynamic Smagorinsky); [a2, -, -, z] (CNN)
   // CNN closure
@@ -183,6 +183,50 @@ int upload_twiddles(sc_plan* p) {
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // ---------------------------------------------------------------------------
+// column-sweep geometry of the 3D transforms
+// ---------------------------------------------------------------------------
+// Between the z and y sweeps a field lives as (kx, ky, z), stored [ky][z][kx]:
+// element kx + K1 (z + n ky).  The compact cube is [kz][ky][kx], so every z
+// line of it spans all kz planes (one plane = K1 (2k+1) elements, 1.17 MB at
+// 810^3 FP32) and touches hundreds of 2 MB pages.  With z innermost in the
+// intermediate, each z sweep has one such page-spread side instead of two and
+// each y sweep gets one: at 810^3 the four sweeps of one right-hand side take
+// about 8.1 ms instead of 9.0 ms with a [z][ky][kx] intermediate.
+// Inverse z: compact cube (K1 x K2 x K2) -> intermediate, k = 0 masked.
+sc::ColArgs z_inverse_args(int K1, int K2, int n, int kc) {
+  sc::ColArgs a{};
+  a.K1 = K1; a.ncols = K2;
+  a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = (long long)K1 * n; a.out_es = K1;
+  a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+  return a;
+}
+// Inverse y: intermediate -> physical-(y, z) rows [z][y][kx].
+sc::ColArgs y_inverse_args(int K1, int n, int kc) {
+  sc::ColArgs b{};
+  b.K1 = K1; b.ncols = n;
+  b.in_cs = K1; b.in_es = (long long)K1 * n; b.out_cs = (long long)K1 * n; b.out_es = K1;
+  b.kpos = kc + 1; b.kneg = kc;
+  return b;
+}
+// Forward y: rows [z][y][kx] (x extent K1) -> intermediate (ky pruned to 2 kout + 1).
+sc::ColArgs y_forward_args(int K1, int n, int kout) {
+  sc::ColArgs f{};
+  f.K1 = K1; f.ncols = n;
+  f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = K1; f.out_es = (long long)K1 * n;
+  f.kpos = kout + 1; f.kneg = kout;
+  return f;
+}
+// Forward z: intermediate -> compact cube of half-width kout (x extent K1 = kout + 1).
+sc::ColArgs z_forward_args(int K1, int n, int kout) {
+  sc::ColArgs g{};
+  const int K2 = 2 * kout + 1;
+  g.K1 = K1; g.ncols = K2;
+  g.in_cs = (long long)K1 * n; g.in_es = K1; g.out_cs = K1; g.out_es = (long long)K1 * K2;
+  g.kpos = kout + 1; g.kneg = kout;
+  return g;
+}
+
+// ---------------------------------------------------------------------------
 // the five-sweep product pipeline: compact u -> compact F[u_i u_j]/n^D in p->sig
 // ---------------------------------------------------------------------------
 // `ev` (optional): events recorded after each launch, ev[0] before the first.
@@ -194,23 +238,20 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
   const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
   if (kout < 0) kout = kc;
   if (!sig) sig = p->sig;
-  const int K1o = kout + 1, K2o = 2 * kout + 1;
+  const int K1o = kout + 1;
   int iev = 0;
   auto mark = [&]() { if (ev) cudaEventRecord(ev[iev++], st); };
   mark();
   sc::ColArgs a{};
   if (p->D == 3) {
+    a = z_inverse_args(K1, K2, n, kc);
     for (int c = 0; c < 3; ++c) { a.in[c] = u[c]; a.out[c] = p->be[c]; }
-    a.ncomp = 3; a.K1 = K1; a.ncols = K2;
-    a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
-    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    a.ncomp = 3;
     if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
     mark();
-    sc::ColArgs b{};
+    sc::ColArgs b = y_inverse_args(K1, n, kc);
     for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
-    b.ncomp = 3; b.K1 = K1; b.ncols = n;
-    b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
-    b.kpos = kc + 1; b.kneg = kc;
+    b.ncomp = 3;
     sc::launch_col_inv<R>(n, b, p->tw, st);
     mark();
     sc::XArgs x{};
@@ -219,18 +260,14 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
     x.D = 3; x.K1in = K1; x.K1out = K1o; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
     mark();
-    sc::ColArgs f{};
+    sc::ColArgs f = y_forward_args(K1o, n, kout);
     for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
-    f.ncomp = 6; f.K1 = K1o; f.ncols = n;
-    f.in_cs = (long long)K1o * n; f.in_es = K1o; f.out_cs = (long long)K1o * K2o; f.out_es = K1o;
-    f.kpos = kout + 1; f.kneg = kout;
+    f.ncomp = 6;
     sc::launch_col_fwd<R>(n, f, p->tw, st);
     mark();
-    sc::ColArgs g{};
+    sc::ColArgs g = z_forward_args(K1o, n, kout);
     for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = sig[c]; }
-    g.ncomp = 6; g.K1 = K1o; g.ncols = K2o;
-    g.in_cs = K1o; g.in_es = (long long)K1o * K2o; g.out_cs = K1o; g.out_es = (long long)K1o * K2o;
-    g.kpos = kout + 1; g.kneg = kout;
+    g.ncomp = 6;
     sc::launch_col_fwd<R>(n, g, p->tw, st);
     mark();
   } else {
@@ -269,16 +306,13 @@ int c2p_batch(sc_plan* p, void* const* bb, void* const* cb, void* const* in, voi
     const int mc = m - c0 < 12 ? m - c0 : 12;
     sc::ColArgs a{};
     if (p->D == 3) {
+      a = z_inverse_args(K1, K2, n, kc);
       for (int c = 0; c < mc; ++c) { a.in[c] = in[c0 + c]; a.out[c] = bb[c]; }
-      a.ncomp = mc; a.K1 = K1; a.ncols = K2;
-      a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
-      a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+      a.ncomp = mc;
       sc::launch_col_inv<R>(n, a, p->tw, st);
-      sc::ColArgs b{};
+      sc::ColArgs b = y_inverse_args(K1, n, kc);
       for (int c = 0; c < mc; ++c) { b.in[c] = bb[c]; b.out[c] = cb[c]; }
-      b.ncomp = mc; b.K1 = K1; b.ncols = n;
-      b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
-      b.kpos = kc + 1; b.kneg = kc;
+      b.ncomp = mc;
       sc::launch_col_inv<R>(n, b, p->tw, st);
     } else {
       for (int c = 0; c < mc; ++c) { a.in[c] = in[c0 + c]; a.out[c] = cb[c]; }
@@ -308,16 +342,13 @@ int p2c_batch(sc_plan* p, void* const* bb, void* const* cb, void* const* in, voi
     sc::launch_x_r2c<R>(n, x, p->tw, st);
     sc::ColArgs f{};
     if (p->D == 3) {
+      f = y_forward_args(K1, n, kc);
       for (int c = 0; c < mc; ++c) { f.in[c] = cb[c]; f.out[c] = bb[c]; }
-      f.ncomp = mc; f.K1 = K1; f.ncols = n;
-      f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = (long long)K1 * K2; f.out_es = K1;
-      f.kpos = kc + 1; f.kneg = kc;
+      f.ncomp = mc;
       sc::launch_col_fwd<R>(n, f, p->tw, st);
-      sc::ColArgs g{};
+      sc::ColArgs g = z_forward_args(K1, n, kc);
       for (int c = 0; c < mc; ++c) { g.in[c] = bb[c]; g.out[c] = out[c0 + c]; }
-      g.ncomp = mc; g.K1 = K1; g.ncols = K2;
-      g.in_cs = K1; g.in_es = (long long)K1 * K2; g.out_cs = K1; g.out_es = (long long)K1 * K2;
-      g.kpos = kc + 1; g.kneg = kc;
+      g.ncomp = mc;
       sc::launch_col_fwd<R>(n, g, p->tw, st);
     } else {
       for (int c = 0; c < mc; ++c) { f.in[c] = cb[c]; f.out[c] = out[c0 + c]; }
@@ -1154,24 +1185,26 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
   sc::XArgs xa{};
   double b = 0;
   const int nin = kernel == 1 ? 6 : 3, nout = kernel == 0 ? 3 : 6;
-  if (kernel == 0 || kernel == 1) {  // y-inverse / y-forward geometry over `count` z planes
-    const size_t small = (size_t)K1 * K2 * count, big = (size_t)K1 * n * count;
-    for (int c = 0; c < nin; ++c) ca.in[c] = alloc(kernel == 0 ? small : big);
-    for (int c = 0; c < nout; ++c) ca.out[c] = alloc(kernel == 0 ? big : small);
-    ca.ncomp = nout; ca.K1 = K1; ca.ncols = (int)count; ca.kpos = kc + 1; ca.kneg = kc;
-    if (kernel == 0) { ca.in_cs = (long long)K1 * K2; ca.in_es = K1; ca.out_cs = (long long)K1 * n; ca.out_es = K1; }
-    else { ca.in_cs = (long long)K1 * n; ca.in_es = K1; ca.out_cs = (long long)K1 * K2; ca.out_es = K1; }
-    b = (double)nin * esz * (kernel == 0 ? small : big) + (double)nout * esz * (kernel == 0 ? big : small);
+  if (kernel == 0 || kernel == 1) {
+    // y-inverse (3 comps) / y-forward (6 comps) of the solver over `count` z
+    // planes: the (kx, ky, z) side is a full-size intermediate, so its lines
+    // keep the solver's strides
+    if (count > n) { cleanup(); return fail(SC_ERR_INVALID, "count exceeds the %d z planes", n); }
+    const size_t mid = (size_t)K1 * n * K2, rows = (size_t)K1 * n * count;
+    ca = kernel == 0 ? y_inverse_args(K1, n, kc) : y_forward_args(K1, n, kc);
+    for (int c = 0; c < nin; ++c) ca.in[c] = alloc(kernel == 0 ? mid : rows);
+    for (int c = 0; c < nout; ++c) ca.out[c] = alloc(kernel == 0 ? rows : mid);
+    ca.ncomp = nout; ca.ncols = (int)count;
+    b = (double)(nin + nout) / 2 * esz * K1 * count * (K2 + n);
   } else if (kernel == 3 || kernel == 4) {
-    // z-inverse / z-forward geometry, one component, over the first `count` ky
-    // columns of a full-size cube: the lines keep the solver's z stride (one
-    // K1 x K2 plane), so TLB and DRAM-page behaviour match the full sweep.
+    // z-inverse / z-forward of the solver, one component, over the first
+    // `count` ky columns of a full-size cube and intermediate
     if (count > K2) { cleanup(); return fail(SC_ERR_INVALID, "count exceeds the %d ky columns", K2); }
-    const size_t small = (size_t)K1 * K2 * K2, big = (size_t)K1 * K2 * n;
-    ca.in[0] = alloc(kernel == 3 ? small : big);
-    ca.out[0] = alloc(kernel == 3 ? big : small);
-    ca.ncomp = 1; ca.K1 = K1; ca.ncols = (int)count; ca.kpos = kc + 1; ca.kneg = kc;
-    ca.in_cs = K1; ca.in_es = (long long)K1 * K2; ca.out_cs = K1; ca.out_es = (long long)K1 * K2;
+    const size_t cube = (size_t)K1 * K2 * K2, mid = (size_t)K1 * n * K2;
+    ca = kernel == 3 ? z_inverse_args(K1, K2, n, kc) : z_forward_args(K1, n, kc);
+    ca.in[0] = alloc(kernel == 3 ? cube : mid);
+    ca.out[0] = alloc(kernel == 3 ? mid : cube);
+    ca.ncomp = 1; ca.ncols = (int)count;
     b = (double)esz * K1 * count * (K2 + n);
   } else if (kernel == 2) {  // 3D x sweep over `count` rows
     for (int c = 0; c < 3; ++c) xa.in[c] = alloc((size_t)K1 * count);
@@ -1723,17 +1756,13 @@ int vmax_impl(sc_plan* p, void* const* uc, double* vmax, cudaStream_t st) {
   // y/z inverse of the D components (zero-padded, k = 0 masked) into the pencil scratch
   const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc, D = p->D;
   if (D == 3) {
-    sc::ColArgs a{};
+    sc::ColArgs a = z_inverse_args(K1, K2, n, kc);
     for (int c = 0; c < 3; ++c) { a.in[c] = uc[c]; a.out[c] = p->be[c]; }
-    a.ncomp = 3; a.K1 = K1; a.ncols = K2;
-    a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1; a.out_es = (long long)K1 * K2;
-    a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+    a.ncomp = 3;
     sc::launch_col_inv<R>(n, a, p->tw, st);
-    sc::ColArgs b{};
+    sc::ColArgs b = y_inverse_args(K1, n, kc);
     for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
-    b.ncomp = 3; b.K1 = K1; b.ncols = n;
-    b.in_cs = (long long)K1 * K2; b.in_es = K1; b.out_cs = (long long)K1 * n; b.out_es = K1;
-    b.kpos = kc + 1; b.kneg = kc;
+    b.ncomp = 3;
     sc::launch_col_inv<R>(n, b, p->tw, st);
   } else {
     sc::ColArgs a{};
@@ -1963,15 +1992,13 @@ int stage_adjoint(sc_plan* p, sc_closure* cl, void* const* u, void* const* lam, 
     const int n = p->n, K1 = p->K1, K2 = p->K2, kc = p->kc;
     for (int c0 = 0; c0 < NP; c0 += 12) {
       const int mc = NP - c0 < 12 ? NP - c0 : 12;
-      sc::ColArgs a{};
+      sc::ColArgs a = z_inverse_args(K1, K2, n, kc);
       for (int c = 0; c < mc; ++c) { a.in[c] = lsig[c0 + c]; a.out[c] = cl->bb[c]; }
-      a.ncomp = mc; a.K1 = K1; a.ncols = K2; a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = K1;
-      a.out_es = (long long)K1 * K2; a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
+      a.ncomp = mc;
       sc::launch_col_inv<R>(n, a, p->tw, st);
-      sc::ColArgs b{};
+      sc::ColArgs b = y_inverse_args(K1, n, kc);
       for (int c = 0; c < mc; ++c) { b.in[c] = cl->bb[c]; b.out[c] = cl->cb[c]; }
-      b.ncomp = mc; b.K1 = K1; b.ncols = n; b.in_cs = (long long)K1 * K2; b.in_es = K1;
-      b.out_cs = (long long)K1 * n; b.out_es = K1; b.kpos = kc + 1; b.kneg = kc;
+      b.ncomp = mc;
       sc::launch_col_inv<R>(n, b, p->tw, st);
       sc::XPlainArgs x{};
       for (int c = 0; c < mc; ++c) { x.in[c] = cl->cb[c]; x.out[c] = m[c0 + c]; }
