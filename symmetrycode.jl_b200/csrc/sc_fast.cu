@@ -159,6 +159,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -734,12 +738,28 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
     const C* in0 = static_cast<const C*>(a.in[0]);
     const C* in1 = static_cast<const C*>(a.in[1]);
     const C* in2 = static_cast<const C*>(a.in[2]);
-    for (int i = t; i < 6 * K1; i += X4Cfg::NT) {
-      const int cr = i / K1, kx = i - cr * K1;
-      const C* src = cr < 2 ? in0 : cr < 4 ? in1 : in2;  // no dynamic index into the parameter array
-      C* dst = rin + i;
-      if ((cr & 1) == 0 || has1) cp_async8(dst, src + (r0 + (cr & 1)) * K1 + kx);
-      else *dst = make_float2(0.f, 0.f);
+    // FULL with both rows present: rows r0 (even) and r0 + 1 of a component are
+    // 2 x 271 contiguous elements starting 4336 r0/2 bytes into the component,
+    // so with 16-byte aligned components each row pair is 271 16-byte copies
+    const bool pair16 =
+        FULL && has1 &&
+        ((reinterpret_cast<unsigned long long>(in0) | reinterpret_cast<unsigned long long>(in1) |
+          reinterpret_cast<unsigned long long>(in2)) & 15) == 0;
+    if (pair16) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const C* src = (c == 0 ? in0 : c == 1 ? in1 : in2) + r0 * K1;
+        C* dst = rin + 2 * c * K1;
+        for (int j = t; j < K1; j += X4Cfg::NT) cp_async16_cg(dst + 2 * j, src + 2 * j);
+      }
+    } else {
+      for (int i = t; i < 6 * K1; i += X4Cfg::NT) {
+        const int cr = i / K1, kx = i - cr * K1;
+        const C* src = cr < 2 ? in0 : cr < 4 ? in1 : in2;  // no dynamic index into the parameter array
+        C* dst = rin + i;
+        if ((cr & 1) == 0 || has1) cp_async8(dst, src + (r0 + (cr & 1)) * K1 + kx);
+        else *dst = make_float2(0.f, 0.f);
+      }
     }
   }
   cp_async_commit();
@@ -905,7 +925,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
   for (int it = t; it < 2 * K1o; it += X4Cfg::NT) {
     const int rr = it >= K1o, kx = it - rr * K1o;
     if (rr == 1 && !has1) continue;
-    const long long o = (r0 + rr) * K1o + kx;
+    const int o = int(r0 + rr) * K1o + kx;  // < 810^2 rows x 406: 32-bit
     const C* zs = rr ? reg1 : reg0;
     const int kc = kx == 0 ? 0 : ko + kx;
 #pragma unroll
