@@ -694,26 +694,32 @@ __device__ __forceinline__ float2 x4_gather(const float2* ra, const float2* rb, 
   return make_float2(0.f, 0.f);
 }
 
-// products of one row at this thread's 9 points, first forward radix-9, twiddle
-__device__ __forceinline__ void x4_f1_row(const float* u1, const float* u2, const float* u3, float sc,
-                                          const float2* wf, float2* region, int t) {
+// products of one row at this thread's 9 points, first forward radix-9, twiddle.
+// KIND selects the pencil at compile time (0: u1 u1 + i u2 u2, 1: u3 u3 + i u1 u2,
+// 2: u2 u3 + i u3 u1), so each point costs two multiplies and no selects.
+template <int KIND>
+__device__ __forceinline__ void x4_f1_kind(const float* u1, const float* u2, const float* u3,
+                                           const float2* wf, float2* region, int t) {
   using C = float2;
-#pragma unroll 1
-  for (int kind = 0; kind < 3; ++kind) {
-    C v[9];
+  C v[9];
 #pragma unroll
-    for (int m1 = 0; m1 < 9; ++m1) {
-      const float a1 = u1[m1], a2 = u2[m1], a3 = u3[m1];
-      const float pa = kind == 0 ? a1 * a1 : kind == 1 ? a3 * a3 : a2 * a3;
-      const float pb = kind == 0 ? a2 * a2 : kind == 1 ? a1 * a2 : a3 * a1;
-      v[m1] = make_float2(pa * sc, pb * sc);
-    }
-    DFT<9, false, C>::run(v);
-    C* ws = region + kind * X4Cfg::PS + t;
-    ws[0] = v[0];
-#pragma unroll
-    for (int s = 1; s < 9; ++s) ws[90 * s] = cmul(v[s], wf[s]);
+  for (int m1 = 0; m1 < 9; ++m1) {
+    const float a1 = u1[m1], a2 = u2[m1], a3 = u3[m1];
+    const float pa = KIND == 0 ? a1 * a1 : KIND == 1 ? a3 * a3 : a2 * a3;
+    const float pb = KIND == 0 ? a2 * a2 : KIND == 1 ? a1 * a2 : a3 * a1;
+    v[m1] = make_float2(pa, pb);
   }
+  DFT<9, false, C>::run(v);
+  C* ws = region + KIND * X4Cfg::PS + t;
+  ws[0] = v[0];
+#pragma unroll
+  for (int s = 1; s < 9; ++s) ws[90 * s] = cmul(v[s], wf[s]);
+}
+__device__ __forceinline__ void x4_f1_row(const float* u1, const float* u2, const float* u3,
+                                          const float2* wf, float2* region, int t) {
+  x4_f1_kind<0>(u1, u2, u3, wf, region, t);
+  x4_f1_kind<1>(u1, u2, u3, wf, region, t);
+  x4_f1_kind<2>(u1, u2, u3, wf, region, t);
 }
 
 template <bool FULL>
@@ -810,7 +816,8 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
   }
   __syncthreads();
   // Ic + F1
-  const float sc = float(a.scale);
+  // the products enter the forward transform unscaled; the 1/n^D scale is
+  // applied with the 1/2 of the final split (the transform is linear)
   float u1[9], u2[9], u3[9], u3b[9];
   C wf[9];
   if (t < 90) {
@@ -829,7 +836,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
     DFT<9, true, C>::run(v);
 #pragma unroll
     for (int s = 0; s < 9; ++s) { u3[s] = v[s].x; u3b[s] = v[s].y; }
-    x4_f1_row(u1, u2, u3, sc, wf, reg0, t);
+    x4_f1_row(u1, u2, u3, wf, reg0, t);
     const C* yc = reg1 + PS + 9 * t;
 #pragma unroll
     for (int m2 = 0; m2 < 9; ++m2) v[m2] = yc[m2];
@@ -838,7 +845,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
     for (int s = 0; s < 9; ++s) { u1[s] = v[s].x; u2[s] = v[s].y; }
   }
   __syncthreads();
-  if (t < 90) x4_f1_row(u1, u2, u3b, sc, wf, reg1, t);
+  if (t < 90) x4_f1_row(u1, u2, u3b, wf, reg1, t);
   __syncthreads();
   // F2, in place per region: read all three pencils, barrier, write
   {
@@ -916,6 +923,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
   }
   __syncthreads();
   // S
+  const float hsc = 0.5f * float(a.scale);
   C* o0 = static_cast<C*>(a.out[0]);
   C* o1 = static_cast<C*>(a.out[1]);
   C* o2 = static_cast<C*>(a.out[2]);
@@ -933,8 +941,8 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
       const C z = zs[b * PS + kx], zc = zs[b * PS + kc];
       C* oa = b == 0 ? o0 : b == 1 ? o2 : o4;
       C* ob = b == 0 ? o1 : b == 1 ? o3 : o5;
-      oa[o] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-      ob[o] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+      oa[o] = make_float2(hsc * (z.x + zc.x), hsc * (z.y - zc.y));
+      ob[o] = make_float2(hsc * (z.y + zc.y), hsc * (zc.x - z.x));
     }
   }
 }
