@@ -540,8 +540,8 @@ def run_gpu(args):
            "y_forward": per["y_forward"], "z_forward": 6 * b + 6 * a, "epilogue": 12 * a}
     dom = max(kms, key=lambda kk: kms[kk])
     # DRAM traffic of the x sweep from one ncu capture (profiles/k_xsweep4_810_x_sweep_65610_rows.md:
-    # 426.8 MB read + 798.4 MB written for 65610 rows), scaled to the launch's n^2 rows
-    traffic = (426.779904e6 + 798.434048e6) / 65610 * n * n if (dom == "x_sweep" and n == 810) else None
+    # 426.9 MB read + 796.2 MB written for 65610 rows), scaled to the launch's n^2 rows
+    traffic = (426.917376e6 + 796.224256e6) / 65610 * n * n if (dom == "x_sweep" and n == 810) else None
     hbm, src = peaks()
     achieved = alg[dom] / (kms[dom] / 1e3) / 1e9
     step_bytes = 4 * b_rhs
