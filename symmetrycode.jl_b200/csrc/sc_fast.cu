@@ -148,13 +148,8 @@ k_col2(const ColArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
-// persistent column sweep with cp.async prefetch of the next tile
+// asynchronous global -> shared copies
 // ---------------------------------------------------------------------------
-// Each CTA walks tiles blockIdx.x, blockIdx.x + gridDim.x, ...  The tile's
-// stored rows (the compact rows on the inverse side, all N on the forward
-// side) are copied asynchronously into a shared stage; as soon as step 1 has
-// read the stage, the copies of the next tile are issued, so they overlap
-// step 2 (and the other resident CTA).
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -165,116 +160,6 @@ __device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-template <int N, int T> struct Col3Cfg {
-  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
-  static constexpr int NJ = N1 > N2 ? N1 : N2;
-  static constexpr int NT = T * NJ;
-  static constexpr int SR = N2 * T + 8;
-  static constexpr size_t STAGE = size_t(N) * T * sizeof(float2);
-  static constexpr size_t SMEM = STAGE + size_t(N1) * SR * sizeof(float2);
-};
-
-template <int N, int T, bool INV>
-__device__ __forceinline__ void col3_issue(const ColArgs& a, float2* stage, long long tile, int ntx, int Kc) {
-  constexpr int NT = Col3Cfg<N, T>::NT;
-  const int kxt = int(tile % ntx);
-  const long long r = tile / ntx;
-  const int c = int(r % a.ncols);
-  const int q = int(r / a.ncols);
-  const bool drv = q >= a.ncomp;
-  const float2* in = static_cast<const float2*>(a.in[drv ? a.drv_src[q - a.ncomp] : q]);
-  const int kx0 = kxt * T;
-  const float2* base = in + kx0 + (long long)c * a.in_cs;
-  const int rows = INV ? Kc : N;
-  for (int idx = threadIdx.x; idx < rows * T; idx += NT) {
-    const int row = idx / T, tt = idx % T;
-    if (kx0 + tt < a.K1) {
-      const int e = INV ? (row < a.kpos ? row : row + N - Kc) : row;
-      cp_async8(stage + e * T + tt, base + tt + (long long)row * a.in_es);
-    }
-  }
-}
-
-template <int N, int T, bool INV>
-__global__ void __launch_bounds__(Col3Cfg<N, T>::NT, 2)
-k_col3(const ColArgs a, const float2* __restrict__ tw, int ntx, long long ntiles) {
-  using C = float2;
-  using Cfg = Col3Cfg<N, T>;
-  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, SR = Cfg::SR;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* stage = reinterpret_cast<C*>(smem_raw);
-  C* ys = reinterpret_cast<C*>(smem_raw + Cfg::STAGE);
-  const int t = threadIdx.x % T, j = threadIdx.x / T;
-  const int Kc = a.kpos + a.kneg;
-  long long tile = blockIdx.x;
-  if (tile < ntiles) col3_issue<N, T, INV>(a, stage, tile, ntx, Kc);
-  cp_async_commit();
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int kxt = int(tile % ntx);
-    const long long r = tile / ntx;
-    const int c = int(r % a.ncols);
-    const int q = int(r / a.ncols);
-    const bool drv = q >= a.ncomp;
-    const int kx = kxt * T + t;
-    const bool live = kx < a.K1;
-    cp_async_wait_all();
-    __syncthreads();
-    if (j < N2) {
-      C v[N1];
-#pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) {
-        const int e = N2 * n1 + j;
-        v[n1] = make_float2(0.f, 0.f);
-        if (INV) {
-          const int p = cpos(e, N, a.kpos, a.kneg);
-          if (live && p >= 0 && !(a.zero_origin && kx == 0 && c == 0 && p == 0)) {
-            v[n1] = stage[e * T + t];
-            if (drv) {
-              const float kk = float(a.kfac * double(p < a.kpos ? p : p - Kc));
-              v[n1] = make_float2(-kk * v[n1].y, kk * v[n1].x);
-            }
-          }
-        } else if (live) {
-          v[n1] = stage[e * T + t];
-        }
-      }
-      DFT<N1, INV, C>::run(v);
-#pragma unroll
-      for (int k1 = 1; k1 < N1; ++k1) {
-        C w = __ldg(&tw[j * k1]);
-        if (INV) w.y = -w.y;
-        v[k1] = cmul(v[k1], w);
-      }
-#pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) ys[k1 * SR + j * T + t] = v[k1];
-    }
-    __syncthreads();
-    {
-      const long long next = tile + gridDim.x;
-      if (next < ntiles) col3_issue<N, T, INV>(a, stage, next, ntx, Kc);
-      cp_async_commit();
-    }
-    if (j < N1 && live) {
-      C w[N2];
-#pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) w[n2] = ys[j * SR + n2 * T + t];
-      DFT<N2, INV, C>::run(w);
-      C* obase = static_cast<C*>(a.out[q]) + kx + (long long)c * a.out_cs;
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) {
-        const int e = j + N1 * k2;
-        if (INV) {
-          obase[(long long)e * a.out_es] = w[k2];
-        } else {
-          const int p = cpos(e, N, a.kpos, a.kneg);
-          if (p >= 0) obase[(long long)p * a.out_es] = w[k2];
-        }
-      }
-    }
-  }
-  cp_async_wait_all();
-}
 
 // ---------------------------------------------------------------------------
 // x sweep with the Navier-Stokes products (rows are contiguous)
@@ -948,219 +833,6 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
-// Persistent column sweep for N = 810 = 9 * 9 * 10 (FP32), both directions.
-// A tile is T = 8 consecutive kx of one column c of one component q.  The
-// tile's stored rows are copied asynchronously (cp.async, 8 B per element)
-// into one of two shared stages while the previous tile is transformed, so
-// the copies of tile i+1 overlap the three radix passes of tile i.  The passes
-// follow the four-step mapping of the 810 x sweep (k = 9 m1 + m2 inverse,
-// x = 90 m1 + m2 forward) with 90 threads per column; shared arrays are
-// [index][kx], so a warp touches 4 indices x 8 kx and global rows stay
-// 64-byte coalesced.  TRUNC: the transform axis is 2/3-truncated (kpos,
-// kneg <= 324), so inputs 324 <= k <= 485 (inverse) are zero and those
-// outputs (forward) are never stored.
-// ---------------------------------------------------------------------------
-struct Col4Cfg {
-  static constexpr int N = 810, T = 8, NT = 720;
-  static constexpr int XR = 882, YR = 810;  // rows of the two exchange arrays
-  static size_t smem(int nin) { return size_t(XR + YR + 2 * nin) * T * sizeof(float2); }
-};
-
-// Tile t = tx + ntx (c + ncols q); every CTA walks t = blockIdx.x + i gridDim.x
-// (ntiles < 2^31).  The walk advances (tx, c, q) incrementally, so the loop
-// runs no division.
-struct TileWalk {
-  int tx, c, q;
-};
-
-template <bool INV, bool TRUNC, bool DRV>
-__global__ void __launch_bounds__(Col4Cfg::NT, 1)
-k_col4(const ColArgs a, const float2* __restrict__ tw, int ntx, int ntiles, int nin) {
-  using C = float2;
-  constexpr int N = 810, T = Col4Cfg::T, NT = Col4Cfg::NT;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* xs = reinterpret_cast<C*>(smem_raw);  // [XR][T]
-  C* ys = xs + Col4Cfg::XR * T;           // [YR][T]
-  C* stg = ys + Col4Cfg::YR * T;          // [2][nin][T]
-  __shared__ const C* s_src[kMaxComp];
-  __shared__ C* s_dst[kMaxComp];
-  const int tid = threadIdx.x, col = tid % T, w = tid / T;  // w = 0 .. 89
-  const int nq = a.ncomp + (INV && DRV ? a.ndrv : 0);
-  if (tid < kMaxComp) {
-    // the component pointers by compile-time indices only (no local copy of the parameters)
-    const int src = tid < a.ncomp ? tid : (tid < nq ? a.drv_src[tid - a.ncomp] : 0);
-    const void* ps = nullptr;
-    void* pd = nullptr;
-#pragma unroll
-    for (int j = 0; j < kMaxComp; ++j) {
-      if (j == src) ps = a.in[j];
-      if (j == tid) pd = a.out[j];
-    }
-    s_src[tid] = static_cast<const C*>(ps);
-    s_dst[tid] = static_cast<C*>(pd);
-  }
-  __syncthreads();
-  const int Kc = a.kpos + a.kneg;
-  // element offsets of one component fit in 32 bits (at most ~3.5e8 elements)
-  const int ies = int(a.in_es), oes = int(a.out_es);
-  const int G = int(gridDim.x);
-  const int dtx = G % ntx, dr = G / ntx, dc = dr % a.ncols, dq = dr / a.ncols;
-  auto advance = [&](TileWalk t) {
-    t.tx += dtx;
-    const int carry = t.tx >= ntx;
-    t.tx -= carry ? ntx : 0;
-    t.c += dc + carry;
-    const int carry2 = t.c >= a.ncols;
-    t.c -= carry2 ? a.ncols : 0;
-    t.q += dq + carry2;
-    return t;
-  };
-  auto issue = [&](const TileWalk& t, int b) {
-    const C* src = s_src[t.q] + (long long)t.c * a.in_cs + t.tx * T;
-    C* dst = stg + b * nin * T;
-    const int live = min(T, a.K1 - t.tx * T);
-    for (int i = tid; i < nin * T; i += NT) {
-      const int row = i / T, tt = i - row * T;
-      if (tt < live) cp_async8(dst + i, src + (row * ies + tt));
-    }
-  };
-  auto compact = [&](int k) { return k < a.kpos ? k : (k >= N - a.kneg ? k - N + Kc : -1); };
-
-  int tile = blockIdx.x;
-  TileWalk cur;
-  {
-    const int r = tile / ntx;
-    cur.tx = tile - r * ntx;
-    cur.c = r % a.ncols;
-    cur.q = r / a.ncols;
-  }
-  int b = 0;
-  if (tile < ntiles) issue(cur, 0);
-  cp_async_commit();
-  for (; tile < ntiles; tile += G, b ^= 1) {
-    const TileWalk nxt = advance(cur);
-    if (tile + G < ntiles) issue(nxt, b ^ 1);  // its stage was last read before a barrier
-    cp_async_commit();
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-    __syncthreads();
-    const int tx = cur.tx, c = cur.c, q = cur.q;
-    cur = nxt;
-    const int kx = tx * T + col;
-    const bool live = kx < a.K1;
-    const C* sg = stg + b * nin * T + col;
-    if (INV) {
-      // A: radix-10 over p of Z[81 p + t], twiddle exp(+2 pi i qq s_a / 90)
-      if (w < 81) {
-        const int t = w, qq = t / 9;
-        const bool drv = DRV && q >= a.ncomp;
-        const bool zo = a.zero_origin && kx == 0 && c == 0;
-        C v[10];
-#pragma unroll
-        for (int p = 0; p < 10; ++p) {
-          v[p] = make_float2(0.f, 0.f);
-          if (TRUNC && (p == 4 || p == 5)) continue;
-          const int pc = compact(81 * p + t);
-          if (pc < 0 || (zo && pc == 0)) continue;
-          C x = sg[pc * T];
-          if (drv) {
-            const float kk = float(a.kfac * double(pc < a.kpos ? pc : pc - Kc));
-            x = make_float2(-kk * x.y, kk * x.x);
-          }
-          v[p] = x;
-        }
-        DFT<10, true, C>::run(v);
-        C* xo = xs + t * T + col;
-        xo[0] = v[0];
-#pragma unroll
-        for (int sa = 1; sa < 10; ++sa) {
-          const C wv = __ldg(&tw[9 * qq * sa]);
-          xo[89 * sa * T] = cmul(v[sa], make_float2(wv.x, -wv.y));
-        }
-      }
-      __syncthreads();
-      // B: radix-9 over qq, twiddle exp(+2 pi i m2 s1 / 810), s1 = s_a + 10 s_b
-      if (w < 90) {
-        const int sa = w / 9, m2 = w - 9 * sa;
-        C v[9];
-        const C* xi = xs + (89 * sa + m2) * T + col;
-#pragma unroll
-        for (int qq = 0; qq < 9; ++qq) v[qq] = xi[9 * qq * T];
-        DFT<9, true, C>::run(v);
-        C* yo = ys + w * T + col;
-#pragma unroll
-        for (int sb = 0; sb < 9; ++sb) {
-          const C wv = __ldg(&tw[m2 * (sa + 10 * sb)]);
-          yo[90 * sb * T] = cmul(v[sb], make_float2(wv.x, -wv.y));
-        }
-      }
-      __syncthreads();
-      // C: radix-9 over m2 -> x = s1 + 90 s2, straight to global memory
-      if (w < 90 && live) {
-        const int s1 = w;
-        C v[9];
-        const C* yi = ys + 9 * s1 * T + col;
-#pragma unroll
-        for (int m2 = 0; m2 < 9; ++m2) v[m2] = yi[m2 * T];
-        DFT<9, true, C>::run(v);
-        C* dst = s_dst[q] + (long long)c * a.out_cs + kx + s1 * oes;
-#pragma unroll
-        for (int s2 = 0; s2 < 9; ++s2) dst[90 * s2 * oes] = v[s2];
-      }
-    } else {
-      // A: radix-9 over m1 of x = 90 m1 + m2, twiddle exp(-2 pi i m2 s1' / 810)
-      if (w < 90) {
-        const int m2 = w;
-        C v[9];
-#pragma unroll
-        for (int m1 = 0; m1 < 9; ++m1) v[m1] = sg[(90 * m1 + m2) * T];
-        DFT<9, false, C>::run(v);
-        C* xo = xs + m2 * T + col;
-        xo[0] = v[0];
-#pragma unroll
-        for (int s = 1; s < 9; ++s) xo[90 * s * T] = cmul(v[s], __ldg(&tw[m2 * s]));
-      }
-      __syncthreads();
-      // B: radix-9 over p (m2 = 10 p + qq), twiddle exp(-2 pi i qq s_a / 90)
-      if (w < 90) {
-        const int s1 = w / 10, qq = w - 10 * s1;
-        C v[9];
-        const C* xi = xs + (90 * s1 + qq) * T + col;
-#pragma unroll
-        for (int p = 0; p < 9; ++p) v[p] = xi[10 * p * T];
-        DFT<9, false, C>::run(v);
-        C* yo = ys + (90 * s1 + 9 * qq) * T + col;
-        yo[0] = v[0];
-#pragma unroll
-        for (int sa = 1; sa < 9; ++sa) yo[sa * T] = cmul(v[sa], __ldg(&tw[9 * qq * sa]));
-      }
-      __syncthreads();
-      // C: radix-10 over qq -> k = s1' + 9 s_a + 81 s_b, retained modes only
-      if (w < 81 && live) {
-        const int s1 = w / 9, sa = w - 9 * s1;
-        C v[10];
-        const C* yi = ys + (90 * s1 + sa) * T + col;
-#pragma unroll
-        for (int qq = 0; qq < 10; ++qq) v[qq] = yi[9 * qq * T];
-        DFT<10, false, C>::run(v);
-        C* dst = s_dst[q] + (long long)c * a.out_cs + kx;
-#pragma unroll
-        for (int sb = 0; sb < 10; ++sb) {
-          if (TRUNC && (sb == 4 || sb == 5)) continue;
-          const int pc = compact(s1 + 9 * sa + 81 * sb);
-          if (pc >= 0) dst[pc * oes] = v[sb];
-        }
-      }
-    }
-    // No barrier here: the next tile's stage copies go to the buffer whose
-    // readers (pass A of the previous tile) finished before the A->B barrier
-    // of this tile; its pass A writes xs after its top barrier, which every
-    // thread reaches only after this tile's pass C; its pass B writes ys after
-    // two more barriers.
-  }
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
-// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
@@ -1169,20 +841,8 @@ template <typename F> static void set_smem2(F* f, size_t bytes) {
 
 template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
 
-static void init_col4() {
-  const int mx = int(Col4Cfg::smem(810));
-  cudaFuncSetAttribute(k_col4<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-  cudaFuncSetAttribute(k_col4<false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-}
-
 template <int N> static void init_fast_n() {
   constexpr int T = col_tile<N>();
-  set_smem2(k_col3<N, T, true>, Col3Cfg<N, T>::SMEM);
-  set_smem2(k_col3<N, T, false>, Col3Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, true, true, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, true, true, true>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, true, false, false>, Col2Cfg<N, T>::SMEM);
@@ -1198,7 +858,7 @@ bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64;
 
 bool init_fast(int N) {
   switch (N) {
-    case 810: init_fast_n<810>(); init_col4(); break;
+    case 810: init_fast_n<810>(); break;
     case 256: init_fast_n<256>(); break;
     case 128: init_fast_n<128>(); break;
     case 64: init_fast_n<64>(); break;
@@ -1208,66 +868,12 @@ bool init_fast(int N) {
 }
 
 // Every column sweep runs one two-level tile per CTA (k_col2), which keeps
-// shared-memory traffic at one exchange per element and, at three CTAs per SM,
-// beats the persistent kernels in both directions (810^3 inverse y sweep, 81
-// planes: 0.166 ms k_col2 against 0.283 ms k_col4).  SC_COL_KERNEL=4 selects
-// the persistent three-level kernel (k_col4) for the 810 inverse sweeps,
-// SC_COL_KERNEL=3 the persistent two-level kernel (k_col3).
-static int col_variant() {
-  static const int v = [] {
-    const char* e = getenv("SC_COL_KERNEL");
-    return (e && (e[0] == '3' || e[0] == '4')) ? e[0] - '0' : 2;
-  }();
-  return v;
-}
-
-static int num_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    if (n <= 0) n = 148;
-  }
-  return n;
-}
-
-template <bool INV> static void col4_launch(const ColArgs& a, const void* tw, cudaStream_t st) {
-  constexpr int T = Col4Cfg::T;
-  const int ntx = (a.K1 + T - 1) / T;
-  const bool drv = INV && a.ndrv > 0;
-  const int ntiles = ntx * a.ncols * (a.ncomp + (drv ? a.ndrv : 0));  // <= 51 * 810 * kMaxComp
-  const int nin = INV ? a.kpos + a.kneg : 810;
-  const bool trunc = a.kpos <= 324 && a.kneg <= 324;
-  const int grid = num_sms() < ntiles ? num_sms() : ntiles;
-  const size_t sm = Col4Cfg::smem(nin);
-  const float2* t2 = static_cast<const float2*>(tw);
-  if constexpr (INV) {
-    if (drv) {
-      if (trunc) k_col4<true, true, true><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
-      else k_col4<true, false, true><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
-      return;
-    }
-  }
-  if (trunc) k_col4<INV, true, false><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
-  else k_col4<INV, false, false><<<grid, Col4Cfg::NT, sm, st>>>(a, t2, ntx, ntiles, nin);
-}
-
+// shared-memory traffic at one exchange per element; at three CTAs per SM it
+// beat persistent cp.async-staged variants (one or two CTAs per SM, double-
+// buffered tiles) in both directions (810^3 inverse y sweep, 81 planes:
+// 0.166 ms against 0.283 ms for a persistent three-level kernel).
 template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
   constexpr int T = col_tile<N>();
-  if (N == 810 && INV && col_variant() == 4 && a.kpos + a.kneg <= 810) {
-    col4_launch<INV>(a, tw, st);
-    return;
-  }
-  if (col_variant() == 3 && INV) {
-    using Cfg = Col3Cfg<N, T>;
-    const int ntx = (a.K1 + T - 1) / T;
-    const long long ntiles = (long long)ntx * a.ncols * (a.ncomp + (INV ? a.ndrv : 0));
-    long long grid = (long long)num_sms() * 2;
-    if (grid > ntiles) grid = ntiles;
-    k_col3<N, T, INV><<<unsigned(grid), Cfg::NT, Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw), ntx, ntiles);
-    return;
-  }
   using Cfg = Col2Cfg<N, T>;
   dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
   const float2* t2 = static_cast<const float2*>(tw);
