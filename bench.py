@@ -31,6 +31,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -324,7 +325,7 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
 
 
 def filter_measure(dev, g, st_state, reps=3):
-    """configs[2]'s filter call: sfs! of the 810^3 FP32 state to 128^3 at
+    """The DNS -> LES filter workload: sfs! of the 810^3 FP32 state to 128^3 at
     Delta/h in {2, 4, 8} (ubar 3 + tau 6 per Delta, FP32), device-timed."""
     import torch
     import symcode as S
@@ -352,7 +353,7 @@ def filter_measure(dev, g, st_state, reps=3):
 
 
 def fp32_vs_fp64_measure(dev, n=256, nsteps=100, every=10):
-    """configs[1]: 256^3 forced DNS (nu=2e-3, dt=2e-3, eps=0.1, k_p=4, seed 1) run
+    """256^3 forced DNS (nu=2e-3, dt=2e-3, eps=0.1, k_p=4, seed 1) run
     in FP32 and FP64 side by side; relative L2 error of the FP32 state every
     `every` steps."""
     import torch
@@ -512,8 +513,8 @@ def run_gpu(args):
     barrier(ws)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clk_path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                            f"clocks_rank{rank}.csv")
+    # the sampled clock log goes to $SC_CLOCKS_DIR (default: the system temp dir)
+    clk_path = os.path.join(os.environ.get("SC_CLOCKS_DIR", tempfile.gettempdir()), f"clocks_rank{rank}.csv")
     with ClockSampler(clk_path) as clk:
         ev0.record(stream)
         for _ in range(args.steps):

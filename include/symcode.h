@@ -170,7 +170,7 @@ typedef struct sc_closure sc_closure;
 SC_API int sc_closure_create(sc_closure** closure, sc_plan* plan, int kind, double delta, const double* params,
                              int nparams);
 SC_API int sc_closure_destroy(sc_closure* closure);
-/* CNN closure (new; no reference counterpart; SURVEY configs[3]): input u (3
+/* CNN closure (new; no reference counterpart; the batched 128^3 LES closure): input u (3
  * physical channels) plus the standardised log Re_Delta, (log(Delta^2
  * sqrt(<|grad u|^2>)/visc) - mu)/sigma, as a 4th constant channel (the
  * convention of fullchain, src/nets.jl:311-331); four 3x3x3 periodic
