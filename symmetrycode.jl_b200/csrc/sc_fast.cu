@@ -544,7 +544,9 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
 // Pencils: A = u1 + i u2 (row r), A' = u1 + i u2 (row r'), B = u3(r) + i u3(r');
 // forward pencils per row: (u1 u1, u2 u2), (u3 u3, u1 u2), (u2 u3, u3 u1).
 // Shared memory: two regions of three pencil slots; the layouts below keep
-// every exchange free of bank conflicts except the F2 stores (two-way).
+// every exchange free of bank conflicts except the F3 loads, which meet two
+// addresses on one or two bank pairs per half-warp (no linear placement of the
+// F2 -> F3 exchange does better without making the F2 stores conflict).
 // ---------------------------------------------------------------------------
 struct X4Cfg {
   static constexpr int N = 810, NT = 96;
