@@ -173,18 +173,17 @@ def job_throughput(ms_local, ws, steps):
 
 
 def initial_compact(n, seed):
-    """Seeded compact FP64 initial field (same generator and bytes as the parity tests)."""
-    import oracle as O
-    return O.random_field_compact(3, n, seed, kpeak=KPEAK, totalenergy=1.0)
+    """Seeded compact FP64 initial field (symcode.fields, the reference's randomfield)."""
+    from symcode import fields
+    return fields.random_field_compact(3, n, seed, kpeak=KPEAK, totalenergy=1.0)
 
 
 def to_full(uc, n, dtype):
     import numpy as np
     import torch
-    import oracle as O
-    g = O.Grid(3, n)
+    from symcode import fields
     cd = np.complex64 if dtype == torch.float32 else np.complex128
-    return [torch.from_numpy(O.unpack_retained(c.astype(cd), g)) for c in uc]
+    return [torch.from_numpy(fields.compact_to_full(c.astype(cd), n)) for c in uc]
 
 
 def cpu_sample_steps(n, nsteps=1):
