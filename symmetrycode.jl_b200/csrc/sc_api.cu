@@ -705,11 +705,16 @@ int rk4_step(sc_plan* p, double dt, double visc, const sc_forcing* frc, cudaStre
     e.forcing = forced ? p->dscal : nullptr;
     static const double wa[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
     static const double cbv[3] = {0.5, 0.5, 1.0};
+    // The accumulator ACC = U + dt sum_j wa[j] k_j is first written at stage 1,
+    // from the stage input S = U + cbv[0] dt k1 that stage reads anyway:
+    // ACC = U + (wa[0] / cbv[0]) (S - U) + wa[1] dt k2.  Stage 0 writes only S.
     for (int c = 0; c < p->D; ++c) {
-      e.base_a[c] = s == 0 ? p->U[c] : p->ACC[c];
-      e.out_a[c] = s == 3 ? p->U[c] : p->ACC[c];
+      e.base_a[c] = s <= 1 ? nullptr : p->ACC[c];
+      e.out_a[c] = s == 0 ? nullptr : (s == 3 ? p->U[c] : p->ACC[c]);
       if (s < 3) { e.base_b[c] = p->U[c]; e.out_b[c] = p->S[c]; }
     }
+    e.mix_a = s == 1;
+    e.mix = wa[0] / cbv[0];
     e.ca = wa[s] * dt;
     e.has_b = s < 3;
     e.cb = s < 3 ? cbv[s] * dt : 0.0;

@@ -73,6 +73,11 @@ struct EpiArgs {
   const double* forcing;  // device scalar A (nullptr: no forcing)
   const void* sig2[6];    // optional second stress spectrum added to sig (closure stress)
   int has_sig2;
+  // mix_a: the base of out_a is base_b + mix (us - base_b) instead of base_a
+  // (RK4 stage 2 rebuilds the accumulator from the stage input it reads
+  // anyway); out_a[c] == nullptr: out_a is not written
+  int mix_a;
+  double mix;
 };
 
 struct PackArgs {

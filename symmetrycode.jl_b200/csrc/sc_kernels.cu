@@ -414,17 +414,17 @@ __global__ void __launch_bounds__(256) k_epilogue(const EpiArgs a) {
       for (int c = 0; c < D; ++c) du[c] = mk<C>(du[c].x + A * u[c].x, du[c].y + A * u[c].y);
     }
   }
-  const R ca = R(a.ca), cb = R(a.cb);
+  const R ca = R(a.ca), cb = R(a.cb), mix = R(a.mix);
   C va[3], vb[3];
 #pragma unroll
   for (int c = 0; c < D; ++c) {
+    C bb = mk<C>(R(0), R(0));
+    if (a.has_b || a.mix_a) bb = static_cast<const C*>(a.base_b[c])[i];
     C b = mk<C>(R(0), R(0));
-    if (a.base_a[c] != nullptr) b = static_cast<const C*>(a.base_a[c])[i];
+    if (a.mix_a) b = mk<C>(bb.x + mix * (u[c].x - bb.x), bb.y + mix * (u[c].y - bb.y));
+    else if (a.base_a[c] != nullptr) b = static_cast<const C*>(a.base_a[c])[i];
     va[c] = mk<C>(b.x + ca * du[c].x, b.y + ca * du[c].y);
-    if (a.has_b) {
-      const C bb = static_cast<const C*>(a.base_b[c])[i];
-      vb[c] = mk<C>(bb.x + cb * du[c].x, bb.y + cb * du[c].y);
-    }
+    if (a.has_b) vb[c] = mk<C>(bb.x + cb * du[c].x, bb.y + cb * du[c].y);
   }
   if (a.proj_a && !origin) {
     C kd = mk<C>(R(0), R(0));
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(256) k_epilogue(const EpiArgs a) {
   }
 #pragma unroll
   for (int c = 0; c < D; ++c) {
-    static_cast<C*>(a.out_a[c])[i] = va[c];
+    if (a.out_a[c] != nullptr) static_cast<C*>(a.out_a[c])[i] = va[c];
     if (a.has_b) static_cast<C*>(a.out_b[c])[i] = vb[c];
   }
 }
