@@ -18,6 +18,7 @@ import math
 
 import torch
 
+from . import fields
 from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
                    ptr_array, sc_forcing, sc_les_instance)
 
@@ -29,7 +30,7 @@ __all__ = [
     "turbulence_statistics", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
     "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights",
     "create_cnn_fp_closure", "closure_num_params", "closure_set_params", "pack_cnn_params", "rollout_record",
-    "rollout_loss", "rollout_adjoint", "les_", "les_wray3_", "les_rk4_",
+    "rollout_loss", "rollout_adjoint", "les_", "les_wray3_", "les_rk4_", "fields",
 ]
 
 
