@@ -174,7 +174,8 @@ SC_API int sc_closure_destroy(sc_closure* closure);
  * physical channels) plus the standardised log Re_Delta, (log(Delta^2
  * sqrt(<|grad u|^2>)/visc) - mu)/sigma, as a 4th constant channel (the
  * convention of fullchain, src/nets.jl:311-331); four 3x3x3 periodic
- * convolutions 4->32->32->32->6 with exact GELU between them; output tau in
+ * convolutions 4->32->32->32->6 with GELU between them (NNlib's tanh form,
+ * src/nets.jl:187; hardware tanh.approx.f32 in this BF16 path); output tau in
  * pair order.  BF16 weights and activations, FP32 accumulation on tcgen05
  * tensor cores.  weights[l]: host FP32 (C_out, C_in, 3, 3, 3) (rounded to BF16
  * here), biases[l]: host FP32 (C_out).  FP32 3D plans with n = 128. */
@@ -365,7 +366,9 @@ SC_API int sc_dissipation(sc_plan* plan, const void* const* u_hat, double visc, 
  * memory is taken by the solver: sc_spectrum there would set up a plan's work
  * buffers and take a stream-ordered shell buffer per call.  The first call on
  * each device looks up the array's address with that device current; make it
- * before any stream capture begins.  Calls on one device share the array, so
+ * before any stream capture begins.  The address is kept per device and CUDA
+ * context, so the first call after a context reset (cudaDeviceReset) looks it
+ * up again and also belongs before any capture.  Calls on one device share the array, so
  * calls that overlap in time (other streams or host threads) race.
  * Synchronous on stream. */
 #define SC_SPECTRUM_STATIC_MAX_SHELLS 512

@@ -20,6 +20,13 @@ physical/mathematical properties (Galerkin energy conservation of the
 dealiased nonlinear term, Taylor-Green analytic RHS, RK order of convergence,
 Hermitian symmetry, divergence-free output).
 
+Two further modules serve the production size 810^3: ``oracle.triad`` (exact
+triad sums of sparse fields, no FFT) and ``oracle.compact`` (the same FFT
+oracle on the compact 2/3 cube, lean enough to run 810^3 in host memory).
+Both are checked against the restatement above by CPU tests
+(``tests/test_oracle_sparse_compact.py``); they are imported explicitly, not
+re-exported here.
+
 Array convention: the reference stores spectral fields column-major with shape
 ``(n/2+1, n, n)`` (x fastest, x is the halved RFFT axis).  Here numpy C-order
 arrays of shape ``(n, n, n/2+1)`` indexed ``[iz, iy, ix]`` have the identical

@@ -2058,6 +2058,15 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
     return SC_OK;
   };
   auto freeall = [&]() { for (void* a : B.all) cudaFreeAsync(a, st); };
+  // a CUDA error in the body frees the rollout buffers before it returns
+#define SC_CU_FREE(call)                                                                     \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      freeall();                                                                             \
+      return fail(SC_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));                     \
+    }                                                                                        \
+  } while (0)
   int rc = SC_OK;
   const bool adj = grad != nullptr;
   const int nck = adj ? nsteps / ck + 1 : 0;
@@ -2102,12 +2111,12 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
   void* x[3];
   state_ptrs(B.seg, 0, x);
   if ((rc = pack_state<R>(p, u0, x, st))) { freeall(); return rc; }
-  SC_CU(cudaMemsetAsync(B.dloss, 0, sizeof(double), st));
-  if (adj) SC_CU(cudaMemcpyAsync(B.ck, x[0], sbytes, cudaMemcpyDeviceToDevice, st));
+  SC_CU_FREE(cudaMemsetAsync(B.dloss, 0, sizeof(double), st));
+  if (adj) SC_CU_FREE(cudaMemcpyAsync(B.ck, x[0], sbytes, cudaMemcpyDeviceToDevice, st));
   for (int s_ = 1; s_ <= nsteps && !rc; ++s_) {
     rc = step(x);
     if (rc) break;
-    if (rec) SC_CU(cudaMemcpyAsync(static_cast<char*>(rec) + (size_t)(s_ - 1) * sbytes, x[0], sbytes,
+    if (rec) SC_CU_FREE(cudaMemcpyAsync(static_cast<char*>(rec) + (size_t)(s_ - 1) * sbytes, x[0], sbytes,
                                    cudaMemcpyDeviceToDevice, st));
     if (traj) {
       const void* t3[3];
@@ -2115,21 +2124,21 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
       sc::launch_mse<R>((const void* const*)x, t3, nullptr, 0.0, D, p->kc, B.dloss, st);
     }
     if (adj && s_ % ck == 0)
-      SC_CU(cudaMemcpyAsync(static_cast<char*>(B.ck) + (size_t)(s_ / ck) * sbytes, x[0], sbytes,
+      SC_CU_FREE(cudaMemcpyAsync(static_cast<char*>(B.ck) + (size_t)(s_ / ck) * sbytes, x[0], sbytes,
                             cudaMemcpyDeviceToDevice, st));
   }
   if (!rc && adj) {
-    SC_CU(cudaMemsetAsync(cl ? (void*)cl->gw : nullptr, 0, cl ? cl->nparam * sizeof(double) : 0, st));
+    SC_CU_FREE(cudaMemsetAsync(cl ? (void*)cl->gw : nullptr, 0, cl ? cl->nparam * sizeof(double) : 0, st));
     sc::launch_axpby<R>(B.lam, nullptr, 0.0, 0.0, D, (long long)p->csz, st);  // lam = 0
     const double coef = 2.0 / nsteps;
     for (int seg = (nsteps - 1) / ck; seg >= 0 && !rc; --seg) {
       const int c0 = seg * ck, c1 = std::min(nsteps, c0 + ck);
       // recompute u_{c0} .. u_{c1} into the segment buffer
-      SC_CU(cudaMemcpyAsync(B.seg, static_cast<char*>(B.ck) + (size_t)seg * sbytes, sbytes, cudaMemcpyDeviceToDevice, st));
+      SC_CU_FREE(cudaMemcpyAsync(B.seg, static_cast<char*>(B.ck) + (size_t)seg * sbytes, sbytes, cudaMemcpyDeviceToDevice, st));
       for (int s_ = c0 + 1; s_ <= c1 && !rc; ++s_) {
         void* xs[3];
         state_ptrs(B.seg, s_ - c0, xs);
-        SC_CU(cudaMemcpyAsync(xs[0], static_cast<char*>(B.seg) + (size_t)(s_ - c0 - 1) * sbytes, sbytes,
+        SC_CU_FREE(cudaMemcpyAsync(xs[0], static_cast<char*>(B.seg) + (size_t)(s_ - c0 - 1) * sbytes, sbytes,
                               cudaMemcpyDeviceToDevice, st));
         rc = step(xs);
       }
@@ -2144,27 +2153,29 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
         // step adjoint at u_{s-1}: recompute the stage inputs, then transpose stages 4..1
         void* un[3];
         state_ptrs(B.seg, s_ - c0 - 1, un);
-        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[0][c], un[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        for (int c = 0; c < D; ++c) SC_CU_FREE(cudaMemcpyAsync(B.u[0][c], un[c], cbytes, cudaMemcpyDeviceToDevice, st));
         static const double cst[3] = {0.5, 0.5, 1.0};
         for (int q = 0; q < 3 && !rc; ++q) {
           rc = stage_F<R>(p, cl, B.u[q], B.k, visc, st);
-          for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.u[q + 1][c], B.u[0][c], cbytes, cudaMemcpyDeviceToDevice, st));
+          if (rc) break;
+          for (int c = 0; c < D; ++c) SC_CU_FREE(cudaMemcpyAsync(B.u[q + 1][c], B.u[0][c], cbytes, cudaMemcpyDeviceToDevice, st));
           sc::launch_axpby<R>(B.u[q + 1], (const void* const*)B.k, cst[q] * dt, 1.0, D, (long long)p->csz, st);
         }
+        if (rc) break;
         // lam_n accumulates in B.lam (identity part already there)
         static const double wq[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
         // lk = w4 dt lam
-        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.lk[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        for (int c = 0; c < D; ++c) SC_CU_FREE(cudaMemcpyAsync(B.lk[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
         sc::launch_axpby<R>(B.lk, nullptr, 0.0, wq[3] * dt, D, (long long)p->csz, st);
         // keep a copy of lam (dL/du_{n+1}) in B.k for the stage combinations
-        for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.k[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
+        for (int c = 0; c < D; ++c) SC_CU_FREE(cudaMemcpyAsync(B.k[c], B.lam[c], cbytes, cudaMemcpyDeviceToDevice, st));
         for (int q = 3; q >= 0 && !rc; --q) {
           rc = stage_adjoint<R>(p, cl, B.u[q], B.lk, B.mu, visc, st);
           if (rc) break;
           sc::launch_axpby<R>(B.lam, (const void* const*)B.mu, 1.0, 1.0, D, (long long)p->csz, st);  // lam_n += mu
           if (q > 0) {
             // lk_{q-1} = w_{q-1} dt lam_{n+1} + c_{q-1} dt mu
-            for (int c = 0; c < D; ++c) SC_CU(cudaMemcpyAsync(B.lk[c], B.k[c], cbytes, cudaMemcpyDeviceToDevice, st));
+            for (int c = 0; c < D; ++c) SC_CU_FREE(cudaMemcpyAsync(B.lk[c], B.k[c], cbytes, cudaMemcpyDeviceToDevice, st));
             sc::launch_axpby<R>(B.lk, (const void* const*)B.mu, cst[q - 1] * dt, wq[q - 1] * dt, D,
                                 (long long)p->csz, st);
           }
@@ -2174,14 +2185,15 @@ int rollout_impl(sc_plan* p, sc_closure* cl, const void* const* u0, const void* 
   }
   double h = 0;
   if (!rc) {
-    SC_CU(cudaMemcpyAsync(&h, B.dloss, sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (adj && cl && cl->gw) SC_CU(cudaMemcpyAsync(grad, cl->gw, cl->nparam * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SC_CU_FREE(cudaMemcpyAsync(&h, B.dloss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (adj && cl && cl->gw) SC_CU_FREE(cudaMemcpyAsync(grad, cl->gw, cl->nparam * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   freeall();
   SC_CU(cudaStreamSynchronize(st));
   if (loss) *loss = traj ? h / nsteps : 0.0;
   return rc;
 }
+#undef SC_CU_FREE
 }  // namespace
 
 extern "C" {

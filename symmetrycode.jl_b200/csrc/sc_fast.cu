@@ -17,8 +17,6 @@
 #include "sc_fft.cuh"
 #include "sc_internal.h"
 
-#include <cstdlib>
-
 namespace sc {
 
 template <int N> struct Split;
@@ -852,7 +850,6 @@ template <int N> static void init_fast_n() {
   set_smem2(k_col2<N, T, false, false, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, false, false, true>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
-  set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
   set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
 }
 
@@ -901,29 +898,18 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
   }
 }
 
-// SC_X_KERNEL=2 / =3 select the older x sweeps (for comparison); the default
-// is the three-level kernel where it exists (N = 810), else k_xsweep3.
-static int x_variant() {
-  static const int v = [] {
-    const char* e = getenv("SC_X_KERNEL");
-    return e && (e[0] == '2' || e[0] == '3') ? e[0] - '0' : 4;
-  }();
-  return v;
-}
-
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
-  if (N == 810 && a.D == 3 && x_variant() == 4) {
+  if (N == 810 && a.D == 3) {
     const unsigned nb4 = unsigned((a.nrows + 1) / 2);
     if (a.K1in == 271 && a.K1out == 271)
       k_xsweep4<true><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
     else
       k_xsweep4<false><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
-  } else if (a.D == 3 && x_variant() != 2) {
+  } else if (a.D == 3) {
     const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
     k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, static_cast<const float2*>(tw));
-  } else if (a.D == 3) k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, static_cast<const float2*>(tw));
-  else k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  } else k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, static_cast<const float2*>(tw));
 }
 
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st) {

@@ -130,8 +130,6 @@ bool fast_supported(int N);
 bool init_fast(int N);
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st);
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st);
-// false when SC_ENGINE=stockham is set in the environment (forces the generic engine)
-bool fast_enabled();
 template <typename R> bool init_kernels(int N);
 template <typename R> void launch_twothirds_full(const PackArgs& a, cudaStream_t st);  // in place on a.dst
 template <typename R> void launch_project_full(const PackArgs& a, double kfac, cudaStream_t st);

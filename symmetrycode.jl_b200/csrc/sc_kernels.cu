@@ -824,16 +824,8 @@ template <typename R> bool init_kernels(int N) {
   }
 }
 
-bool fast_enabled() {
-  static const bool on = [] {
-    const char* e = getenv("SC_ENGINE");
-    return !(e && strcmp(e, "stockham") == 0);
-  }();
-  return on;
-}
-
 template <typename R> static bool use_fast(int N) {
-  return sizeof(R) == 4 && fast_enabled() && fast_supported(N);
+  return sizeof(R) == 4 && fast_supported(N);
 }
 
 template <typename R> bool launch_col_inv(int N, const ColArgs& a, const void* tw, cudaStream_t st) {

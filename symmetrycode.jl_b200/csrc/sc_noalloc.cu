@@ -14,9 +14,14 @@
 // The shell accumulators live in g_shell_scratch.  The first call on each
 // device looks up its device address with that device current
 // (cudaGetSymbolAddress); that lookup may load the module, so make the first
-// call on each device before any stream capture begins.  Every call on a device
-// shares the one array: two calls that overlap in time, on other streams or
-// from other host threads, race on it and both return wrong sums.
+// call on each device before any stream capture begins.  The address is cached
+// per device together with the id of the CUDA context it was looked up in; a
+// call in a new context (after cudaDeviceReset, or a primary-context reset by
+// another library in the process) repeats the lookup, so its first call comes
+// before any capture too.  Every call on a device shares the one array: two
+// calls that overlap in time, on other streams or from other host threads,
+// race on it and both return wrong sums.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,22 +40,62 @@ static __device__ __align__(256) double g_shell_scratch[SC_SPECTRUM_STATIC_MAX_S
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+struct ScratchSlot {
+  unsigned long long ctx_id;  // context the address belongs to (0: none yet)
+  double* ptr;
+};
+ScratchSlot g_scratch[kMaxDevices] = {};
 
-// Device address of g_shell_scratch on the current device (looked up once per device).
+// Unique id of the calling thread's current CUDA context (ids are never reused
+// within a process, unlike context handles).  The driver calls are reached
+// through the runtime's entry-point table, so the library needs no -lcuda.
+int current_context_id(unsigned long long* id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1{}, q2{};
+    cudaError_t e1 = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1);
+    cudaError_t e2 = cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || q1 != cudaDriverEntryPointSuccess ||
+        q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+      return sc::api_fail(SC_ERR_CUDA, "cudaGetDriverEntryPoint(cuCtxGetCurrent / cuCtxGetId)", "");
+    get_current = reinterpret_cast<GetCurrent>(f1);
+    get_id = reinterpret_cast<GetId>(f2);
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return sc::api_fail(SC_ERR_CUDA, "no current CUDA context", "");
+  if (get_id(ctx, id) != CUDA_SUCCESS) return sc::api_fail(SC_ERR_CUDA, "cuCtxGetId", "");
+  return SC_OK;
+}
+
+// Device address of g_shell_scratch in the current device's current context
+// (looked up once per device and context).
 int scratch_for_current_device(double** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return sc::api_fail(SC_ERR_CUDA, "cudaGetDevice", cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return sc::api_fail(SC_ERR_UNSUPPORTED, "device ordinal beyond 63", "");
+  // initialise the device's primary context and make it current (CUDA >= 12:
+  // cudaSetDevice does both; a no-op when it already is)
+  e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return sc::api_fail(SC_ERR_CUDA, "cudaSetDevice", cudaGetErrorString(e));
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
+  unsigned long long id = 0;
+  int rc = current_context_id(&id);
+  if (rc) return rc;
+  ScratchSlot& slot = g_scratch[dev];
+  if (!slot.ptr || slot.ctx_id != id) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_shell_scratch);
     if (e != cudaSuccess) return sc::api_fail(SC_ERR_CUDA, "cudaGetSymbolAddress(shell scratch)", cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<double*>(p);
+    slot.ptr = static_cast<double*>(p);
+    slot.ctx_id = id;
   }
-  *out = g_scratch_ptr[dev];
+  *out = slot.ptr;
   return SC_OK;
 }
 

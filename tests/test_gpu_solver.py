@@ -74,32 +74,6 @@ def test_fft_fp32_matches_pocketfft(D, n):
     assert rel_l2(to_np(sp), O.to_spec(x, go)) < 1e-6
 
 
-def test_rhs_810_fp32_matches_fp64_path():
-    """At the benchmark size the FP32 two-level engine agrees with the FP64 path
-    (itself pinned to the oracle at smaller sizes) within the FP32 tolerance."""
-    n = 810
-    g32 = S.Grid(3, n, dtype=torch.float32, device="cuda:0")
-    gen = torch.Generator(device="cuda:0").manual_seed(7)
-    u64 = []
-    for _ in range(3):
-        c = torch.randn(g32.spec_shape, dtype=torch.complex128, device="cuda:0", generator=gen)
-        u64.append(c * 1e-3)
-    u32 = [c.to(torch.complex64) for c in u64]
-    du32 = S.vectorfield(g32)
-    S.convectiondiffusion_(du32, u32, g32, 6e-4)
-    res32 = [c.to(torch.complex128) for c in du32]
-    del du32, u32
-    g32.close()
-    g64 = S.Grid(3, n, dtype=torch.float64, device="cuda:0")
-    u64r = [c.to(torch.complex64).to(torch.complex128) for c in u64]  # same input bytes
-    du64 = S.vectorfield(g64)
-    S.convectiondiffusion_(du64, u64r, g64, 6e-4)
-    num = sum(float((a - b).abs().pow(2).sum()) for a, b in zip(res32, du64))
-    den = sum(float(b.abs().pow(2).sum()) for b in du64)
-    g64.close()
-    assert (num / den) ** 0.5 < TOL32
-
-
 # ------------------------------------------------------------- point kernels
 def test_twothirds_and_project():
     g, go = _grid(2, 24, torch.float64)

@@ -24,7 +24,8 @@ def _spectrum_static(u, n, D, dtype, nshell):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("D,n,dtype", [(3, 48, torch.float64), (3, 64, torch.float32), (2, 96, torch.float64)])
+@pytest.mark.parametrize("D,n,dtype", [(3, 48, torch.float64), (3, 64, torch.float32), (2, 96, torch.float64),
+                                       (2, 120, torch.float32)])
 def test_static_spectrum_matches_sc_spectrum(D, n, dtype):
     g, go = S.Grid(D, n, dtype=dtype, device="cuda:0"), O.Grid(D, n)
     u = O.random_field(go, seed=60, kpeak=4)
@@ -36,6 +37,17 @@ def test_static_spectrum_matches_sc_spectrum(D, n, dtype):
     for _ in range(2):
         s = _spectrum_static(ut, n, D, code, nshell)
         assert np.allclose(s, ref, rtol=1e-12, atol=1e-300)
+    # the defining property: further calls take no device memory (neither the
+    # device's free memory nor torch's caching pool moves)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    res0 = torch.cuda.memory_reserved()
+    for _ in range(3):
+        s = _spectrum_static(ut, n, D, code, nshell)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0 and torch.cuda.memory_reserved() == res0
+    assert np.allclose(s, ref, rtol=1e-12, atol=1e-300)
     # fewer shells than the plan's n/3 reads the same leading shells
     s = _spectrum_static(ut, n, D, code, 5)
     assert np.allclose(s, ref[:5], rtol=1e-12, atol=1e-300)
