@@ -263,6 +263,16 @@ SC_API int sc_les_batch_destroy(sc_les_batch* batch);
 
 /* ---- plan options ---------------------------------------------------------------- */
 #define SC_OPT_USE_GRAPH 1 /* 1 (default): steppers replay a captured CUDA graph; 0: launch eagerly */
+/* Bound of the device-side waits of the plan's tensor-core CNN closures (polls
+ * of an mbarrier before a wait gives up, sets the closure's error flag --
+ * sc_closure_status then reports SC_ERR_TIMEOUT -- frees its tensor memory and
+ * returns).  A negative value restores the default (2^26 polls); 0 makes
+ * every such wait give up at once, which lets a test exercise the timeout path
+ * without hanging or faulting anything; the kernels' last wait for work still
+ * in flight before they free tensor memory always keeps the default bound.
+ * Takes effect at the next evaluation (not in step graphs captured before the
+ * change). */
+#define SC_OPT_WAIT_LIMIT 2
 SC_API int sc_plan_set_option(sc_plan* plan, int option, long long value);
 
 /* ---- a-posteriori training: rollout, loss and hand-written adjoint ----------

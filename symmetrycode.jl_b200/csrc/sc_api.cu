@@ -78,6 +78,7 @@ struct sc_plan {
   cudaGraphExec_t g_wray = nullptr;
   double k_wray[3] = {0, 0, 0};
   int use_graph = 1;  // SC_OPT_USE_GRAPH
+  long long wait_limit = sc::kDefaultWaitLimit;  // SC_OPT_WAIT_LIMIT
 };
 
 // A closure model `model(u, G) -> tau` (src/les.jl:19, src/closures.jl) bound
@@ -165,18 +166,28 @@ void plan_free(sc_plan* p) {
   if (p->cap) cudaStreamDestroy(p->cap);
 }
 
+// Host image of a twiddle buffer: exp(-2 pi i m / n) from long double, and for
+// FP32 n = 810 the x sweep's pair table after it (sc::twiddle_buffer_bytes).
 template <typename R>
-int upload_twiddles(sc_plan* p) {
+std::vector<unsigned char> twiddle_image(int n) {
   using C = typename sc::V2<R>::T;
-  std::vector<C> h(p->n);
-  for (int m = 0; m < p->n; ++m) {
-    // exp(-2 pi i m / n) from long double, reduced to the first half-turn for accuracy
+  std::vector<unsigned char> img(sc::twiddle_buffer_bytes(n, sizeof(C)));
+  C* h = reinterpret_cast<C*>(img.data());
+  for (int m = 0; m < n; ++m) {
     const long double pi = 3.141592653589793238462643383279502884L;
-    const long double th = 2.0L * pi * (long double)m / (long double)p->n;
+    const long double th = 2.0L * pi * (long double)m / (long double)n;
     h[m].x = (R)cosl(th);
     h[m].y = (R)(-sinl(th));
   }
-  SC_CU(cudaMemcpy(p->tw, h.data(), sizeof(C) * p->n, cudaMemcpyHostToDevice));
+  if (img.size() > sizeof(C) * (size_t)n)
+    sc::xpair810_twiddles(reinterpret_cast<const float2*>(h), reinterpret_cast<float*>(h + n));
+  return img;
+}
+
+template <typename R>
+int upload_twiddles(sc_plan* p) {
+  const std::vector<unsigned char> img = twiddle_image<R>(p->n);
+  SC_CU(cudaMemcpy(p->tw, img.data(), img.size(), cudaMemcpyHostToDevice));
   return SC_OK;
 }
 
@@ -496,6 +507,7 @@ int tc_forward(sc_closure* cl, void* const* u, cudaStream_t st) {
   a.delta = cl->delta; a.nu = cl->nu; a.mu = cl->mu; a.sigma = cl->sigma;
   a.err = cl->err;
   a.nsm = num_sms_api();
+  a.wait_limit = p->wait_limit;
   sc::launch_cnn_forward(a, st);
   return check_launch("cnn forward (tensor cores, adjoint)");
 }
@@ -519,6 +531,7 @@ int tc_backward(sc_closure* cl, cudaStream_t st) {
   for (int l = 0; l < 4; ++l) b.woff[l] = cc_layer_offset(l);
   b.err = cl->err;
   b.nsm = num_sms_api();
+  b.wait_limit = p->wait_limit;
   sc::launch_cnn_backward(b, st);
   SC_CU(cudaMemsetAsync(cl->dsum + 1, 0, sizeof(double), st));
   sc::launch_sum<float>(static_cast<const float*>(cl->ccg0) + 3 * np, np, cl->dsum + 1, st);
@@ -639,6 +652,7 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     a.nsm = nsm;
+    a.wait_limit = p->wait_limit;
     sc::launch_cnn_forward(a, st);
     if ((rc = check_launch("cnn closure"))) return rc;
   } else if (cl->kind == sc::kCnnFp) {
@@ -991,7 +1005,7 @@ int sc_plan_create(sc_plan** out, int D, int n, double l, int dtype, size_t* wor
   int rc = SC_OK;
   bool ok = (dtype == SC_FLOAT64) ? sc::init_kernels<double>(n) : sc::init_kernels<float>(n);
   if (!ok) { rc = fail(SC_ERR_CUDA, "kernel attribute setup failed for n=%d", n); goto bad; }
-  if ((rc = plan_alloc(p, &p->tw, (size_t)n * p->esz))) goto bad;
+  if ((rc = plan_alloc(p, &p->tw, sc::twiddle_buffer_bytes(n, p->esz)))) goto bad;
   for (int c = 0; c < D; ++c) {
     if ((rc = plan_alloc(p, &p->U[c], p->csz * p->esz))) goto bad;
     if ((rc = plan_alloc(p, &p->ACC[c], p->csz * p->esz))) goto bad;
@@ -1175,16 +1189,10 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
     return ptr;
   };
   auto cleanup = [&]() { for (void* b : bufs) cudaFree(b); };
-  void* tw = alloc(n);
+  const std::vector<unsigned char> timg = twiddle_image<R>(n);  // the solver's twiddles
+  void* tw = alloc((timg.size() + esz - 1) / esz);
   if (!tw) { cleanup(); return fail(SC_ERR_OOM, "microbench allocation failed"); }
-  {  // real twiddles so the arithmetic matches the solver's
-    std::vector<typename sc::V2<R>::T> h(n);
-    for (int m = 0; m < n; ++m) {
-      const long double th = 2.0L * 3.141592653589793238462643383279502884L * m / n;
-      h[m].x = (R)cosl(th); h[m].y = (R)(-sinl(th));
-    }
-    cudaMemcpy(tw, h.data(), n * esz, cudaMemcpyHostToDevice);
-  }
+  cudaMemcpy(tw, timg.data(), timg.size(), cudaMemcpyHostToDevice);
   if (!(esz == 8 ? sc::init_kernels<float>(n) : sc::init_kernels<double>(n))) { cleanup(); return fail(SC_ERR_SIZE, "n"); }
   sc::ColArgs ca{};
   sc::XArgs xa{};
@@ -2272,6 +2280,10 @@ int sc_rollout_adjoint_batch(int njobs, const sc_rollout_job* jobs, int* status,
 int sc_plan_set_option(sc_plan* p, int option, long long value) {
   if (!p) return fail(SC_ERR_INVALID, "null plan");
   if (option == SC_OPT_USE_GRAPH) { p->use_graph = value ? 1 : 0; return SC_OK; }
+  if (option == SC_OPT_WAIT_LIMIT) {
+    p->wait_limit = value < 0 ? sc::kDefaultWaitLimit : value;
+    return SC_OK;
+  }
   return fail(SC_ERR_INVALID, "unknown option %d", option);
 }
 

@@ -18,7 +18,10 @@
 // One elected thread issues the MMAs; tcgen05.commit signals an mbarrier; the
 // accumulator (128 lanes x C_out columns) is read back with tcgen05.ld for the
 // bias + GELU + BF16 epilogue.  Every mbarrier wait is bounded: on timeout the
-// kernel raises an error flag, frees its tensor memory and returns.
+// kernel raises an error flag, frees its tensor memory and returns.  The bound
+// of the row pipeline's waits is a launch argument (a plan option, so that a
+// test can make a wait run out); the last wait for MMAs still in flight before
+// the tensor memory is freed always keeps the full default bound.
 #include <cuda_bf16.h>
 #include <stdint.h>
 
@@ -27,8 +30,6 @@
 namespace sc {
 
 namespace {
-
-constexpr long long kSpinLimit = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -66,9 +67,11 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Polls the mbarrier phase `parity` at most `limit` times (try_wait suspends
+// for a hardware-defined time per poll); false when the wait ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
   const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kSpinLimit; ++it) {
+  for (long long it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -155,7 +158,7 @@ constexpr int kConvThreads = 384;
 template <int KN, int CP, int COP, int MODE>
 __global__ void __launch_bounds__(kConvThreads, 1)
 k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restrict__ wgt,
-        const float* __restrict__ bias, const ConvOut out, int* __restrict__ err) {
+        const float* __restrict__ bias, const ConvOut out, int* __restrict__ err, long long wait_limit) {
   constexpr int kRowPlane = row_plane<KN>();
   constexpr int CPC = CP / 8;              // 16-byte channel chunks
   constexpr int PLANE_ROW = CPC * kRowPlane;
@@ -236,7 +239,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
   // bounded wait of this thread for the MMAs of buffer b
   auto wait_buf = [&](int b) -> bool {
-    const bool r = mbar_wait(bar + b, (phase >> b) & 1u);
+    const bool r = mbar_wait(bar + b, (phase >> b) & 1u, wait_limit);
     asm volatile("tcgen05.fence::after_thread_sync;");
     return r;
   };
@@ -351,7 +354,7 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     // a wait ran out: give the MMAs still in flight one more bounded wait before
     // the tensor memory they write is released
     for (int bb = 0; bb < 2; ++bb)
-      if ((inflight >> bb) & 1u) mbar_wait(bar + bb, (phase >> bb) & 1u);
+      if ((inflight >> bb) & 1u) mbar_wait(bar + bb, (phase >> bb) & 1u, kDefaultWaitLimit);
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -525,8 +528,9 @@ template <int KN, int CP, int COP, int MODE> static void conv_attr() {
 
 template <int KN, int CP, int COP, int MODE>
 static void conv_launch(int grid, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* b, const ConvOut& o,
-                        int* err, cudaStream_t st) {
-  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(in, w, b, o, err);
+                        int* err, long long wait_limit, cudaStream_t st) {
+  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(in, w, b, o, err,
+                                                                                         wait_limit);
 }
 
 bool cnn_supported(int n, int D) { return (n == 64 || n == 128) && D == 3; }
@@ -566,15 +570,15 @@ template <int KN> static void cnn_forward_n(const CnnArgs& a, cudaStream_t st) {
   o3.act = a3; o3.pre = a.pre[2];
   o4.tau = a.tau;
   if (a.pre[0]) {
-    conv_launch<KN, 16, 32, kGeluSave>(grid, a.act0, a.w[0], a.b[0], o1, a.err, st);
-    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act1, a.w[1], a.b[1], o2, a.err, st);
-    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act2, a.w[2], a.b[2], o3, a.err, st);
+    conv_launch<KN, 16, 32, kGeluSave>(grid, a.act0, a.w[0], a.b[0], o1, a.err, a.wait_limit, st);
+    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act1, a.w[1], a.b[1], o2, a.err, a.wait_limit, st);
+    conv_launch<KN, 32, 32, kGeluSave>(grid, a.act2, a.w[2], a.b[2], o3, a.err, a.wait_limit, st);
   } else {
-    conv_launch<KN, 16, 32, kGelu>(grid, a.act0, a.w[0], a.b[0], o1, a.err, st);
-    conv_launch<KN, 32, 32, kGelu>(grid, a.act1, a.w[1], a.b[1], o2, a.err, st);
-    conv_launch<KN, 32, 32, kGelu>(grid, a.act2, a.w[2], a.b[2], o3, a.err, st);
+    conv_launch<KN, 16, 32, kGelu>(grid, a.act0, a.w[0], a.b[0], o1, a.err, a.wait_limit, st);
+    conv_launch<KN, 32, 32, kGelu>(grid, a.act1, a.w[1], a.b[1], o2, a.err, a.wait_limit, st);
+    conv_launch<KN, 32, 32, kGelu>(grid, a.act2, a.w[2], a.b[2], o3, a.err, a.wait_limit, st);
   }
-  conv_launch<KN, 32, 16, kTau>(grid, a3, a.w[3], a.b[3], o4, a.err, st);
+  conv_launch<KN, 32, 16, kTau>(grid, a3, a.w[3], a.b[3], o4, a.err, a.wait_limit, st);
 }
 
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st) {
@@ -599,17 +603,17 @@ template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t s
   wgrad_launch<KN, 32, 16>(a.gbf, a.act[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st);
   ConvOut o{};
   o.pre = a.gf;
-  conv_launch<KN, 16, 32, kLinear>(grid, a.gbf, a.wt[3], nullptr, o, a.err, st);
+  conv_launch<KN, 16, 32, kLinear>(grid, a.gbf, a.wt[3], nullptr, o, a.err, a.wait_limit, st);
   // layers 3, 2: g_pre = g_post * gelu'(h); input and weight gradients
   for (int l = 2; l >= 1; --l) {
     k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[l], a.gbf, npts * 32);
     wgrad_launch<KN, 32, 32>(a.gbf, a.act[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st);
-    conv_launch<KN, 32, 32, kLinear>(grid, a.gbf, a.wt[l], nullptr, o, a.err, st);
+    conv_launch<KN, 32, 32, kLinear>(grid, a.gbf, a.wt[l], nullptr, o, a.err, a.wait_limit, st);
   }
   // layer 1: input gradient into 16 channels (4 used), then planar
   k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[0], a.gbf, npts * 32);
   wgrad_launch<KN, 16, 32>(a.gbf, a.act[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st);
-  conv_launch<KN, 32, 16, kLinear>(grid, a.gbf, a.wt[0], nullptr, o, a.err, st);
+  conv_launch<KN, 32, 16, kLinear>(grid, a.gbf, a.wt[0], nullptr, o, a.err, a.wait_limit, st);
   k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);
 }
 

@@ -29,7 +29,11 @@ struct CnnArgs {
   double delta, nu, mu, sigma;
   int* err;                    // set to 1 when a bounded wait times out
   int nsm;
+  long long wait_limit;        // polls of each mbarrier wait before it gives up (kDefaultWaitLimit)
 };
+
+// Default bound of the CNN kernels' mbarrier waits (polls of try_wait).
+constexpr long long kDefaultWaitLimit = 1ll << 26;
 
 // Backward pass of the network after a forward pass that kept act0..act3 and
 // the pre-activations: from dL/dtau to dL/d(input channels) and the weight and
@@ -48,6 +52,7 @@ struct CnnBwdArgs {
   long long woff[4];
   int* err;
   int nsm;
+  long long wait_limit;
 };
 
 bool cnn_supported(int n, int D);

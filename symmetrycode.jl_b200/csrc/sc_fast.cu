@@ -857,7 +857,7 @@ bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64;
 
 bool init_fast(int N) {
   switch (N) {
-    case 810: init_fast_n<810>(); break;
+    case 810: init_fast_n<810>(); init_xpair810(); break;
     case 256: init_fast_n<256>(); break;
     case 128: init_fast_n<128>(); break;
     case 64: init_fast_n<64>(); break;
@@ -901,11 +901,7 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
   if (N == 810 && a.D == 3) {
-    const unsigned nb4 = unsigned((a.nrows + 1) / 2);
-    if (a.K1in == 271 && a.K1out == 271)
-      k_xsweep4<true><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
-    else
-      k_xsweep4<false><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, static_cast<const float2*>(tw));
+    launch_xpair810(a, static_cast<const float2*>(tw) + 810, st);
   } else if (a.D == 3) {
     const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
     k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, static_cast<const float2*>(tw));

@@ -130,6 +130,18 @@ bool fast_supported(int N);
 bool init_fast(int N);
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st);
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st);
+// FP32 n = 810 x sweep on paired rows (sc_xpair.cu).  Its twiddles are the
+// plain table's exp(-2 pi i j / 810) as register-pair entries
+// (c, c, s, s, -s, -s, 0, 0), stored in the same device buffer right after the
+// plain table (byte offset 810 * 8).
+size_t xpair810_twiddle_bytes();
+void xpair810_twiddles(const float2* tw, float* out8);
+bool init_xpair810();
+void launch_xpair810(const XArgs& a, const void* twp_table, cudaStream_t st);
+// bytes of a plan's twiddle buffer: the plain table plus, for FP32 n = 810, the pair table
+inline size_t twiddle_buffer_bytes(int n, size_t esz) {
+  return (size_t)n * esz + (esz == 8 && n == 810 ? xpair810_twiddle_bytes() : 0);
+}
 template <typename R> bool init_kernels(int N);
 template <typename R> void launch_twothirds_full(const PackArgs& a, cudaStream_t st);  // in place on a.dst
 template <typename R> void launch_project_full(const PackArgs& a, double kfac, cudaStream_t st);

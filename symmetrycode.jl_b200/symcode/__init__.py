@@ -559,7 +559,10 @@ class LesBatch:
 
 
 def set_option(g: Grid, option, value):
-    """``sc_plan_set_option`` (1 = use CUDA graphs for the steppers)."""
+    """``sc_plan_set_option``: ``SC_OPT_USE_GRAPH`` (1) replays captured CUDA
+    graphs in the steppers (default) or launches eagerly (0);
+    ``SC_OPT_WAIT_LIMIT`` (2) bounds the tensor-core CNN's device waits (polls;
+    negative: the default)."""
     check(lib().sc_plan_set_option(g.plan, int(option), int(value)))
 
 

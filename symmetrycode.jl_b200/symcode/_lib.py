@@ -16,6 +16,7 @@ HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "symcode.h")
 
 SC_OK, SC_ERR_INVALID, SC_ERR_SIZE, SC_ERR_CUDA, SC_ERR_OOM, SC_ERR_DIVERGED, SC_ERR_UNSUPPORTED, SC_ERR_TIMEOUT = range(8)
 SC_FLOAT32, SC_FLOAT64 = 0, 1
+SC_OPT_USE_GRAPH, SC_OPT_WAIT_LIMIT = 1, 2  # sc_plan_set_option
 
 
 class SymcodeError(RuntimeError):

@@ -103,3 +103,63 @@ def test_rollout_adjoint_batch_rejects_shared_plans():
     job = dict(grid=g, closure=cl, u0=u0, traj=traj, dt=2e-3, visc=1e-3, nsteps=2)
     with pytest.raises(S.SymcodeError):
         S.rollout_adjoint_batch([job, job])
+
+
+# ---------------------------------------------------------------- the a-posteriori training configuration
+# 64^3, 40 RK4 steps (dt = 5e-3), checkpoints every 5 steps, nu = 1e-3,
+# Delta/h = 4, the CNN closure, target rollout of the closure with weights
+# x (1 + 0.01 N(0, 1)).
+T_N, T_STEPS, T_CK, T_DT, T_NU = 64, 40, 5, 5e-3, 1e-3
+
+
+def _training_case(dtype, seed=101):
+    g, go = S.Grid(3, T_N, dtype=dtype, device="cuda:0"), O.Grid(3, T_N)
+    u0 = [to_dev(c, g) for c in O.random_field(go, seed=seed, kpeak=4)]
+    ws, bs = S.kaiming_cnn_weights(5)
+    theta = S.pack_cnn_params(ws, bs)
+    cl = S.create_cnn_fp_closure(4 * go.l / T_N, T_NU, g, ws, bs, mu=5.0, sigma=2.0)
+    rng = np.random.default_rng(seed + 1)
+    S.closure_set_params(cl, theta * (1 + 0.01 * rng.standard_normal(theta.size)))
+    traj = S.rollout_record(g, cl, u0, T_DT, T_NU, T_STEPS)
+    S.closure_set_params(cl, theta)
+    return g, cl, u0, traj, theta
+
+
+def test_training_adjoint_matches_finite_differences_at_64():
+    """FP64 gradient by the adjoint (checkpoints every 5 of 40 steps) against
+    central finite differences of the FP64 loss on 4 random weight directions."""
+    g, cl, u0, traj, theta = _training_case(torch.float64)
+    loss, grad = S.rollout_adjoint(g, cl, u0, traj, T_DT, T_NU, T_STEPS, ckpt_every=T_CK)
+    rng = np.random.default_rng(103)
+    h = 1e-4 * np.linalg.norm(theta) / math.sqrt(theta.size)
+    for k in range(4):
+        d = rng.standard_normal(theta.size)
+        d /= np.linalg.norm(d)
+        S.closure_set_params(cl, theta + h * d)
+        lp = S.rollout_loss(g, cl, u0, traj, T_DT, T_NU, T_STEPS)
+        S.closure_set_params(cl, theta - h * d)
+        lm = S.rollout_loss(g, cl, u0, traj, T_DT, T_NU, T_STEPS)
+        fd = (lp - lm) / (2 * h)
+        ad = float(grad @ d)
+        print(f"direction {k}: adjoint {ad:.10e}  central FD {fd:.10e}  rel {abs(fd - ad) / abs(ad):.2e}")
+        assert abs(fd - ad) <= 1e-5 * abs(ad), (k, fd, ad)
+    S.closure_set_params(cl, theta)
+    cl.close()
+    g.close()
+
+
+def test_training_adjoint_fp32_matches_fp64():
+    """The FP32 CUDA-core adjoint (the batched training path's precision) against
+    the FP64 adjoint on the same initial field, target and weights."""
+    res = {}
+    for dtype in (torch.float64, torch.float32):
+        g, cl, u0, traj, theta = _training_case(dtype)
+        res[dtype] = S.rollout_adjoint(g, cl, u0, traj, T_DT, T_NU, T_STEPS, ckpt_every=T_CK)
+        cl.close()
+        g.close()
+    (l64, g64), (l32, g32) = res[torch.float64], res[torch.float32]
+    e_loss = abs(l32 - l64) / l64
+    e_grad = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+    print(f"FP32 vs FP64: loss {e_loss:.2e}, gradient {e_grad:.2e}")
+    assert e_loss < 1e-4
+    assert e_grad < 1e-3
