@@ -186,48 +186,65 @@ def to_full(uc, n, dtype):
     return [torch.from_numpy(fields.compact_to_full(c.astype(cd), n)) for c in uc]
 
 
-def cpu_sample_steps(n, nsteps=1):
-    """Time `nsteps` forced RK4 steps of the FP64 oracle at n^3 on all host threads."""
-    import oracle as O
-    g = O.Grid(3, n)
-    u = O.random_field(g, seed=SEED, kpeak=KPEAK)
+def cpu_rk4_step(uc):
+    """Time one forced RK4 step of the FP64 oracle at full size (810^3) on all
+    host threads, from the compact field uc; returns (seconds, threads)."""
+    from oracle.compact import CompactOracle
+    o = CompactOracle(N_GRID)
     t0 = time.perf_counter()
-    for _ in range(nsteps):
-        u = O.rk4_step(u, DT, g, NU, EPS)
-    return (time.perf_counter() - t0) / nsteps
-
-
-def scale_to_810(sec_per_step, n):
-    """FFT-dominated cost ~ N log N with N = n^3: seconds per 810^3 step."""
-    f = (N_GRID ** 3 * math.log2(N_GRID ** 3)) / (n ** 3 * math.log2(n ** 3))
-    return sec_per_step * f
+    o.rk4_step(uc, DT, NU, EPS)
+    sec = time.perf_counter() - t0
+    o.release()
+    return sec, o.workers
 
 
 def run_reference(args):
-    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    """The reference path's CPU arm: the FP64 oracle (numpy + scipy.fft, the
+    restatement of the reference's solver; the reference itself is Julia and
+    cannot run here) on the 810^3 workload.  One timed "step" is one RK4 stage
+    of the full 810^3 field (its right-hand side and stage update, a quarter
+    of an RK4 step), so that K samples fit in a few minutes; steps/s =
+    1 / (4 x mean stage time)."""
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # largest sample grid whose W + K steps fit in about three minutes
-    t128 = cpu_sample_steps(128, 1)
-    sample_n = 128
-    for cand in (192, 256):
-        est = t128 * (cand / 128) ** 3 * math.log2(cand ** 3) / math.log2(128 ** 3)
-        if est * (args.steps + args.warmup) <= 180:
-            sample_n = cand
-    for _ in range(args.warmup):
-        cpu_sample_steps(sample_n, 1)
-    times = [cpu_sample_steps(sample_n, 1) for _ in range(args.steps)]
-    sps = 1.0 / scale_to_810(sum(times) / len(times), sample_n)
-    cores = os.cpu_count()
+    from oracle.compact import CompactOracle
+    uc = initial_compact(N_GRID, SEED)
+    o = CompactOracle(N_GRID)
+    stage = [c.copy() for c in uc]
+    acc = [c.copy() for c in uc]
+    coef = ((0.5, 1 / 6), (0.5, 1 / 3), (1.0, 1 / 3), (0.0, 1 / 6))
+
+    def one_stage(q):
+        kq = o.rk4_rhs(stage, NU, EPS)
+        cs, w = coef[q % 4]
+        o._axpy(acc, kq, w * DT)
+        if q % 4 == 3:  # the step is complete: u_{n+1} = acc starts the next one
+            for u_, c_, a_ in zip(uc, stage, acc):
+                u_[...] = a_
+                c_[...] = a_
+        else:
+            o._axpy(uc, kq, cs * DT, out=stage)
+
+    for q in range(min(args.warmup, 1)):
+        one_stage(q)
+    times = []
+    for q in range(args.steps):
+        t0 = time.perf_counter()
+        one_stage(q)
+        times.append(time.perf_counter() - t0)
+    sec_stage = sum(times) / len(times)
+    sps = 1.0 / (4 * sec_stage)
     line = {
         "impl": "reference", "metric": METRIC, "value": sps, "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / sps, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 4e3 * sec_stage, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": N_GRID},
-        "cpu_baseline": {"value": sps, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} forced RK4 step(s) of the FP64 numpy/scipy.fft (pocketfft, "
-                                   f"{cores} threads) restatement of the reference at {sample_n}^3, scaled to "
-                                   f"810^3 by N log N (Julia/FFTW reference unavailable: no Julia toolchain)"},
+        "cpu_baseline": {"value": sps, "unit": UNIT, "cores": o.workers, "kind": "port",
+                         "sample": f"{args.steps} RK4 stages (right-hand side + stage update, 4 per step) of the "
+                                   f"full 810^3 field by the FP64 numpy/scipy.fft restatement of the reference "
+                                   f"({o.workers} threads, {sec_stage:.1f} s per stage); the Julia/FFTW reference "
+                                   f"cannot run here (no Julia toolchain)"},
         "e2e": {"value": sps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -278,6 +295,14 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
             keep.append((g, cl))
         return insts, keep
 
+    def states(insts):
+        out = []
+        for d in insts:
+            u = S.vectorfield(d["grid"])
+            S.State(d["grid"]).store(u)
+            out.append([c.to(torch.complex128).cpu() for c in u])
+        return out
+
     stream = torch.cuda.current_stream()
     insts, keep = make(torch.float32)
     batch = S.LesBatch(insts)
@@ -290,10 +315,13 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
     torch.cuda.synchronize()
     ms_batch = e0.elapsed_time(e1) / steps
     status, _ = batch.status()
+    u32 = states(insts)
     batch.close()
     del insts, keep
     torch.cuda.empty_cache()
 
+    # the plain per-instance FP64 path: timed over plain_steps steps, then run on
+    # to the batch's step count for the FP32-vs-FP64 error of every instance
     insts64, keep64 = make(torch.float64)
     for d in insts64:
         S.set_option(d["grid"], 1, 0)  # eager launches
@@ -306,8 +334,16 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_plain = e0.elapsed_time(e1) / plain_steps
+    for d in insts64:
+        S.State(d["grid"]).les_rk4(d["closure"], LES_DT, d["visc"], warmup + steps - 1 - plain_steps)
+    u64 = states(insts64)
     del insts64, keep64
     torch.cuda.empty_cache()
+    errs = []
+    for a, b in zip(u32, u64):
+        num = sum(float((x - y).abs().pow(2).sum()) for x, y in zip(a, b))
+        den = sum(float(y.abs().pow(2).sum()) for y in b)
+        errs.append(math.sqrt(num / den))
     return {
         "metric": "batched LES steps/s (12 x 128^3, one RK4 step of every instance per step)",
         "value": 1e3 / ms_batch, "unit": "steps/s", "ms_per_step": ms_batch,
@@ -318,6 +354,10 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
                     "the same CNN on CUDA cores in FP64",
         "instances": [{"nu": nu, "delta_over_h": dh, "closure": "dynsmag" if k == 0 else "cnn"} for nu, dh, k in specs],
         "diverged": [i for i, s_ in enumerate(status) if s_ != 0],
+        "rel_l2_fp32_vs_fp64": errs,
+        "rel_l2_note": f"state of each instance after {warmup + steps} steps, batched FP32 against the plain FP64 "
+                       "path from the same initial field; the CNN instances differ mostly by the BF16 rounding of "
+                       "the tensor-core closure (the FP64 path runs the same weights unrounded)",
         "config": f"FP32, RK4 dt={LES_DT}, unforced, initial fields sfs! of a seeded 256^3 field (k_p=4, seed {LES_SEED}); "
                   "plain path: the same instances in FP64, one after another, eager launches",
     }
@@ -325,13 +365,16 @@ def les_batch_measure(dev, steps, warmup, plain_steps=2):
 
 def filter_measure(dev, g, st_state, reps=3):
     """The DNS -> LES filter workload: sfs! of the 810^3 FP32 state to 128^3 at
-    Delta/h in {2, 4, 8} (ubar 3 + tau 6 per Delta, FP32), device-timed."""
+    Delta/h in {2, 4, 8} (ubar 3 + tau 6 per Delta, FP32), device-timed; then
+    the same call on an FP64 plan from the same input bytes (the FP64 path is
+    pinned to the FP64 oracle at 810^3 by the tests) for the FP32 error."""
     import torch
     import symcode as S
-    gl = S.Grid(3, 128, dtype=torch.float32, device=dev)
+    nl = 128
+    gl = S.Grid(3, nl, dtype=torch.float32, device=dev)
     u = [S.scalarfield(g) for _ in range(3)]
     st_state.store(u)
-    deltas = [dh * gl.l / 128 for dh in (2, 4, 8)]
+    deltas = [dh * gl.l / nl for dh in (2, 4, 8)]
     ubar = [[S.scalarfield(gl) for _ in range(3)] for _ in deltas]
     tau = [[S.scalarfield(gl) for _ in range(6)] for _ in deltas]
     S.sfs_(ubar, tau, u, g, gl, deltas)  # warm-up
@@ -343,12 +386,105 @@ def filter_measure(dev, g, st_state, reps=3):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / reps
-    ok = all(bool(torch.isfinite(t).all()) for grp in tau for t in grp)
-    del u, ubar, tau
     gl.close()
+    u64 = [c.to(torch.complex128) for c in u]
+    del u
+    torch.cuda.empty_cache()
+    g64 = S.Grid(3, g.n, dtype=torch.float64, device=dev)
+    gl64 = S.Grid(3, nl, dtype=torch.float64, device=dev)
+    ub64 = [[S.scalarfield(gl64) for _ in range(3)] for _ in deltas]
+    ta64 = [[S.scalarfield(gl64) for _ in range(6)] for _ in deltas]
+    S.sfs_(ub64, ta64, u64, g64, gl64, deltas)
+    torch.cuda.synchronize()
+
+    def rel(a, b):
+        num = sum(float((x.to(torch.complex128) - y).abs().pow(2).sum()) for x, y in zip(a, b))
+        den = sum(float(y.abs().pow(2).sum()) for y in b)
+        return math.sqrt(num / den)
+    err_ubar = [rel(a, b) for a, b in zip(ubar, ub64)]
+    err_tau = [rel(a, b) for a, b in zip(tau, ta64)]
+    del u64, ubar, tau, ub64, ta64
+    g64.close()
+    gl64.close()
     torch.cuda.empty_cache()
     return {"metric": "sfs! 810^3 -> 128^3, Delta/h in {2,4,8} (one call, all three filters)", "ms": ms,
-            "calls_per_s": 1e3 / ms, "finite": ok}
+            "calls_per_s": 1e3 / ms, "rel_l2_fp32_vs_fp64_ubar": err_ubar, "rel_l2_fp32_vs_fp64_tau": err_tau}
+
+
+def cufft_measure(dev, host_full, reps=2):
+    """Comparison only: the same forced 810^3 FP32 RK4 step written with cuFFT
+    (torch.fft: 3 c2r + 6 r2c per right-hand side on the full RFFT arrays) and
+    torch elementwise kernels for the products, viscous term, divergence,
+    2/3 rule, projection, forcing and stage updates.  Device-timed."""
+    import torch
+    n = N_GRID
+    u0 = [c.to(dev) for c in host_full]
+    f = torch.fft.fftfreq(n, 1.0 / n, device=dev).to(torch.float32)
+    K = (torch.arange(n // 2 + 1, device=dev, dtype=torch.float32)[None, None, :], f[None, :, None], f[:, None, None])
+    kc = n // 3
+    mask = (K[0] <= kc) & (K[1].abs() <= kc) & (K[2].abs() <= kc)
+    mask[0, 0, 0] = False
+    k2 = K[0] * K[0] + K[1] * K[1] + K[2] * K[2]
+    k2[0, 0, 0] = 1.0
+    band = mask & (k2 < 9)
+    wdc = torch.where(K[0] > 0, 2.0, 1.0)
+    pairs = [(0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (2, 0)]
+
+    def rhs(u, fft_only=False):
+        v = [torch.fft.irfftn(c, s=(n, n, n), norm="forward") for c in u]
+        du = [torch.zeros_like(c) for c in u]
+        for (i, j) in pairs:
+            sg = torch.fft.rfftn(v[i] * v[j], norm="forward")
+            if fft_only:
+                continue
+            sg = sg - (NU * 1j) * (K[j] * u[i] + K[i] * u[j])
+            du[i] += (-1j * K[j]) * sg
+            if i != j:
+                du[j] += (-1j * K[i]) * sg
+        if fft_only:
+            return du
+        du = [d * mask for d in du]
+        pj = (K[0] * du[0] + K[1] * du[1] + K[2] * du[2]) / k2
+        du = [d - k * pj for d, k in zip(du, K)]
+        ef = sum((wdc * c.abs().square() * band).to(torch.float64).sum() for c in u) / 2
+        A = (EPS / (2 * ef)).to(torch.float32)
+        return [d + A * c * band for d, c in zip(du, u)]
+
+    def step(u):
+        acc = [c.clone() for c in u]
+        kq = rhs(u)
+        for cs, w in ((0.5, 1 / 6), (0.5, 1 / 3), (1.0, 1 / 3), (None, 1 / 6)):
+            for a_, d_ in zip(acc, kq):
+                a_.add_(d_, alpha=w * DT)
+            if cs is None:
+                break
+            kq = rhs([c + (cs * DT) * d for c, d in zip(u, kq)])
+        return acc
+
+    u = step(u0)  # warm-up (cuFFT plans)
+    rhs(u, fft_only=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        u = step(u)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_step = e0.elapsed_time(e1) / reps
+    e0.record()
+    for _ in range(reps):
+        rhs(u, fft_only=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_fft = e0.elapsed_time(e1) / reps
+    del u, u0, mask, k2, band, wdc
+    torch.cuda.empty_cache()
+    return {"what": "comparison only: the same 810^3 FP32 forced RK4 step with cuFFT (torch.fft) and torch "
+                    "elementwise kernels on the full RFFT layout",
+            "steps_per_s": 1e3 / ms_step, "ms_per_step": ms_step,
+            "ms_9_ffts_per_rhs": ms_fft,
+            "note": "ms_9_ffts_per_rhs: the 3 c2r + 6 r2c cuFFT transforms and the 6 physical products of one "
+                    "right-hand side, without the spectral epilogue"}
 
 
 def fp32_vs_fp64_measure(dev, n=256, nsteps=100, every=10):
@@ -411,13 +547,13 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
         gl.close()
     gd.close()
 
-    def make(dtype, idx):
+    def make(dtype, idx, tensor_cores=True):
         jobs = []
         for i in idx:
             nu = ADJ_NU[i % 2]
             g = S.Grid(3, ADJ_N, dtype=dtype, device=dev)
             u0 = [c.to(g.cdtype).contiguous() for c in fields[i // 2]]
-            make = S.create_cnn_closure if dtype == torch.float32 else S.create_cnn_fp_closure
+            make = S.create_cnn_closure if (dtype == torch.float32 and tensor_cores) else S.create_cnn_fp_closure
             cl = make(ADJ_DH * g.l / ADJ_N, nu, g, ws, bs, mu=5.0, sigma=2.0)
             rng = np.random.default_rng(ADJ_SEED * 100 + i)
             S.closure_set_params(cl, theta * (1 + 0.01 * rng.standard_normal(theta.size)))
@@ -426,18 +562,23 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
             jobs.append(dict(grid=g, closure=cl, u0=u0, traj=traj, dt=ADJ_DT, visc=nu, nsteps=nsteps, ckpt_every=ck))
         return jobs
 
-    jobs32 = make(torch.float32, range(8))
-    S.rollout_adjoint_batch(jobs32)  # warm-up
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    res32 = S.rollout_adjoint_batch(jobs32)
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    for j in jobs32:
-        j["closure"].close()
-        j["grid"].close()
-    del jobs32
-    torch.cuda.empty_cache()
+    def run_batch(tensor_cores):
+        jobs = make(torch.float32, range(8), tensor_cores)
+        S.rollout_adjoint_batch(jobs)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = S.rollout_adjoint_batch(jobs)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        for j in jobs:
+            j["closure"].close()
+            j["grid"].close()
+        del jobs
+        torch.cuda.empty_cache()
+        return res, t
+
+    res32, t_batch = run_batch(True)
+    res32cc, t_batch_cc = run_batch(False)
 
     jobs64 = make(torch.float64, range(plain_instances))
     torch.cuda.synchronize()
@@ -448,6 +589,8 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
     t_plain = (time.perf_counter() - t0) / plain_instances
     errs = [float(np.linalg.norm(res32[i][1] - res64[i][1]) / np.linalg.norm(res64[i][1]))
             for i in range(plain_instances)]
+    errs_cc = [float(np.linalg.norm(res32cc[i][1] - res64[i][1]) / np.linalg.norm(res64[i][1]))
+               for i in range(plain_instances)]
     for j in jobs64:
         j["closure"].close()
         j["grid"].close()
@@ -459,6 +602,12 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
         "speedup_vs_plain": (8 * t_plain) / t_batch,
         "grad_rel_err_fp32_vs_fp64": errs,
         "losses": [r[0] for r in res32],
+        "fp32_cuda_cores": {
+            "what": "the same batched training step with the CNN on CUDA cores in FP32 (no BF16 rounding): the "
+                    "path whose gradient matches FP64",
+            "value": 8 * nsteps / t_batch_cc, "unit": "steps/s", "s_per_training_step": t_batch_cc,
+            "speedup_vs_plain": (8 * t_plain) / t_batch_cc,
+            "grad_rel_err_fp32_vs_fp64": errs_cc},
         "config": f"64^3, nu in {list(ADJ_NU)}, Delta/h={ADJ_DH}, RK4 dt={ADJ_DT}, {nsteps} steps, checkpoint every "
                   f"{ck}; CNN closure (4 layers 3x3x3, 32 channels, GELU, seeded Kaiming weights): batched on "
                   "tcgen05 BF16 (forward and input-gradient convolutions; weight gradients on CUDA cores in FP32), "
@@ -579,22 +728,22 @@ def run_gpu(args):
     if rank == 0 and not args.skip_les:
         les = les_batch_measure(dev, args.les_steps, 3)
 
-    filt = c1 = None
+    filt = c1 = cuf = None
     if rank == 0 and not args.skip_extra:
         filt = filter_measure(dev, g, st)
         c1 = fp32_vs_fp64_measure(dev)
+        cuf = cufft_measure(dev, host)
 
     adj = None
     if rank == 0 and not args.skip_adj:
         adj = les_adjoint_measure(dev, args.adj_steps, 5)
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.skip_cpu:
-        sec = cpu_sample_steps(args.cpu_sample_n, 1)
-        v = 1.0 / scale_to_810(sec, args.cpu_sample_n)
-        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-               "sample": f"1 forced RK4 step of the FP64 numpy/scipy.fft restatement at {args.cpu_sample_n}^3 "
-                         f"({sec:.2f} s on {os.cpu_count()} threads), scaled to 810^3 by N log N"}
+    if rank == 0 and ws == 1 and not args.skip_cpu and n == N_GRID:
+        sec, cores = cpu_rk4_step(uc)
+        cpu = {"value": 1.0 / sec, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"1 forced RK4 step of the full 810^3 field (the benchmark's own initial field) by the "
+                         f"FP64 numpy/scipy.fft restatement of the reference, {sec:.1f} s on {cores} threads"}
 
     if rank == 0:
         clocks = clk.summary(local)
@@ -619,6 +768,7 @@ def run_gpu(args):
             "les_adjoint": adj,
             "filter": filt,
             "fp32_vs_fp64_256": c1,
+            "cufft_comparison": cuf,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -635,7 +785,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_GRID)
-    ap.add_argument("--cpu-sample-n", type=int, default=256)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-les", action="store_true")
