@@ -12,6 +12,8 @@ in the build environment); the same entry points are exercised from Python.
 module SymCodeB200
 
 using CUDA
+using ChainRulesCore  # a dependency of Zygote, which the reference already uses (Project.toml)
+using JLD2            # the reference's own field-file format (src/solver.jl:76-86, src/data.jl:200-216)
 
 const LIB = get(ENV, "SYMCODE_LIB", joinpath(@__DIR__, "..", "libsymcode.so"))
 
@@ -79,6 +81,85 @@ function sfs!(ubars, τs, u, dns::Plan, les::Plan, Δs)
         dns.ptr, les.ptr, ptrs(u), d, length(d), reduce(vcat, ptrs.(ubars)), reduce(vcat, ptrs.(τs)), stream()))
     return nothing
 end
+
+"`filter_reynolds(ubar, g_les, visc, Δ)` (src/solver.jl:768-774)."
+function filter_reynolds(ubar, les::Plan, visc, Δ)
+    re = Ref{Cdouble}(0)
+    check(ccall((:sc_filter_reynolds, LIB), Cint, (Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, Cdouble, Cdouble, Ptr{Cdouble},
+        Ptr{Cvoid}), les.ptr, ptrs(ubar), visc, Δ, re, stream()))
+    return re[]
+end
+
+"""
+    FieldSeries(nfilters)
+
+Host-side accumulator of the filtered-field series that `create_data`
+(src/data.jl:170-197) writes per filter width: `inputs[k]` (ū per snapshot),
+`outputs[k]` (τ per snapshot), `redelta[k]` (Re_Δ per snapshot), with ū and τ
+as NamedTuples of host `Array{Complex{T},3}` in the reference's spectral layout
+and component names, so `fieldsfile` data written from this path loads with
+the reference's own readers (src/experiment.jl:203-207, src/data.jl:656-803).
+"""
+struct FieldSeries
+    inputs::Vector{Vector{Any}}
+    outputs::Vector{Vector{Any}}
+    redelta::Vector{Vector{Float64}}
+end
+FieldSeries(nfilters::Integer) = FieldSeries([Any[] for _ in 1:nfilters], [Any[] for _ in 1:nfilters],
+                                             [Float64[] for _ in 1:nfilters])
+
+"""
+    push_snapshot!(series, u, dns, les, Δs, visc)
+
+One snapshot of `create_data`'s filter loop (src/data.jl:185-192): `sfs!` of the
+DNS field `u` at every Δ in one call (the DNS products are shared), then the
+device->host copies `map(Array, ubar)` / `map(Array, τ)` and `filter_reynolds`.
+"""
+function push_snapshot!(series::FieldSeries, u, dns::Plan, les::Plan, Δs, visc)
+    T = les.T
+    sz = (les.n ÷ 2 + 1, ntuple(_ -> les.n, les.D - 1)...)
+    nt = les.D == 3 ? 6 : 3
+    ubars = [[CUDA.zeros(Complex{T}, sz) for _ in 1:les.D] for _ in Δs]
+    τs = [[CUDA.zeros(Complex{T}, sz) for _ in 1:nt] for _ in Δs]
+    sfs!(ubars, τs, u, dns, les, Δs)
+    vnames = les.D == 3 ? (:x, :y, :z) : (:x, :y)
+    tnames = les.D == 3 ? (:xx, :yy, :zz, :xy, :yz, :zx) : (:xx, :yy, :xy)
+    for (k, Δ) in enumerate(Δs)
+        push!(series.inputs[k], NamedTuple{vnames}(Tuple(map(Array, ubars[k]))))
+        push!(series.outputs[k], NamedTuple{tnames}(Tuple(map(Array, τs[k]))))
+        push!(series.redelta[k], filter_reynolds(ubars[k], les, visc, Δ))
+    end
+    return series
+end
+
+"""
+    save_fieldsfile(file, series, k; Δ, Δ_factor, visc)
+
+Write filter `k` of `series` as the reference's `fieldsfile` (src/data.jl:207-211):
+`jldsave` to a temporary file and `mv` over `file` (the atomic write of
+`jldsave_atomic`, src/solver.jl:76-86), with the keys `inputs`, `outputs`,
+`redelta`, `Δ`, `Δ_factor`, `visc`.
+"""
+function save_fieldsfile(file, series::FieldSeries, k::Integer; Δ, Δ_factor, visc)
+    tmp = tempname(dirname(file); cleanup = false)
+    try
+        jldsave(tmp; inputs = [x for x in series.inputs[k]], outputs = [x for x in series.outputs[k]],
+                redelta = series.redelta[k], Δ, Δ_factor, visc)
+        mv(tmp, file; force = true)
+    catch
+        isfile(tmp) && rm(tmp; force = true)
+        rethrow()
+    end
+    return file
+end
+
+"""
+    load_fieldsfile(file) -> (; inputs, outputs, redelta, Δ, Δ_factor, visc)
+
+Read a `fieldsfile` (written by the reference or by `save_fieldsfile`) back;
+`CuArray.(values(inputs[i]))` gives the device fields for this library's calls.
+"""
+load_fieldsfile(file) = (; (Symbol(k) => v for (k, v) in JLD2.load(file))...)
 
 "A closure `model(u, G)` bound to a plan (`create_clark`, `create_dynamic_smagorinsky`, ...)."
 mutable struct Closure
@@ -221,6 +302,41 @@ function rollout_adjoint(c::Closure, u0, traj, p::Plan; Δt, visc, nsteps, ckpt_
          Ptr{Cdouble}, Ptr{Cvoid}),
         p.ptr, c.ptr, ptrs(u0), pointer(traj), Δt, visc, nsteps, ckpt_every, loss, grad, stream()))
     return loss[], grad
+end
+
+"""
+    rollout_loss(θ, c, u0, traj, p; Δt, visc, nsteps, ckpt_every = 5)
+
+Trajectory-MSE loss L = 1/nsteps Σ_s ⟨u_s - u*_s, u_s - u*_s⟩ of an RK4 LES
+rollout from `u0` with closure `c` at parameters `θ` against the target
+trajectory `traj` (`rollout_record`).  Zygote differentiates it through the
+`rrule` below, whose pullback is the hand-written adjoint
+(`sc_rollout_adjoint`: RK4 stages recomputed from checkpoints every
+`ckpt_every` steps) instead of tracing the solver (the reference's in-place
+KernelAbstractions kernels, src/solver.jl:434-521, are not differentiable by
+Zygote).
+"""
+function rollout_loss(θ::AbstractVector{<:Real}, c::Closure, u0, traj, p::Plan; Δt, visc, nsteps,
+                      ckpt_every = 5)
+    set_params!(c, Vector{Float64}(θ))
+    loss = Ref{Cdouble}(0)
+    check(ccall((:sc_rollout_loss, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{CuPtr{Cvoid}}, CuPtr{Cvoid}, Cdouble, Cdouble, Cint, Ptr{Cdouble}, Ptr{Cvoid}),
+        p.ptr, c.ptr, ptrs(u0), pointer(traj), Δt, visc, nsteps, loss, stream()))
+    return loss[]
+end
+
+# Only θ is differentiated: the initial state, the target trajectory, the
+# closure object and the plan get NoTangent (the C ABI returns dL/dθ only).
+function ChainRulesCore.rrule(::typeof(rollout_loss), θ::AbstractVector{<:Real}, c::Closure, u0, traj, p::Plan;
+                              Δt, visc, nsteps, ckpt_every = 5)
+    set_params!(c, Vector{Float64}(θ))
+    loss, grad = rollout_adjoint(c, u0, traj, p; Δt, visc, nsteps, ckpt_every)
+    function rollout_loss_pullback(ȳ)
+        dθ = ProjectTo(θ)(unthunk(ȳ) .* grad)
+        return (NoTangent(), dθ, NoTangent(), NoTangent(), NoTangent(), NoTangent())
+    end
+    return loss, rollout_loss_pullback
 end
 
 end # module
