@@ -273,7 +273,24 @@ SC_API int sc_les_batch_destroy(sc_les_batch* batch);
  * Takes effect at the next evaluation (not in step graphs captured before the
  * change). */
 #define SC_OPT_WAIT_LIMIT 2
+/* Kernel variant of one sweep of the 3D product pipeline of an FP32 plan
+ * (value 0 .. sc_plan_num_variants - 1; 0 is the default): the candidates of
+ * the autotuner (symcode.autotune), which times every variant of every sweep
+ * on the plan's own buffers and keeps the fastest.  The variants are the same
+ * transforms by other tile widths, splits N = N1 N2 or x-sweep kernels; the
+ * steppers' cached graphs are rebuilt after a change.  No reference
+ * counterpart (the reference's plan choice is cuFFT/FFTW planning,
+ * src/solver.jl:432). */
+#define SC_OPT_VARIANT_ZINV 3
+#define SC_OPT_VARIANT_YINV 4
+#define SC_OPT_VARIANT_X 5
+#define SC_OPT_VARIANT_YFWD 6
+#define SC_OPT_VARIANT_ZFWD 7
 SC_API int sc_plan_set_option(sc_plan* plan, int option, long long value);
+/* Number of variants of sweep 0..4 (z-inverse, y-inverse, x, y-forward,
+ * z-forward) for this plan (1 where there is no choice: FP64 plans, 2D, sizes
+ * without the FP32 two-level engine). */
+SC_API int sc_plan_num_variants(const sc_plan* plan, int sweep, int* count);
 
 /* ---- a-posteriori training: rollout, loss and hand-written adjoint ----------
  * New (the reference trains a-priori only, src/training.jl:3-109).  A rollout

@@ -79,6 +79,9 @@ struct sc_plan {
   double k_wray[3] = {0, 0, 0};
   int use_graph = 1;  // SC_OPT_USE_GRAPH
   long long wait_limit = sc::kDefaultWaitLimit;  // SC_OPT_WAIT_LIMIT
+  // kernel variant of each sweep of the product pipeline (SC_OPT_VARIANT_*:
+  // z-inverse, y-inverse, x, y-forward, z-forward), chosen by the autotuner
+  int variant[5] = {0, 0, 0, 0, 0};
 };
 
 // A closure model `model(u, G) -> tau` (src/les.jl:19, src/closures.jl) bound
@@ -258,27 +261,32 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
     a = z_inverse_args(K1, K2, n, kc);
     for (int c = 0; c < 3; ++c) { a.in[c] = u[c]; a.out[c] = p->be[c]; }
     a.ncomp = 3;
+    a.variant = p->variant[0];
     if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
     mark();
     sc::ColArgs b = y_inverse_args(K1, n, kc);
     for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
     b.ncomp = 3;
+    b.variant = p->variant[1];
     sc::launch_col_inv<R>(n, b, p->tw, st);
     mark();
     sc::XArgs x{};
     for (int c = 0; c < 3; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 6; ++c) x.out[c] = p->dd[c];
     x.D = 3; x.K1in = K1; x.K1out = K1o; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
+    x.variant = p->variant[2];
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
     mark();
     sc::ColArgs f = y_forward_args(K1o, n, kout);
     for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
     f.ncomp = 6;
+    f.variant = p->variant[3];
     sc::launch_col_fwd<R>(n, f, p->tw, st);
     mark();
     sc::ColArgs g = z_forward_args(K1o, n, kout);
     for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = sig[c]; }
     g.ncomp = 6;
+    g.variant = p->variant[4];
     sc::launch_col_fwd<R>(n, g, p->tw, st);
     mark();
   } else {
@@ -2277,11 +2285,31 @@ int sc_rollout_adjoint_batch(int njobs, const sc_rollout_job* jobs, int* status,
   return SC_OK;
 }
 
+int sc_plan_num_variants(const sc_plan* p, int sweep, int* count) {
+  if (!p || !count || sweep < 0 || sweep > 4) return fail(SC_ERR_INVALID, "bad argument");
+  *count = 1;
+  if (p->dtype != SC_FLOAT32 || !sc::fast_supported(p->n)) return SC_OK;
+  if (p->D != 3) return SC_OK;
+  *count = sweep == 2 ? sc::xsweep_variants(p->n, p->D) : sc::col2_variants(p->n);
+  return SC_OK;
+}
+
 int sc_plan_set_option(sc_plan* p, int option, long long value) {
   if (!p) return fail(SC_ERR_INVALID, "null plan");
   if (option == SC_OPT_USE_GRAPH) { p->use_graph = value ? 1 : 0; return SC_OK; }
   if (option == SC_OPT_WAIT_LIMIT) {
     p->wait_limit = value < 0 ? sc::kDefaultWaitLimit : value;
+    return SC_OK;
+  }
+  if (option >= SC_OPT_VARIANT_ZINV && option <= SC_OPT_VARIANT_ZFWD) {
+    const int sweep = option - SC_OPT_VARIANT_ZINV;
+    int nv = 0;
+    sc_plan_num_variants(p, sweep, &nv);
+    if (value < 0 || value >= nv) return fail(SC_ERR_INVALID, "sweep %d has %d variants", sweep, nv);
+    p->variant[sweep] = int(value);
+    // cached step graphs hold the old launches
+    if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
+    if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
     return SC_OK;
   }
   return fail(SC_ERR_INVALID, "unknown option %d", option);

@@ -19,11 +19,17 @@
 
 namespace sc {
 
-template <int N> struct Split;
-template <> struct Split<810> { static constexpr int N1 = 27, N2 = 30; };
-template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
-template <> struct Split<128> { static constexpr int N1 = 16, N2 = 8; };
-template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+// N = N1 * N2 of the two-level column sweeps; S = 1 is the transposed split,
+// one of the autotuner's candidates (the x sweeps use S = 0).
+template <int N, int S = 0> struct Split;
+template <> struct Split<810, 0> { static constexpr int N1 = 27, N2 = 30; };
+template <> struct Split<810, 1> { static constexpr int N1 = 30, N2 = 27; };
+template <> struct Split<256, 0> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<256, 1> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<128, 0> { static constexpr int N1 = 16, N2 = 8; };
+template <> struct Split<128, 1> { static constexpr int N1 = 8, N2 = 16; };
+template <> struct Split<64, 0> { static constexpr int N1 = 8, N2 = 8; };
+template <> struct Split<64, 1> { static constexpr int N1 = 8, N2 = 8; };
 
 __device__ __forceinline__ int cpos(int f, int N, int kpos, int kneg) {
   return f < kpos ? f : (f >= N - kneg ? f - N + kpos + kneg : -1);
@@ -32,13 +38,14 @@ __device__ __forceinline__ int cpos(int f, int N, int kpos, int kneg) {
 // ---------------------------------------------------------------------------
 // column sweeps: tile of T consecutive kx, one column c, all N elements
 // ---------------------------------------------------------------------------
-template <int N, int T> struct Col2Cfg {
-  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+template <int N, int T, int S = 0> struct Col2Cfg {
+  static constexpr int N1 = Split<N, S>::N1, N2 = Split<N, S>::N2;
   static constexpr int NJ = N1 > N2 ? N1 : N2;
   static constexpr int NT = T * NJ;
   static constexpr int SR = N2 * T + 8;  // exchange row stride (+8: half-bank shift between rows)
   static constexpr size_t SMEM = size_t(N1) * SR * sizeof(float2);
-  static constexpr int MINB = N == 810 ? 3 : 1;  // 80 registers at 810: three CTAs per SM
+  // at 810 the tile of 8 columns keeps 80 registers and three CTAs per SM
+  static constexpr int MINB = N == 810 ? (T == 4 ? 6 : (T == 8 ? 3 : 1)) : 1;
 };
 
 // Where a block of B consecutive transform indices e0 .. e0 + B - 1 falls in
@@ -58,11 +65,11 @@ constexpr int crange(int e0, int B, int N, int kpos, int kneg) {
 // or N2 stores (forward) touch a retained mode is known at compile time except
 // in the one block that straddles a boundary; the unused forward outputs are
 // then never formed.
-template <int N, int T, bool INV, bool DRV, bool FULL>
-__global__ void __launch_bounds__(Col2Cfg<N, T>::NT, Col2Cfg<N, T>::MINB)
+template <int N, int T, bool INV, bool DRV, bool FULL, int S = 0>
+__global__ void __launch_bounds__(Col2Cfg<N, T, S>::NT, Col2Cfg<N, T, S>::MINB)
 k_col2(const ColArgs a, const float2* __restrict__ tw) {
   using C = float2;
-  using Cfg = Col2Cfg<N, T>;
+  using Cfg = Col2Cfg<N, T, S>;
   constexpr int N1 = Cfg::N1, N2 = Cfg::N2, SR = Cfg::SR;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* ys = reinterpret_cast<C*>(smem_raw);
@@ -839,18 +846,51 @@ template <typename F> static void set_smem2(F* f, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
 }
 
-template <int N> constexpr int col_tile() { return N == 810 ? 8 : 16; }
+// Column-sweep variants the autotuner chooses from, per N: (tile width T,
+// split S).  Variant 0 is the default; launches with derivative outputs always
+// use variant 0.
+template <int N> struct ColVariants;
+template <> struct ColVariants<810> {
+  static constexpr int count = 4;
+  static constexpr int T[4] = {8, 8, 4, 16}, S[4] = {0, 1, 0, 0};
+};
+template <> struct ColVariants<256> {
+  static constexpr int count = 2;
+  static constexpr int T[2] = {16, 8}, S[2] = {0, 0};
+};
+template <> struct ColVariants<128> {
+  static constexpr int count = 3;
+  static constexpr int T[3] = {16, 8, 16}, S[3] = {0, 0, 1};
+};
+template <> struct ColVariants<64> {
+  static constexpr int count = 2;
+  static constexpr int T[2] = {16, 8}, S[2] = {0, 0};
+};
+
+template <int N, int T, int S> static void init_col2_variant() {
+  using Cfg = Col2Cfg<N, T, S>;
+  set_smem2(k_col2<N, T, true, false, false, S>, Cfg::SMEM);
+  set_smem2(k_col2<N, T, true, false, true, S>, Cfg::SMEM);
+  set_smem2(k_col2<N, T, false, false, false, S>, Cfg::SMEM);
+  set_smem2(k_col2<N, T, false, false, true, S>, Cfg::SMEM);
+}
+
+template <int N, int V = 0> static void init_col2_variants() {
+  if constexpr (V < ColVariants<N>::count) {
+    init_col2_variant<N, ColVariants<N>::T[V], ColVariants<N>::S[V]>();
+    init_col2_variants<N, V + 1>();
+  }
+}
 
 template <int N> static void init_fast_n() {
-  constexpr int T = col_tile<N>();
+  constexpr int T = ColVariants<N>::T[0];
   set_smem2(k_col2<N, T, true, true, false>, Col2Cfg<N, T>::SMEM);
   set_smem2(k_col2<N, T, true, true, true>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, true, false, false>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, true, false, true>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, false, false, false>, Col2Cfg<N, T>::SMEM);
-  set_smem2(k_col2<N, T, false, false, true>, Col2Cfg<N, T>::SMEM);
+  init_col2_variants<N>();
   set_smem2(k_xsweep2<N, 2>, X2Cfg<N, 2>::SMEM);
+  set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
   set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
+  if (N == 810) set_smem2(k_xsweep4<true>, X4Cfg::SMEM), set_smem2(k_xsweep4<false>, X4Cfg::SMEM);
 }
 
 bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64; }
@@ -871,21 +911,37 @@ bool init_fast(int N) {
 // beat persistent cp.async-staged variants (one or two CTAs per SM, double-
 // buffered tiles) in both directions (810^3 inverse y sweep, 81 planes:
 // 0.166 ms against 0.283 ms for a persistent three-level kernel).
-template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
-  constexpr int T = col_tile<N>();
-  using Cfg = Col2Cfg<N, T>;
-  dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + (INV ? a.ndrv : 0));
-  const float2* t2 = static_cast<const float2*>(tw);
+template <int N, int T, int S, bool INV> static void col2_launch(const ColArgs& a, const float2* t2, cudaStream_t st) {
+  using Cfg = Col2Cfg<N, T, S>;
+  dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp);
   const bool full = a.kpos == N / 3 + 1 && a.kneg == N / 3;
+  if (full) k_col2<N, T, INV, false, true, S><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+  else k_col2<N, T, INV, false, false, S><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+}
+
+template <int N, bool INV, int V = 0> static void col2_variant(int v, const ColArgs& a, const float2* t2,
+                                                              cudaStream_t st) {
+  if constexpr (V < ColVariants<N>::count) {
+    if (v == V) col2_launch<N, ColVariants<N>::T[V], ColVariants<N>::S[V], INV>(a, t2, st);
+    else col2_variant<N, INV, V + 1>(v, a, t2, st);
+  }
+}
+
+template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, cudaStream_t st) {
+  const float2* t2 = static_cast<const float2*>(tw);
   if constexpr (INV) {
     if (a.ndrv > 0) {
+      constexpr int T = ColVariants<N>::T[0];
+      using Cfg = Col2Cfg<N, T>;
+      dim3 grid((a.K1 + T - 1) / T, a.ncols, a.ncomp + a.ndrv);
+      const bool full = a.kpos == N / 3 + 1 && a.kneg == N / 3;
       if (full) k_col2<N, T, true, true, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
       else k_col2<N, T, true, true, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
       return;
     }
   }
-  if (full) k_col2<N, T, INV, false, true><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
-  else k_col2<N, T, INV, false, false><<<grid, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+  const int v = a.variant >= 0 && a.variant < ColVariants<N>::count ? a.variant : 0;
+  col2_variant<N, INV>(v, a, t2, st);
 }
 
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st) {
@@ -898,14 +954,45 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
   }
 }
 
+int col2_variants(int N) {
+  switch (N) {
+    case 810: return ColVariants<810>::count;
+    case 256: return ColVariants<256>::count;
+    case 128: return ColVariants<128>::count;
+    case 64: return ColVariants<64>::count;
+    default: return 1;
+  }
+}
+
+// x-sweep variants (3D): at 810, 0 = the paired-row f32x2 sweep, 1 = the
+// scalar three-level sweep, 2 = the two-level sweep of four rows per CTA;
+// elsewhere 0 = the two-level four-row-group sweep, 1 = the plain two-level sweep.
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
+  const float2* t2 = static_cast<const float2*>(tw);
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
-  if (N == 810 && a.D == 3) {
-    launch_xpair810(a, static_cast<const float2*>(tw) + 810, st);
-  } else if (a.D == 3) {
-    const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
-    k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, static_cast<const float2*>(tw));
-  } else k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, static_cast<const float2*>(tw));
+  const unsigned nb3 = unsigned((a.nrows + X3Rows<N>::TR - 1) / X3Rows<N>::TR);
+  if (a.D == 2) {
+    k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, t2);
+  } else if (N == 810) {
+    if (a.variant == 1) {
+      const unsigned nb4 = unsigned((a.nrows + 1) / 2);
+      if (a.K1in == 271 && a.K1out == 271) k_xsweep4<true><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, t2);
+      else k_xsweep4<false><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, t2);
+    } else if (a.variant == 2) {
+      k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, t2);
+    } else {
+      launch_xpair810(a, t2 + 810, st);
+    }
+  } else if (a.variant == 1) {
+    k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, t2);
+  } else {
+    k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, t2);
+  }
+}
+
+int xsweep_variants(int N, int D) {
+  if (D != 3 || !fast_supported(N)) return 1;
+  return N == 810 ? 3 : 2;
 }
 
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st) {

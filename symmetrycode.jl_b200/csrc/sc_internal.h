@@ -29,6 +29,7 @@ struct ColArgs {
   int ndrv;
   int drv_src[kMaxComp];
   double kfac;
+  int variant;  // FP32 fast sizes: kernel variant chosen by the autotuner (0 = default)
 };
 
 // The x sweep of the Navier-Stokes right-hand side: per row (y[, z]) read the
@@ -42,6 +43,7 @@ struct XArgs {
   int K1in, K1out;
   long long nrows;
   double scale;
+  int variant;  // FP32 fast sizes: kernel variant chosen by the autotuner (0 = default)
 };
 
 // Plain batched c2r / r2c along x for `ncomp` rows-of-fields (FFT API).
@@ -130,6 +132,9 @@ bool fast_supported(int N);
 bool init_fast(int N);
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st);
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st);
+// number of autotuner variants of the FP32 column sweeps / 3D x sweep of size N
+int col2_variants(int N);
+int xsweep_variants(int N, int D);
 // FP32 n = 810 x sweep on paired rows (sc_xpair.cu).  Its twiddles are the
 // plain table's exp(-2 pi i j / 810) as register-pair entries
 // (c, c, s, s, -s, -s, 0, 0), stored in the same device buffer right after the

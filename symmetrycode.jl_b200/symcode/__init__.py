@@ -18,7 +18,7 @@ import math
 
 import torch
 
-from . import fields
+from . import autotune, fields  # noqa: F401
 from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
                    ptr_array, sc_forcing, sc_les_instance)
 

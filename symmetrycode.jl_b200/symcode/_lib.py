@@ -17,6 +17,7 @@ HEADER = os.path.join(os.path.dirname(PKG_DIR), "include", "symcode.h")
 SC_OK, SC_ERR_INVALID, SC_ERR_SIZE, SC_ERR_CUDA, SC_ERR_OOM, SC_ERR_DIVERGED, SC_ERR_UNSUPPORTED, SC_ERR_TIMEOUT = range(8)
 SC_FLOAT32, SC_FLOAT64 = 0, 1
 SC_OPT_USE_GRAPH, SC_OPT_WAIT_LIMIT = 1, 2  # sc_plan_set_option
+SC_OPT_VARIANT_ZINV = 3  # ... SC_OPT_VARIANT_ZFWD = 7: sweep variants (z-inv, y-inv, x, y-fwd, z-fwd)
 
 
 class SymcodeError(RuntimeError):
@@ -92,6 +93,7 @@ _SIGS = {
     "sc_les_batch_status": ([_vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, _vp], ct.c_int),
     "sc_les_batch_destroy": ([_vp], ct.c_int),
     "sc_plan_set_option": ([_vp, ct.c_int, ct.c_longlong], ct.c_int),
+    "sc_plan_num_variants": ([_vp, ct.c_int, ct.POINTER(ct.c_int)], ct.c_int),
     "sc_propose_timestep": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_shell_energies": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_maintain_shell_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),

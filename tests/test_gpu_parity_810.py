@@ -166,3 +166,60 @@ def test_sfs_810_fp32_matches_oracle(bench_field, oracle810):
         assert et < 1e-5
     gd.close()
     gl.close()
+
+
+def test_every_810_sweep_variant_matches_triad_oracle():
+    """Every kernel variant the autotuner may pick at 810 (column tiles 8 / 4 /
+    16, the 30 x 27 split, the three x-sweep kernels) computes the same FP32
+    right-hand side, pinned to the exact triad oracle."""
+    from symcode import autotune as A
+    k, u = T.random_sparse_field(N, 200, 23, extra=EDGES)
+    kout, du_ref = T.convectiondiffusion(k, u, N, NU)
+    g = S.Grid(3, N, dtype=torch.float32, device=DEV)
+    kf, uf = T.full_modes(k, u)
+    m = kf[:, 0] >= 0
+    iz, iy, ix = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kf[m], N))
+    uin = []
+    for c in range(3):
+        t = torch.zeros(g.spec_shape, dtype=g.cdtype, device=DEV)
+        t[iz, iy, ix] = torch.from_numpy(uf[m][:, c]).to(g.cdtype).to(DEV)
+        uin.append(t)
+    oz, oy, ox = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kout, N))
+    ref = [torch.from_numpy(du_ref[:, c]).to(DEV) for c in range(3)]
+    counts = A.num_variants(g)
+    assert counts == [4, 4, 3, 4, 4]
+    du = S.vectorfield(g)
+    for s, name in enumerate(A.SWEEPS):
+        for v in range(counts[s]):
+            A.set_variants(g, {nm: (v if nm == name else 0) for nm in A.SWEEPS})
+            S.convectiondiffusion_(du, uin, g, NU)
+            num = den = 0.0
+            for c in range(3):
+                got = du[c][oz, oy, ox].to(torch.complex128)
+                total = float(du[c].abs().to(torch.float64).pow(2).sum())
+                num += float((got - ref[c]).abs().pow(2).sum()) + max(total - float(got.abs().pow(2).sum()), 0.0)
+                den += float(ref[c].abs().pow(2).sum())
+            err = math.sqrt(num / den)
+            print(f"{name} variant {v}: {err:.3e}")
+            assert err < 1e-5, (name, v, err)
+    g.close()
+
+
+def test_autotune_picks_the_fastest_measured_variant(tmp_path):
+    from symcode import autotune as A
+    g = S.Grid(3, N, dtype=torch.float32, device=DEV)
+    st = S.State(g)
+    # any state: the timing does not depend on the field
+    st.load([torch.zeros(g.spec_shape, dtype=g.cdtype, device=DEV) for _ in range(3)])
+    cache = str(tmp_path / "tune.json")
+    rep = A.tune(g, visc=NU, reps=2, cache=cache)
+    assert rep["source"] == "timed"
+    counts = A.num_variants(g)
+    timings = {int(v): t for v, t in rep["ms"].items()}
+    for s, name in enumerate(A.SWEEPS):
+        best = min(range(counts[s]), key=lambda v: (timings[v][name], v))
+        assert rep["variants"][name] == best
+    # a second plan of the same shape takes the cached choice without timing
+    rep2 = A.tune(g, visc=NU, cache=cache)
+    assert rep2["source"] == "cache" and rep2["variants"] == rep["variants"]
+    g.close()
