@@ -1186,6 +1186,8 @@ int sc_state_profile_rhs(sc_plan* p, double visc, int reps, double* ms, int* nke
 namespace {
 template <typename R>
 int microbench_impl(int kernel, int n, long long count, int reps, double* ms, double* bytes) {
+  const int variant = kernel >> 8;  // autotuner variant of the sweep (sc_plan_num_variants)
+  kernel &= 0xff;
   const int kc = n / 3, K1 = kc + 1, K2 = 2 * kc + 1;
   const size_t esz = sizeof(typename sc::V2<R>::T);
   std::vector<void*> bufs;
@@ -1231,6 +1233,7 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
     for (int c = 0; c < 3; ++c) xa.in[c] = alloc((size_t)K1 * count);
     for (int c = 0; c < 6; ++c) xa.out[c] = alloc((size_t)K1 * count);
     xa.D = 3; xa.K1in = K1; xa.K1out = K1; xa.nrows = count; xa.scale = 1.0 / ((double)n * n * n);
+    xa.variant = variant;
     b = 9.0 * K1 * count * esz;
   } else {
     cleanup();
@@ -1264,7 +1267,7 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
 extern "C" {
 
 int sc_microbench(int kernel, int n, int dtype, long long count, int reps, double* ms, double* bytes) {
-  if (!ms || !bytes || reps < 1 || count < 1) return fail(SC_ERR_INVALID, "bad argument");
+  if (!ms || !bytes || reps < 1 || count < 1 || kernel < 0) return fail(SC_ERR_INVALID, "bad argument");
   if (!sc::fft_size_supported(n)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
   return dtype == SC_FLOAT64 ? microbench_impl<double>(kernel, n, count, reps, ms, bytes)
                              : microbench_impl<float>(kernel, n, count, reps, ms, bytes);

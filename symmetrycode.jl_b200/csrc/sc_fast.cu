@@ -965,7 +965,8 @@ int col2_variants(int N) {
 }
 
 // x-sweep variants (3D): at 810, 0 = the paired-row f32x2 sweep, 1 = the
-// scalar three-level sweep, 2 = the two-level sweep of four rows per CTA;
+// scalar three-level sweep, 2 = the two-level sweep of four rows per CTA,
+// 3 = the paired-row sweep with four CTAs per SM (more registers);
 // elsewhere 0 = the two-level four-row-group sweep, 1 = the plain two-level sweep.
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const float2* t2 = static_cast<const float2*>(tw);
@@ -981,7 +982,7 @@ template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t s
     } else if (a.variant == 2) {
       k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, t2);
     } else {
-      launch_xpair810(a, t2 + 810, st);
+      launch_xpair810(a, t2 + 810, a.variant == 3 ? 4 : 5, st);
     }
   } else if (a.variant == 1) {
     k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, t2);
@@ -992,7 +993,7 @@ template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t s
 
 int xsweep_variants(int N, int D) {
   if (D != 3 || !fast_supported(N)) return 1;
-  return N == 810 ? 3 : 2;
+  return N == 810 ? 4 : 2;
 }
 
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st) {

@@ -142,7 +142,7 @@ int xsweep_variants(int N, int D);
 size_t xpair810_twiddle_bytes();
 void xpair810_twiddles(const float2* tw, float* out8);
 bool init_xpair810();
-void launch_xpair810(const XArgs& a, const void* twp_table, cudaStream_t st);
+void launch_xpair810(const XArgs& a, const void* twp_table, int minb, cudaStream_t st);
 // bytes of a plan's twiddle buffer: the plain table plus, for FP32 n = 810, the pair table
 inline size_t twiddle_buffer_bytes(int n, size_t esz) {
   return (size_t)n * esz + (esz == 8 && n == 810 ? xpair810_twiddle_bytes() : 0);

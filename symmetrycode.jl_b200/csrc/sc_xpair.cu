@@ -102,8 +102,10 @@ __device__ __forceinline__ void f1_kind(const float2* u1, const float2* u2, cons
   for (int s = 1; s < 9; ++s) ws[90 * s] = pmul(v[s], twp(t4, t * s));
 }
 
-template <bool FULL>
-__global__ void __launch_bounds__(kXT, 5) k_xpair810(const XArgs a, const float4* __restrict__ t4) {
+// MINB: CTAs per SM the register budget is cut for (5: 128 registers; 4: 168,
+// room to keep the DFT constants' register pairs resident)
+template <bool FULL, int MINB>
+__global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const float4* __restrict__ t4) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   P2* s0 = reinterpret_cast<P2*>(smem_raw);
   P2* s1 = s0 + kXPS;
@@ -330,18 +332,24 @@ void xpair810_twiddles(const float2* tw, float* out8) {
 }
 
 bool init_xpair810() {
-  cudaFuncSetAttribute(k_xpair810<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
-  cudaFuncSetAttribute(k_xpair810<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
+  cudaFuncSetAttribute(k_xpair810<true, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
+  cudaFuncSetAttribute(k_xpair810<false, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
+  cudaFuncSetAttribute(k_xpair810<true, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
+  cudaFuncSetAttribute(k_xpair810<false, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kXSmem));
   return cudaGetLastError() == cudaSuccess;
 }
 
-void launch_xpair810(const XArgs& a, const void* twp_table, cudaStream_t st) {
+void launch_xpair810(const XArgs& a, const void* twp_table, int minb, cudaStream_t st) {
   const unsigned nb = unsigned((a.nrows + 1) / 2);
   const float4* t4 = static_cast<const float4*>(twp_table);
-  if (a.K1in == 271 && a.K1out == 271)
-    k_xpair810<true><<<nb, kXT, kXSmem, st>>>(a, t4);
-  else
-    k_xpair810<false><<<nb, kXT, kXSmem, st>>>(a, t4);
+  const bool full = a.K1in == 271 && a.K1out == 271;
+  if (minb == 4) {
+    if (full) k_xpair810<true, 4><<<nb, kXT, kXSmem, st>>>(a, t4);
+    else k_xpair810<false, 4><<<nb, kXT, kXSmem, st>>>(a, t4);
+  } else {
+    if (full) k_xpair810<true, 5><<<nb, kXT, kXSmem, st>>>(a, t4);
+    else k_xpair810<false, 5><<<nb, kXT, kXSmem, st>>>(a, t4);
+  }
 }
 
 }  // namespace sc

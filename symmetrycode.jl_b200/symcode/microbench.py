@@ -54,10 +54,11 @@ def run_cnn(n, count, reps=5):
             "tflops": flops / (best / 1e3) / 1e12}
 
 
-def run(kernel, n, count, dtype="f32", reps=5):
+def run(kernel, n, count, dtype="f32", reps=5, variant=0):
     ms, by = ct.c_double(), ct.c_double()
-    check(lib().sc_microbench(KERNELS[kernel], n, 0 if dtype == "f32" else 1, count, reps, ct.byref(ms), ct.byref(by)))
-    return {"kernel": kernel, "n": n, "count": count, "dtype": dtype, "ms": ms.value,
+    code = KERNELS[kernel] | (int(variant) << 8)  # the sweep's autotuner variant in bits 8..
+    check(lib().sc_microbench(code, n, 0 if dtype == "f32" else 1, count, reps, ct.byref(ms), ct.byref(by)))
+    return {"kernel": kernel, "variant": variant, "n": n, "count": count, "dtype": dtype, "ms": ms.value,
             "bytes": by.value, "gbs": by.value / (ms.value / 1e3) / 1e9}
 
 
@@ -68,11 +69,12 @@ def main(argv=None):
     ap.add_argument("--count", type=int, required=True)
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--variant", type=int, default=0, help="autotuner variant of the sweep (sc_plan_num_variants)")
     a = ap.parse_args(argv)
     if a.kernel == "cnn":
         print(json.dumps(run_cnn(a.n, a.count, a.reps)))
     else:
-        print(json.dumps(run(a.kernel, a.n, a.count, a.dtype, a.reps)))
+        print(json.dumps(run(a.kernel, a.n, a.count, a.dtype, a.reps, a.variant)))
     return 0
 
 

@@ -40,7 +40,9 @@ def test_cnn_wait_timeout_is_reported_and_the_context_recovers():
 
     S.set_option(g, L.SC_OPT_WAIT_LIMIT, 0)  # every pipeline wait gives up at once
     cl = S.create_cnn_closure(delta, nu, g, ws, bs, mu=1.0, sigma=2.0)
-    cl(ut, None)
+    with pytest.raises(S.SymcodeError) as err:  # the evaluation reports the timeout
+        cl(ut, None)
+    assert err.value.status == L.SC_ERR_TIMEOUT
     torch.cuda.synchronize()  # the kernels returned: no hang, no fault
     assert _status(cl) == L.SC_ERR_TIMEOUT
     cl.close()

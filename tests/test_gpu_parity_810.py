@@ -65,6 +65,23 @@ def oracle810():
     o.release()
 
 
+def _triad_err(du, ref, idx):
+    """Relative L2 error of the device spectra du against the triad oracle's
+    values ref at the oracle's modes idx; every other mode must be zero, so its
+    energy counts as error (summed directly: a difference of two large sums
+    would lose it to rounding)."""
+    num = den = 0.0
+    for c in range(3):
+        got = du[c][idx].to(torch.complex128)
+        num += float((got - ref[c]).abs().pow(2).sum())
+        den += float(ref[c].abs().pow(2).sum())
+        rest = du[c].clone()
+        rest[idx] = 0
+        num += float(rest.abs().to(torch.float64).pow(2).sum())
+        del rest
+    return math.sqrt(num / den)
+
+
 # --------------------------------------------------------------- exact (triad) oracle
 EDGES = [(270, 270, 270), (270, -270, 270), (270, 0, -270), (0, 270, -270), (0, 270, 270), (0, 1, 0),
          (0, 0, 1), (1, 1, 1), (2, 0, -1), (1, -2, 1), (135, 270, -3), (269, -1, 270), (3, -270, -270)]
@@ -87,17 +104,9 @@ def test_rhs_810_matches_triad_oracle(dtype, tol):
     S.convectiondiffusion_(du, uin, g, NU)
     del uin
     oz, oy, ox = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kout, N))
-    num = den = 0.0
-    for c in range(3):
-        ref = torch.from_numpy(du_ref[:, c]).to(DEV)
-        got = du[c][oz, oy, ox].to(torch.complex128)
-        total = float(du[c].abs().to(torch.float64).pow(2).sum())
-        at = float(got.abs().pow(2).sum())
-        # every mode the oracle does not list must be zero: count it in the error
-        num += float((got - ref).abs().pow(2).sum()) + max(total - at, 0.0)
-        den += float(ref.abs().pow(2).sum())
+    ref = [torch.from_numpy(du_ref[:, c]).to(DEV) for c in range(3)]
+    err = _triad_err(du, ref, (oz, oy, ox))
     g.close()
-    err = math.sqrt(num / den)
     print(f"810^3 {dtype} rhs vs triad oracle: {err:.3e} over {len(kout)} modes")
     assert err < tol
 
@@ -193,13 +202,7 @@ def test_every_810_sweep_variant_matches_triad_oracle():
         for v in range(counts[s]):
             A.set_variants(g, {nm: (v if nm == name else 0) for nm in A.SWEEPS})
             S.convectiondiffusion_(du, uin, g, NU)
-            num = den = 0.0
-            for c in range(3):
-                got = du[c][oz, oy, ox].to(torch.complex128)
-                total = float(du[c].abs().to(torch.float64).pow(2).sum())
-                num += float((got - ref[c]).abs().pow(2).sum()) + max(total - float(got.abs().pow(2).sum()), 0.0)
-                den += float(ref[c].abs().pow(2).sum())
-            err = math.sqrt(num / den)
+            err = _triad_err(du, ref, (oz, oy, ox))
             print(f"{name} variant {v}: {err:.3e}")
             assert err < 1e-5, (name, v, err)
     g.close()
