@@ -260,6 +260,20 @@ SC_API int sc_les_batch_run(sc_les_batch* batch, int nsteps, void* stream);
 /* Synchronous: per-instance status and energy (energy may be NULL). */
 SC_API int sc_les_batch_status(sc_les_batch* batch, int* status, double* energy, int freeze, void* stream);
 SC_API int sc_les_batch_destroy(sc_les_batch* batch);
+/* The a-posteriori reductions of solve_les!'s reduce! (src/les.jl:94-148),
+ * fused into the batched stepper: every `every` steps of sc_les_batch_run the
+ * step graph also reduces, for every active instance, its kinetic energy,
+ * viscous dissipation (FP64 sums, as sc_les_diagnostics), SFS dissipation,
+ * spectrum and shell transfer (shells 1..nshell) into a device record of at
+ * most max_snap snapshots, with no host round trip during the run; e_post,
+ * which needs a reference trajectory, stays with sc_les_diagnostics.
+ * every = 0 turns it off; calling it again starts a new record.
+ * sc_les_batch_snapshots returns the number recorded and (out != NULL) the
+ * record [nsnap][ninstances][3 + 2 nshell] = (ke, eps_visc, eps_sfs,
+ * spectrum[nshell], transfer[nshell]); synchronous.  Frozen (diverged)
+ * instances keep their last values. */
+SC_API int sc_les_batch_set_snapshots(sc_les_batch* batch, int every, int nshell, int max_snap);
+SC_API int sc_les_batch_snapshots(sc_les_batch* batch, int* nsnap, double* out, void* stream);
 
 /* ---- plan options ---------------------------------------------------------------- */
 #define SC_OPT_USE_GRAPH 1 /* 1 (default): steppers replay a captured CUDA graph; 0: launch eagerly */

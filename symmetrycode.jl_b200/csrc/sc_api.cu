@@ -144,6 +144,15 @@ struct sc_les_batch {
   double* energy = nullptr;  // [ninst] FP64 energies of the last guard
   int* status = nullptr;     // [ninst] 0 ok, SC_ERR_DIVERGED
   int dev = 0;
+  // fused a-posteriori reductions (sc_les_batch_set_snapshots): every `snap_every`
+  // steps the snapshot graph (the step graph plus the reductions) runs instead
+  cudaGraphExec_t snap_graph = nullptr;
+  int snap_every = 0, nshell = 0, max_snap = 0;
+  long long steps_done = 0;  // steps since the snapshots were configured
+  int nsnap = 0;             // snapshots recorded (host count; the device keeps its own)
+  double* scratch = nullptr; // [ninst][stride] reductions of the current snapshot
+  double* snaps = nullptr;   // [max_snap][ninst][stride]
+  int* dcount = nullptr;     // device snapshot counter
 };
 
 namespace {
@@ -2329,8 +2338,71 @@ __global__ void k_guard(const double* e, int* status, int n, double limit) {
   }
 }
 
+// Record stride of one instance's snapshot: ke, eps_visc, eps_sfs, spectrum
+// (nshell shells), shell transfer (nshell shells).
+int snap_stride(int nshell) { return 3 + 2 * nshell; }
+
+// The per-instance reductions of one snapshot into b->scratch, on the
+// instance's stream (the quantities of sc_les_diagnostics, src/les.jl:94-148,
+// without e_post, which needs a reference trajectory).
+template <typename R>
+int snapshot_reductions(sc_les_batch* b, int i, cudaStream_t st) {
+  const sc_les_instance& in = b->inst[i];
+  sc_plan* p = in.plan;
+  const int stride = snap_stride(b->nshell);
+  double* d = b->scratch + (size_t)i * stride;
+  cudaMemsetAsync(d, 0, stride * sizeof(double), st);
+  const double kfac = 2.0 * M_PI / p->l;
+  sc::launch_spectral_energy<R>((const void* const*)p->U, p->D, p->D, p->n, p->K1, p->K2, 1, p->kc, kfac, 0, d, st);
+  sc::launch_spectral_energy<R>((const void* const*)p->U, p->D, p->D, p->n, p->K1, p->K2, 1, p->kc, kfac, 1, d + 1,
+                                st);
+  sc::PackArgs a{};
+  for (int c = 0; c < p->D; ++c) a.src[c] = p->U[c];
+  a.ncomp = p->D; a.D = p->D; a.n = p->n; a.kc = p->kc;
+  sc::launch_spectrum<R>(a, b->nshell, d + 3, st);
+  sc_closure* cl = in.closure && in.closure->kind != sc::kNoClosure ? in.closure : nullptr;
+  if (cl) {
+    int rc = products<R>(p, p->U, st);
+    if (!rc) rc = closure_tauhat<R>(cl, p->U, st);
+    if (rc) return rc;
+    sc::DiagArgs g{};
+    g.D = p->D; g.n = p->n; g.kc = p->kc; g.kfac = kfac;
+    for (int c = 0; c < p->D; ++c) g.u[c] = p->U[c];
+    for (int c = 0; c < (p->D == 3 ? 6 : 3); ++c) g.th[c] = cl->th[c];
+    sc::launch_sfs_diag<R>(g, b->nshell, d + 2, d + 3 + b->nshell, st);
+  }
+  return check_launch("snapshot reductions");
+}
+
+// Append the snapshot scratch to the record (ke = sum/2, eps_visc = visc sum,
+// eps_sfs sign as sc_les_diagnostics) at the device counter, then count it.
+__global__ void k_snap_append(const double* scratch, double* snaps, int* count, const double* visc, int ninst,
+                              int stride, int max_snap) {
+  const int c = *count;
+  if (c < max_snap) {
+    for (int j = threadIdx.x; j < ninst * stride; j += blockDim.x) {
+      const int i = j / stride, q = j - i * stride;
+      double v = scratch[j];
+      if (q == 0) v *= 0.5;
+      else if (q == 1) v *= visc[i];
+      else if (q == 2) v = -v;
+      snaps[(size_t)c * ninst * stride + j] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && c < max_snap) *count = c + 1;
+}
+
+int batch_capture_one(sc_les_batch* b, bool snapshot, cudaGraphExec_t* out);
+
 int batch_capture(sc_les_batch* b) {
-  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  int rc = batch_capture_one(b, false, &b->graph);
+  if (!rc && b->snap_every > 0) rc = batch_capture_one(b, true, &b->snap_graph);
+  return rc;
+}
+
+int batch_capture_one(sc_les_batch* b, bool snapshot, cudaGraphExec_t* out) {
+  if (*out) { cudaGraphExecDestroy(*out); *out = nullptr; }
   const int ni = (int)b->inst.size();
   cudaGraph_t g;
   SC_CU(cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal));
@@ -2353,21 +2425,38 @@ int batch_capture(sc_les_batch* b) {
     else
       sc::launch_spectral_energy<float>((const void* const*)p->U, p->D, p->D, p->n, p->K1, p->K2, 1, p->kc,
                                         2.0 * M_PI / p->l, 0, b->energy + i, b->streams[i]);
+    if (snapshot)
+      rc = p->dtype == SC_FLOAT64 ? snapshot_reductions<double>(b, i, b->streams[i])
+                                  : snapshot_reductions<float>(b, i, b->streams[i]);
     cudaEventRecord(b->events[i], b->streams[i]);
     cudaStreamWaitEvent(b->origin, b->events[i], 0);
   }
   // energy is accumulated as sum |u|^2 (RFFT weights); the guard limit is 2 * 1e5
   k_guard<<<1, 256, 0, b->origin>>>(b->energy, b->status, ni, 2.0e5);
+  if (snapshot)
+    k_snap_append<<<1, 256, 0, b->origin>>>(b->scratch, b->snaps, b->dcount, b->scratch + (size_t)ni * snap_stride(b->nshell),
+                                            ni, snap_stride(b->nshell), b->max_snap);
   cudaError_t e = cudaStreamEndCapture(b->origin, &g);
   if (rc) return rc;
   if (e != cudaSuccess) return fail(SC_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&b->graph, g, 0);
+  e = cudaGraphInstantiate(out, g, 0);
   cudaGraphDestroy(g);
-  if (e != cudaSuccess) { b->graph = nullptr; return fail(SC_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e)); }
+  if (e != cudaSuccess) { *out = nullptr; return fail(SC_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e)); }
   return SC_OK;
 }
 
+void snap_free(sc_les_batch* b) {
+  if (b->snap_graph) cudaGraphExecDestroy(b->snap_graph);
+  if (b->scratch) cudaFree(b->scratch);
+  if (b->snaps) cudaFree(b->snaps);
+  if (b->dcount) cudaFree(b->dcount);
+  b->snap_graph = nullptr; b->scratch = nullptr; b->snaps = nullptr; b->dcount = nullptr;
+  b->snap_every = b->nshell = b->max_snap = b->nsnap = 0;
+  b->steps_done = 0;
+}
+
 void batch_free(sc_les_batch* b) {
+  snap_free(b);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (auto s : b->streams) cudaStreamDestroy(s);
   for (auto e : b->events) cudaEventDestroy(e);
@@ -2424,7 +2513,52 @@ int sc_les_batch_create(sc_les_batch** out, const sc_les_instance* inst, int nin
 int sc_les_batch_run(sc_les_batch* b, int nsteps, void* stream) {
   if (!b || nsteps < 0) return fail(SC_ERR_INVALID, "bad argument");
   SC_CU(cudaSetDevice(b->dev));
-  for (int i = 0; i < nsteps; ++i) SC_CU(cudaGraphLaunch(b->graph, as_stream(stream)));
+  for (int i = 0; i < nsteps; ++i) {
+    ++b->steps_done;
+    const bool snap = b->snap_every > 0 && b->steps_done % b->snap_every == 0 && b->nsnap < b->max_snap;
+    SC_CU(cudaGraphLaunch(snap ? b->snap_graph : b->graph, as_stream(stream)));
+    if (snap) ++b->nsnap;
+  }
+  return SC_OK;
+}
+
+int sc_les_batch_set_snapshots(sc_les_batch* b, int every, int nshell, int max_snap) {
+  if (!b || every < 0 || (every > 0 && (nshell < 1 || max_snap < 1))) return fail(SC_ERR_INVALID, "bad argument");
+  for (const sc_les_instance& in : b->inst)
+    if (every > 0 && nshell > in.plan->kc)
+      return fail(SC_ERR_INVALID, "shells beyond n/3 are not retained (nshell <= %d)", in.plan->kc);
+  SC_CU(cudaSetDevice(b->dev));
+  snap_free(b);
+  if (every == 0) return SC_OK;
+  const int ni = (int)b->inst.size();
+  const size_t stride = snap_stride(nshell);
+  b->snap_every = every; b->nshell = nshell; b->max_snap = max_snap;
+  // scratch: [ninst][stride] reductions, then [ninst] viscosities
+  if (cudaMalloc((void**)&b->scratch, (ni * stride + ni) * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&b->snaps, (size_t)max_snap * ni * stride * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&b->dcount, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    snap_free(b);
+    return fail(SC_ERR_OOM, "snapshot record");
+  }
+  std::vector<double> visc(ni);
+  for (int i = 0; i < ni; ++i) visc[i] = b->inst[i].visc;
+  SC_CU(cudaMemcpy(b->scratch + ni * stride, visc.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
+  SC_CU(cudaMemset(b->dcount, 0, sizeof(int)));
+  SC_CU(cudaMemset(b->snaps, 0, (size_t)max_snap * ni * stride * sizeof(double)));
+  int rc = batch_capture_one(b, true, &b->snap_graph);
+  if (rc) snap_free(b);
+  return rc;
+}
+
+int sc_les_batch_snapshots(sc_les_batch* b, int* nsnap, double* out, void* stream) {
+  if (!b || !nsnap) return fail(SC_ERR_INVALID, "bad argument");
+  *nsnap = b->nsnap;
+  if (!out || b->nsnap == 0) return SC_OK;
+  SC_CU(cudaSetDevice(b->dev));
+  const size_t n = (size_t)b->nsnap * b->inst.size() * snap_stride(b->nshell);
+  SC_CU(cudaMemcpyAsync(out, b->snaps, n * sizeof(double), cudaMemcpyDeviceToHost, as_stream(stream)));
+  SC_CU(cudaStreamSynchronize(as_stream(stream)));
   return SC_OK;
 }
 

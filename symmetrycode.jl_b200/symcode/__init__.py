@@ -546,6 +546,29 @@ class LesBatch:
         check(lib().sc_les_batch_status(self._ptr, st, en, 1 if freeze else 0, _stream_ptr(stream)))
         return list(st), list(en)
 
+    def set_snapshots(self, every, nshell, max_snap):
+        """Fuse reduce!'s reductions (src/les.jl:94-148) into the stepper: every
+        `every` steps, record each instance's ke, eps_visc, eps_sfs, spectrum and
+        shell transfer on the device (``sc_les_batch_set_snapshots``)."""
+        self.nshell = int(nshell)
+        check(lib().sc_les_batch_set_snapshots(self._ptr, int(every), int(nshell), int(max_snap)))
+
+    def snapshots(self, stream=None):
+        """The record so far: a list over snapshots of a list over instances of
+        dicts (ke, eps_visc, eps_sfs, spectrum, transfer)."""
+        import numpy as np
+        ns = ct.c_int()
+        check(lib().sc_les_batch_snapshots(self._ptr, ct.byref(ns), None, _stream_ptr(stream)))
+        if ns.value == 0:
+            return []
+        stride = 3 + 2 * self.nshell
+        buf = np.zeros(ns.value * self.n * stride, dtype=np.float64)
+        check(lib().sc_les_batch_snapshots(self._ptr, ct.byref(ns), buf.ctypes.data_as(ct.POINTER(ct.c_double)),
+                                           _stream_ptr(stream)))
+        rec = buf.reshape(ns.value, self.n, stride)
+        return [[{"ke": r[0], "eps_visc": r[1], "eps_sfs": r[2], "spectrum": r[3:3 + self.nshell].copy(),
+                  "transfer": r[3 + self.nshell:].copy()} for r in snap] for snap in rec]
+
     def close(self):
         if getattr(self, "_ptr", None):
             lib().sc_les_batch_destroy(self._ptr)

@@ -226,3 +226,50 @@ def test_tbnn_closure_matches_oracle(dtype, tol, D, redelta):
     du = S.vectorfield(g)
     S.les_(du, [to_dev(c, g) for c in u], g, cl, visc)
     assert rel_l2([to_np(c) for c in du], ref) < tol
+
+
+def test_les_batch_snapshot_reductions_match_per_snapshot_diagnostics():
+    """reduce! fused into the batched stepper (src/les.jl:94-148): the device
+    record of every second step equals sc_les_diagnostics called on the same
+    states between the steps (FP64, several closure kinds and none)."""
+    n, dt, nshell, every, nsnap = 32, 2e-3, 10, 2, 3
+    go = O.Grid(3, n)
+    specs = [(1e-3, "dynsmag", 2), (6e-4, "clark", 4), (1e-3, None, 2), (3e-4, "smagorinsky", 2)]
+    fields = [O.random_field(go, seed=50 + i, kpeak=3) for i in range(len(specs))]
+
+    def make():
+        out = []
+        for (nu, kind, dh), u in zip(specs, fields):
+            g = S.Grid(3, n, dtype=torch.float64, device="cuda:0")
+            cl = _models(kind, dh * go.l / n, g, 3)[0] if kind else None
+            S.State(g).load([to_dev(c, g) for c in u])
+            out.append(dict(grid=g, closure=cl, visc=nu, dt=dt, eps=None))
+        return out
+
+    insts = make()
+    b = S.LesBatch(insts)
+    b.set_snapshots(every, nshell, nsnap)
+    b.run(every * nsnap + 1)  # one step past the last snapshot: no fourth record
+    rec = b.snapshots()
+    assert len(rec) == nsnap and len(rec[0]) == len(specs)
+
+    singles = make()
+    for s in range(nsnap):
+        for i, d in enumerate(singles):
+            st = S.State(d["grid"])
+            st.les_rk4(d["closure"], dt, d["visc"], nsteps=every)
+            u = S.vectorfield(d["grid"])
+            st.store(u)
+            ref = S.les_diagnostics(u, d["grid"], d["closure"], None, d["visc"], nshell)
+            got = rec[s][i]
+            for k in ("ke", "eps_visc"):
+                assert math.isclose(got[k], ref[k], rel_tol=1e-10), (s, i, k, got[k], ref[k])
+            assert np.allclose(got["spectrum"], ref["spectrum"], rtol=1e-10, atol=1e-300)
+            if d["closure"] is None:
+                assert got["eps_sfs"] == 0 and not np.any(got["transfer"])
+            else:
+                assert math.isclose(got["eps_sfs"], ref["eps_sfs"], rel_tol=1e-9), (s, i)
+                t, tr = got["transfer"], np.array(ref["transfer"])
+                assert np.linalg.norm(t - tr) <= 1e-9 * np.linalg.norm(tr)
+    b.set_snapshots(0, 0, 0)  # off again
+    b.close()
