@@ -18,7 +18,7 @@ import numpy as np
 
 from .spectral import Grid, getenergy, twothirds, vectorgradient
 
-__all__ = ["bf16", "gelu", "gelu_grad", "cnn_redelta_channel", "cnn_rows"]
+__all__ = ["bf16", "gelu", "gelu_grad", "cnn_redelta_channel", "cnn_rows", "cnn_field"]
 
 _GELU_C = math.sqrt(2.0 / math.pi)
 _GELU_A = 0.044715
@@ -91,3 +91,23 @@ def cnn_rows(uphys, zval, weights, biases, rows, round_bf16=True):
                 act = rnd(gelu(act))
         out.append(act[:, 0, 0, :])
     return np.stack(out, 1)
+
+
+def cnn_field(uphys, zval, weights, biases, round_bf16=True):
+    """tau (6, n, n, n) of the CNN closure on the whole periodic grid (the same
+    network and BF16 roundings as :func:`cnn_rows`); each 3x3x3 tap is one
+    (C_out x C_in) by (C_in x n^3) product of a rolled activation."""
+    rnd = bf16 if round_bf16 else (lambda x: np.asarray(x, dtype=np.float64))
+    act = np.concatenate([rnd(uphys), np.full((1,) + uphys.shape[1:], rnd(np.array([zval]))[0])], 0)
+    for li, (w, b) in enumerate(zip(weights, biases)):
+        w = rnd(w)
+        out = np.zeros((w.shape[0],) + act.shape[1:])
+        for kz in range(3):
+            for ky in range(3):
+                for kx in range(3):
+                    sl = np.roll(act, shift=(1 - kz, 1 - ky, 1 - kx), axis=(1, 2, 3))
+                    out += np.tensordot(w[:, :, kz, ky, kx], sl, axes=(1, 0))
+        act = out + np.asarray(b, dtype=np.float64)[:, None, None, None]
+        if li < 3:
+            act = rnd(gelu(act))
+    return act

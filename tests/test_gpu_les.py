@@ -273,3 +273,54 @@ def test_les_batch_snapshot_reductions_match_per_snapshot_diagnostics():
                 assert np.linalg.norm(t - tr) <= 1e-9 * np.linalg.norm(tr)
     b.set_snapshots(0, 0, 0)  # off again
     b.close()
+
+
+def test_les_batch_with_cnn_matches_oracle():
+    """The batch of the 12-instance LES configuration in miniature: a tensor-core
+    CNN instance and a dynamic Smagorinsky instance at 64^3 (FP32) advance in one
+    graph; after one RK4 step each state is compared with the FP64 oracle's RK4
+    step of les! with the same closure (the CNN with BF16 rounding emulated)."""
+    n, dt = 64, 5e-3
+    go = O.Grid(3, n)
+    ws, bs = S.kaiming_cnn_weights(3)
+    specs = [(6e-4, "cnn", 4), (1e-3, "dynsmag", 2)]
+    fields = [O.random_field(go, seed=70 + i, kpeak=4) for i in range(len(specs))]
+    insts, oracles = [], []
+    for (nu, kind, dh), u in zip(specs, fields):
+        g = S.Grid(3, n, dtype=torch.float32, device="cuda:0")
+        delta = dh * go.l / n
+        if kind == "cnn":
+            cl = S.create_cnn_closure(delta, nu, g, ws, bs, mu=5.0, sigma=2.0)
+
+            def model(uu, GG, delta=delta, nu=nu):
+                uphys = np.stack([O.to_phys(O.twothirds(c, go), go) for c in uu], 0)
+                z = O.cnn_redelta_channel(uu, go, delta, nu, mu=5.0, sigma=2.0)
+                return O.cnn_field(uphys, z, ws, bs)
+        else:
+            cl = S.create_dynamic_smagorinsky(delta, g)
+
+            def model(uu, GG, delta=delta):
+                return O.dynamic_smagorinsky(uu, delta, go)
+        S.State(g).load([to_dev(c, g) for c in u])
+        insts.append(dict(grid=g, closure=cl, visc=nu, dt=dt, eps=None))
+        oracles.append((model, nu))
+    b = S.LesBatch(insts)
+    b.run(1)
+    status, _ = b.status()
+    assert status == [0, 0]
+    for d, (model, nu), u, spec in zip(insts, oracles, fields, specs):
+        def rhs(v):
+            return O.project([O.twothirds(c, go) for c in O.les_rhs(v, go, model, nu)], go)
+        k1 = rhs(u)
+        k2 = rhs([a + 0.5 * dt * c for a, c in zip(u, k1)])
+        k3 = rhs([a + 0.5 * dt * c for a, c in zip(u, k2)])
+        k4 = rhs([a + dt * c for a, c in zip(u, k3)])
+        ref = [a + dt / 6 * (p + 2 * q + 2 * r + s) for a, p, q, r, s in zip(u, k1, k2, k3, k4)]
+        out = S.vectorfield(d["grid"])
+        S.State(d["grid"]).store(out)
+        got = [to_np(c) for c in out]
+        e_state = rel_l2(got, ref)
+        e_inc = rel_l2([a - c for a, c in zip(got, u)], [a - c for a, c in zip(ref, u)])
+        print(f"{spec[1]}: state {e_state:.2e}, increment {e_inc:.2e}")
+        assert e_state < 2e-5 and e_inc < 2e-3
+    b.close()

@@ -36,3 +36,16 @@ def test_cnn_rows_window_matches_full_grid():
             act = O.bf16(0.5 * act * (1 + np.tanh(np.sqrt(2 / np.pi) * (act + 0.044715 * act ** 3))))
     ref = np.stack([act[:, z, y, :] for (y, z) in rows], 1)
     np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_cnn_field_equals_cnn_rows():
+    """The whole-grid CNN oracle gives the row oracle's values on its rows."""
+    import symcode as S
+    n = 16
+    rng = np.random.default_rng(0)
+    uphys = rng.standard_normal((3, n, n, n))
+    ws, bs = S.kaiming_cnn_weights(7)
+    f = O.cnn_field(uphys, 0.3, ws, bs)
+    rows = [(0, 0), (5, 7), (15, 3)]
+    r = O.cnn_rows(uphys, 0.3, ws, bs, rows)
+    assert np.array_equal(np.stack([f[:, z, y, :] for (y, z) in rows], 1), r)
