@@ -964,10 +964,11 @@ int col2_variants(int N) {
   }
 }
 
-// x-sweep variants (3D): at 810, 0 = the paired-row f32x2 sweep, 1 = the
-// scalar three-level sweep, 2 = the two-level sweep of four rows per CTA,
-// 3 = the paired-row sweep with four CTAs per SM (more registers);
-// elsewhere 0 = the two-level four-row-group sweep, 1 = the plain two-level sweep.
+// x-sweep variants (3D): at 810, 0 = the scalar three-level sweep (default:
+// the fastest measured), 1 = the paired-row f32x2 sweep at five CTAs per SM,
+// 2 = the same at four CTAs per SM (registers for its twiddles), 3 = the
+// two-level sweep of four rows per CTA; elsewhere 0 = the two-level four-row-
+// group sweep, 1 = the plain two-level sweep.
 template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t st) {
   const float2* t2 = static_cast<const float2*>(tw);
   const unsigned nb = unsigned((a.nrows + X2Rows<N>::TR - 1) / X2Rows<N>::TR);
@@ -975,14 +976,14 @@ template <int N> static void x2_n(const XArgs& a, const void* tw, cudaStream_t s
   if (a.D == 2) {
     k_xsweep2<N, 2><<<nb, X2Cfg<N, 2>::NT, X2Cfg<N, 2>::SMEM, st>>>(a, t2);
   } else if (N == 810) {
-    if (a.variant == 1) {
+    if (a.variant == 1 || a.variant == 2) {
+      launch_xpair810(a, t2 + 810, a.variant == 2 ? 4 : 5, st);
+    } else if (a.variant == 3) {
+      k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, t2);
+    } else {
       const unsigned nb4 = unsigned((a.nrows + 1) / 2);
       if (a.K1in == 271 && a.K1out == 271) k_xsweep4<true><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, t2);
       else k_xsweep4<false><<<nb4, X4Cfg::NT, X4Cfg::SMEM, st>>>(a, t2);
-    } else if (a.variant == 2) {
-      k_xsweep3<N><<<nb3, X3Cfg<N>::NT, X3Cfg<N>::SMEM, st>>>(a, t2);
-    } else {
-      launch_xpair810(a, t2 + 810, a.variant == 3 ? 4 : 5, st);
     }
   } else if (a.variant == 1) {
     k_xsweep2<N, 3><<<nb, X2Cfg<N, 3>::NT, X2Cfg<N, 3>::SMEM, st>>>(a, t2);

