@@ -690,9 +690,12 @@ def run_gpu(args):
     alg = {"z_inverse": per["z_inverse"], "y_inverse": per["y_inverse"], "x_sweep": per["x_sweep"],
            "y_forward": per["y_forward"], "z_forward": 6 * b + 6 * a, "epilogue": 12 * a}
     dom = max(kms, key=lambda kk: kms[kk])
-    # DRAM traffic of the x sweep from one ncu capture (profiles/k_xsweep4_810_x_sweep_65610_rows.md:
-    # 426.9 MB read + 796.2 MB written for 65610 rows), scaled to the launch's n^2 rows
-    traffic = (426.917376e6 + 796.224256e6) / 65610 * n * n if (dom == "x_sweep" and n == 810) else None
+    # DRAM read + write per row of the x sweep at n = 810, from one ncu capture of
+    # each variant's kernel on 65 610 rows (traffic grows with the rows), scaled
+    # to the launch's n^2 rows; variant 0 is k_xsweep4, 1 the paired-row sweep
+    dram_per_row = {0: (426.917376e6 + 796.224256e6) / 65610, 1: (427.062784e6 + 798.828544e6) / 65610}
+    xv = tuned["variants"].get("x_sweep", 0)
+    traffic = dram_per_row[xv] * n * n if (dom == "x_sweep" and n == 810 and xv in dram_per_row) else None
     hbm, src = peaks()
     achieved = alg[dom] / (kms[dom] / 1e3) / 1e9
     step_bytes = 4 * b_rhs
