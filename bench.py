@@ -636,7 +636,8 @@ def run_gpu(args):
     stream = torch.cuda.current_stream()
     forced = True
     # the autotuner times every kernel variant of each sweep on this plan and keeps the fastest
-    tuned = S.autotune.tune(g, visc=NU, reps=3, cache=False)
+    # (a cached choice for this device and grid, $SC_TUNE_CACHE, is reused without timing)
+    tuned = S.autotune.tune(g, visc=NU, reps=3)
     launches_per_step = st.launches_per_step(forced)
 
     # FP32 vs FP64 error of one RK4 step (relative L2 on the state)
@@ -759,7 +760,8 @@ def run_gpu(args):
             "config": {"workload": WORKLOAD, "n": n, "parallelism": f"replicas{ws}" if ws > 1 else "single",
                        "l2": "inputs larger than L2 (5.7 GB compact state; every sweep streams >1 GB)",
                        "err_vs_fp64_one_step": err,
-                       "autotune": {"variants": tuned["variants"], "ms_per_variant": tuned["ms"]}},
+                       "autotune": {"variants": tuned["variants"], "source": tuned["source"],
+                                    "ms_per_variant": tuned["ms"]}},
             "grid_points_per_s": value * n ** 3,
             "step_hbm": {"algorithmic_bytes_per_step": step_bytes, "achieved_gbs": step_gbs,
                          "frac": step_gbs / hbm},
