@@ -120,6 +120,21 @@ SC_API int sc_wray3_step(sc_plan* plan, void* const* u_hat, double dt, double vi
 SC_API int sc_rk4_steps(sc_plan* plan, void* const* u_hat, double dt, double visc, int nsteps,
                  const sc_forcing* forcing, void* stream);
 
+/* ---- initial field ---------------------------------------------------------
+ * randomfield(peak_profile, g; kpeak, totalenergy) (src/solver.jl:576-641,
+ * :523) on the device, in FP64: complex normal coefficients on the retained
+ * 2/3 cube (each part N(0, 1/2)), symmetrize! of the kx = 0 plane, project!,
+ * twothirds!, and the rescale of every shell floor|k| = s to
+ * totalenergy * s^4 exp(-2 (s/kpeak)^2) / sum_s (...).  The result becomes the
+ * plan's state (as sc_state_load) and, when u_hat is not NULL, is written to
+ * u_hat in the full layout.  draws: D device arrays of the coefficients in the
+ * compact layout (complex FP64, (K2, K2, K1) x-fastest; the caller's own
+ * generator), or NULL for the device's counter-based generator keyed by seed
+ * (splitmix64 + Box-Muller; Julia's Xoshiro stream is not reproduced).
+ * Synchronous. */
+SC_API int sc_random_field(sc_plan* plan, unsigned long long seed, const void* const* draws, double kpeak,
+                           double totalenergy, void* const* u_hat, void* stream);
+
 /* ---- device-resident state (compact 2/3 cube held by the plan) ----------- */
 /* Gather the retained modes of u_hat into the plan's state. */
 SC_API int sc_state_load(sc_plan* plan, const void* const* u_hat, void* stream);

@@ -2522,6 +2522,65 @@ int sc_les_batch_run(sc_les_batch* b, int nsteps, void* stream) {
   return SC_OK;
 }
 
+int sc_random_field(sc_plan* p, unsigned long long seed, const void* const* draws, double kpeak, double totalenergy,
+                    void* const* u_hat, void* stream) {
+  if (!p || !(kpeak > 0) || !(totalenergy >= 0)) return fail(SC_ERR_INVALID, "bad argument");
+  if (draws) {
+    int rc = check_ptrs(draws, p->D);
+    if (rc) return rc;
+  }
+  if (u_hat) {
+    int rc = check_ptrs((const void* const*)u_hat, p->D);
+    if (rc) return rc;
+  }
+  int rc = ensure_device(p);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const int D = p->D, n = p->n;
+  // peak_profile(k, kpeak) = k^4 exp(-2 (k / kpeak)^2) on shells 0 .. floor(sqrt(D) n / 2)
+  const int smax = int(std::floor(std::sqrt(double(D)) * (n / 2)));
+  std::vector<double> target(smax + 1);
+  double tot = 0;
+  for (int s_ = 0; s_ <= smax; ++s_) {
+    const double k = s_;
+    target[s_] = k * k * k * k * std::exp(-2.0 * (k / kpeak) * (k / kpeak));
+    tot += target[s_];
+  }
+  for (double& v : target) v = tot > 0 ? totalenergy * v / tot : 0.0;
+  const size_t cb = p->csz * 16;  // one FP64 compact component
+  void* w[3] = {nullptr, nullptr, nullptr};
+  double* dbuf = nullptr;  // [eshell (smax + 1) | target (smax + 1)]
+  auto release = [&]() {
+    for (int c = 0; c < 3; ++c)
+      if (w[c]) cudaFreeAsync(w[c], st);
+    if (dbuf) cudaFreeAsync(dbuf, st);
+  };
+  for (int c = 0; c < D; ++c)
+    if (cudaMallocAsync(&w[c], cb, st) != cudaSuccess) { cudaGetLastError(); release(); return fail(SC_ERR_OOM, "randomfield scratch"); }
+  if (cudaMallocAsync((void**)&dbuf, 2 * (smax + 1) * sizeof(double), st) != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return fail(SC_ERR_OOM, "randomfield scratch");
+  }
+  cudaError_t e = cudaMemsetAsync(dbuf, 0, (smax + 1) * sizeof(double), st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dbuf + smax + 1, target.data(), (smax + 1) * sizeof(double), cudaMemcpyHostToDevice, st);
+  for (int c = 0; c < D && e == cudaSuccess; ++c)
+    if (draws) e = cudaMemcpyAsync(w[c], draws[c], cb, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) { release(); return fail(SC_ERR_CUDA, "randomfield: %s", cudaGetErrorString(e)); }
+  if (!draws) sc::launch_random_draws(w, D, p->K1, p->kc, seed, st);
+  if (p->dtype == SC_FLOAT64)
+    sc::launch_random_finish<double>(w, p->U, D, n, p->K1, p->kc, dbuf, dbuf + smax + 1, st);
+  else
+    sc::launch_random_finish<float>(w, p->U, D, n, p->K1, p->kc, dbuf, dbuf + smax + 1, st);
+  rc = check_launch("randomfield");
+  if (!rc && u_hat) rc = SC_DTYPE_DISPATCH(p, unpack_state, p, p->U, u_hat, st);
+  release();
+  e = cudaStreamSynchronize(st);  // the host target array is read by the copy above
+  if (!rc && e != cudaSuccess) rc = fail(SC_ERR_CUDA, "randomfield: %s", cudaGetErrorString(e));
+  return rc;
+}
+
 int sc_les_batch_set_snapshots(sc_les_batch* b, int every, int nshell, int max_snap) {
   if (!b || every < 0 || (every > 0 && (nshell < 1 || max_snap < 1))) return fail(SC_ERR_INVALID, "bad argument");
   for (const sc_les_instance& in : b->inst)

@@ -132,6 +132,14 @@ bool fast_supported(int N);
 bool init_fast(int N);
 bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t st);
 bool launch_xsweep2(int N, const XArgs& a, const void* tw, cudaStream_t st);
+// randomfield on the device (sc_random.cu): counter-based N(0, 1/2) draws into
+// the FP64 compact work arrays w, then symmetrize!, project!, twothirds! and
+// the per-shell rescale to target[s] (eshell: smax + 1 zeroed doubles) into
+// the compact arrays out of the plan's precision
+void launch_random_draws(void* const* w, int D, int K1, int kc, unsigned long long seed, cudaStream_t st);
+template <typename R>
+void launch_random_finish(void* const* w, void* const* out, int D, int n, int K1, int kc, double* eshell,
+                          const double* target, cudaStream_t st);
 // number of autotuner variants of the FP32 column sweeps / 3D x sweep of size N
 int col2_variants(int N);
 int xsweep_variants(int N, int D);

@@ -581,6 +581,19 @@ class LesBatch:
             pass
 
 
+def random_field(g: Grid, seed=0, kpeak=4.0, totalenergy=1.0, draws=None, out=None, stream=None):
+    """``randomfield(peak_profile, g; kpeak, totalenergy)`` (src/solver.jl:576-641) on
+    the device (``sc_random_field``).  The field becomes the plan's state; it is
+    also returned in the full layout (``out`` or new tensors).  ``draws``:
+    complex128 device tensors of the normal coefficients on the compact 2/3
+    cube (``fields.compact_shape``), or None for the device generator (seed)."""
+    out = vectorfield(g) if out is None else out
+    pd, _k1 = ptr_array([c.data_ptr() for c in draws]) if draws is not None else (None, None)
+    po, _k2 = ptr_array([g._check_spec(c) for c in out])
+    check(lib().sc_random_field(g.plan, int(seed), pd, float(kpeak), float(totalenergy), po, _stream_ptr(stream)))
+    return out
+
+
 def set_option(g: Grid, option, value):
     """``sc_plan_set_option``: ``SC_OPT_USE_GRAPH`` (1) replays captured CUDA
     graphs in the steppers (default) or launches eagerly (0);

@@ -92,6 +92,7 @@ _SIGS = {
     "sc_les_batch_run": ([_vp, ct.c_int, _vp], ct.c_int),
     "sc_les_batch_status": ([_vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), ct.c_int, _vp], ct.c_int),
     "sc_les_batch_set_snapshots": ([_vp, ct.c_int, ct.c_int, ct.c_int], ct.c_int),
+    "sc_random_field": ([_vp, ct.c_ulonglong, _pp, ct.c_double, ct.c_double, _pp, _vp], ct.c_int),
     "sc_les_batch_snapshots": ([_vp, ct.POINTER(ct.c_int), ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_les_batch_destroy": ([_vp], ct.c_int),
     "sc_plan_set_option": ([_vp, ct.c_int, ct.c_longlong], ct.c_int),
