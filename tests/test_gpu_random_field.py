@@ -52,7 +52,9 @@ def test_device_generator_field_has_the_reference_properties(D, n):
     g, go = S.Grid(D, n, dtype=torch.float64, device="cuda:0"), O.Grid(D, n)
     u = [to_np(c) for c in S.random_field(g, seed=11, kpeak=3.0, totalenergy=0.2)]
     u2 = [to_np(c) for c in S.random_field(g, seed=11, kpeak=3.0, totalenergy=0.2)]
-    assert all(np.array_equal(a, b) for a, b in zip(u, u2))  # deterministic per seed
+    # deterministic per seed (the draws are; the shell sums are FP64 atomics, so
+    # the rescale may differ in the last bit)
+    assert O.rel_l2(u2, u) < 1e-14
     u3 = [to_np(c) for c in S.random_field(g, seed=12, kpeak=3.0, totalenergy=0.2)]
     assert O.rel_l2(u3, u) > 0.5  # another seed, another field
     assert np.abs(O.vectordivergence(u, go)).max() < 1e-12
