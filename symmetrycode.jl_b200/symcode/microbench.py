@@ -10,6 +10,10 @@ Prints one JSON line with ms per launch, algorithmic bytes and GB/s.  Used to
 make small, self-contained cases of the exact kernels the solver runs (for
 ncu) and to compare tile shapes.
 
+``--kernel sfs`` runs sfs! from an n^3 FP32 field to ``--n-les`` at three filter
+widths; ``--kernel clark`` / ``dynsmag`` evaluate that closure's ``model(u, G)``
+at n^3 (FP32).
+
 ``--kernel cnn`` evaluates the tensor-core CNN closure (n = 128, FP32) COUNT
 times on a seeded random field and reports ms per evaluation and the
 convolutions' TFLOP/s (2 x 27 x sum(C_in C_out) flops per grid point).
@@ -54,6 +58,64 @@ def run_cnn(n, count, reps=5):
             "tflops": flops / (best / 1e3) / 1e12}
 
 
+def run_sfs(n, nl, count, reps=3):
+    """sfs! of a seeded n^3 FP32 field to nl^3 at Delta/h in {2, 4, 8}, COUNT calls."""
+    import torch
+
+    from . import Grid, random_field, scalarfield, sfs_
+
+    g = Grid(3, n, dtype=torch.float32, device="cuda:0")
+    gl = Grid(3, nl, dtype=torch.float32, device="cuda:0")
+    u = random_field(g, seed=2, kpeak=4.0)
+    deltas = [dh * gl.l / nl for dh in (2, 4, 8)]
+    ub = [[scalarfield(gl) for _ in range(3)] for _ in deltas]
+    ta = [[scalarfield(gl) for _ in range(6)] for _ in deltas]
+    sfs_(ub, ta, u, g, gl, deltas)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(count):
+            sfs_(ub, ta, u, g, gl, deltas)
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / count
+        best = t if best is None else min(best, t)
+    return {"kernel": "sfs", "n": n, "n_les": nl, "count": count, "ms": best}
+
+
+def run_closure(kind, n, count, reps=3):
+    """One classical closure's tau = model(u, G) on a seeded n^3 FP32 field, COUNT evaluations."""
+    import torch
+
+    from . import Grid, create_clark, create_dynamic_smagorinsky, random_field, spacescalarfield, to_phys_
+
+    g = Grid(3, n, dtype=torch.float32, device="cuda:0")
+    u = random_field(g, seed=3, kpeak=4.0)
+    delta = 2 * g.l / n
+    cl = create_clark(delta, g) if kind == "clark" else create_dynamic_smagorinsky(delta, g)
+    # physical velocity gradient G[a + 3 b] = to_phys(i k_b u_a), the les! input of model(u, G)
+    f = torch.fft.fftfreq(n, 1.0 / n, device=g.device).to(torch.float32)
+    ks = (torch.arange(n // 2 + 1, device=g.device, dtype=torch.float32)[None, None, :], f[None, :, None],
+          f[:, None, None])
+    G = [to_phys_(spacescalarfield(g), (1j * ks[b] * u[a]).contiguous(), g) for b in range(3) for a in range(3)]
+    cl(u, G)
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(count):
+            cl(u, G)
+        e1.record()
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / count
+        best = t if best is None else min(best, t)
+    cl.close()
+    return {"kernel": kind, "n": n, "count": count, "ms": best}
+
+
 def run(kernel, n, count, dtype="f32", reps=5, variant=0):
     ms, by = ct.c_double(), ct.c_double()
     code = KERNELS[kernel] | (int(variant) << 8)  # the sweep's autotuner variant in bits 8..
@@ -64,7 +126,8 @@ def run(kernel, n, count, dtype="f32", reps=5, variant=0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", choices=sorted(KERNELS) + ["cnn"], required=True)
+    ap.add_argument("--kernel", choices=sorted(KERNELS) + ["cnn", "sfs", "clark", "dynsmag"], required=True)
+    ap.add_argument("--n-les", type=int, default=128)
     ap.add_argument("--n", type=int, default=810)
     ap.add_argument("--count", type=int, required=True)
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
@@ -73,6 +136,10 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.kernel == "cnn":
         print(json.dumps(run_cnn(a.n, a.count, a.reps)))
+    elif a.kernel == "sfs":
+        print(json.dumps(run_sfs(a.n, a.n_les, a.count, a.reps)))
+    elif a.kernel in ("clark", "dynsmag"):
+        print(json.dumps(run_closure(a.kernel, a.n, a.count, a.reps)))
     else:
         print(json.dumps(run(a.kernel, a.n, a.count, a.dtype, a.reps, a.variant)))
     return 0
