@@ -840,6 +840,173 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
 }
 
 // ---------------------------------------------------------------------------
+// plain x transforms (to_phys! / to_spec! along x, the closures' and les!'s
+// batches of fields): two-level register FFT per pencil, a pencil being one
+// row of two components packed as a + i b
+// ---------------------------------------------------------------------------
+template <int N> struct XPF;
+template <> struct XPF<810> { static constexpr int TP = 8; };
+template <> struct XPF<256> { static constexpr int TP = 16; };
+template <> struct XPF<128> { static constexpr int TP = 32; };
+template <> struct XPF<64> { static constexpr int TP = 32; };
+
+template <int N> struct XPFCfg {
+  static constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, N2P = N2 + 1;
+  static constexpr int TP = XPF<N>::TP, NT = 256;
+  static constexpr int KMAX = N / 2 + 1;  // widest spectral row (full RFFT layout)
+  static constexpr size_t RIN = size_t(TP) * 2 * KMAX * sizeof(float2);    // c2r: staged rows; r2c: Z rows
+  static constexpr size_t YB = size_t(TP) * N1 * N2P * sizeof(float2);
+  static constexpr size_t SMEM = RIN + YB;
+};
+
+// Hermitian extension of one real row's half spectrum (K1 modes), the imaginary
+// parts of the mean and of the Nyquist mode dropped (a real row's c2r ignores them)
+template <int N> __device__ __forceinline__ float2 hext3(const float2* row, int K1, int f) {
+  const int kmax = K1 - 1;
+  if (f == 0) return make_float2(row[0].x, 0.f);
+  if (f <= kmax) {
+    float2 v = row[f];
+    if (2 * f == N) v.y = 0.f;
+    return v;
+  }
+  if (f >= N - kmax) { const float2 v = row[N - f]; return make_float2(v.x, -v.y); }
+  return make_float2(0.f, 0.f);
+}
+
+template <int N>
+__global__ void __launch_bounds__(XPFCfg<N>::NT) k_xc2r_fast(const XPlainArgs a, const float2* __restrict__ tw) {
+  using Cfg = XPFCfg<N>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, N2P = Cfg::N2P, TP = Cfg::TP, NT = Cfg::NT, KMAX = Cfg::KMAX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* rin = reinterpret_cast<float2*>(smem_raw);              // [TP][2][KMAX]
+  float2* yb = reinterpret_cast<float2*>(smem_raw + Cfg::RIN);    // [TP][N1][N2P]
+  const int npair = (a.ncomp + 1) / 2, K1 = a.K1;
+  const long long npen = a.nrows * npair, pen0 = (long long)blockIdx.x * TP;
+  for (int idx = threadIdx.x; idx < TP * 2 * K1; idx += NT) {
+    const int p = idx / (2 * K1), rem = idx - p * 2 * K1, h = rem / K1, kx = rem - h * K1;
+    const long long pen = pen0 + p;
+    float2 v = make_float2(0.f, 0.f);
+    if (pen < npen) {
+      const long long row = pen / npair;
+      const int q = 2 * int(pen % npair) + h;
+      if (q < a.ncomp) v = __ldg(static_cast<const float2*>(a.in[q]) + row * K1 + kx);
+    }
+    rin[(p * 2 + h) * KMAX + kx] = v;
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < TP * N2; it += NT) {
+    const int p = it / N2, j = it - p * N2;
+    const float2* ra = rin + (p * 2) * KMAX;
+    const float2* rb = ra + KMAX;
+    float2 v[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int f = N2 * n1 + j;
+      const float2 x = hext3<N>(ra, K1, f), y = hext3<N>(rb, K1, f);
+      v[n1] = make_float2(x.x - y.y, x.y + y.x);
+    }
+    DFT<N1, true, float2>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+      const float2 w = __ldg(&tw[j * k1]);
+      v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
+    }
+    float2* yp = yb + p * N1 * N2P;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+  }
+  __syncthreads();
+  const float sc = float(a.scale);
+  for (int it = threadIdx.x; it < TP * N1; it += NT) {
+    const int p = it / N1, i = it - p * N1;
+    const long long pen = pen0 + p;
+    if (pen >= npen) continue;
+    float2 w[N2];
+    const float2* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+    DFT<N2, true, float2>::run(w);
+    const long long row = pen / npair;
+    const int pr = int(pen % npair);
+    float* oa = static_cast<float*>(a.out[2 * pr]) + row * N + i;
+    float* ob = 2 * pr + 1 < a.ncomp ? static_cast<float*>(a.out[2 * pr + 1]) + row * N + i : nullptr;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      oa[N1 * k2] = w[k2].x * sc;
+      if (ob) ob[N1 * k2] = w[k2].y * sc;
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(XPFCfg<N>::NT) k_xr2c_fast(const XPlainArgs a, const float2* __restrict__ tw) {
+  using Cfg = XPFCfg<N>;
+  constexpr int N1 = Cfg::N1, N2 = Cfg::N2, N2P = Cfg::N2P, TP = Cfg::TP, NT = Cfg::NT, KMAX = Cfg::KMAX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* zb = reinterpret_cast<float2*>(smem_raw);               // [TP][2 KMAX]: kept outputs
+  float2* yb = reinterpret_cast<float2*>(smem_raw + Cfg::RIN);    // [TP][N1][N2P]
+  const int npair = (a.ncomp + 1) / 2, K1 = a.K1, ko = K1 - 1;
+  const long long npen = a.nrows * npair, pen0 = (long long)blockIdx.x * TP;
+  const float sc = float(a.scale);
+  for (int it = threadIdx.x; it < TP * N2; it += NT) {
+    const int p = it / N2, j = it - p * N2;
+    const long long pen = pen0 + p;
+    float2 v[N1];
+    const float* ia = nullptr;
+    const float* ib = nullptr;
+    if (pen < npen) {
+      const long long row = pen / npair;
+      const int pr = int(pen % npair);
+      ia = static_cast<const float*>(a.in[2 * pr]) + row * N;
+      if (2 * pr + 1 < a.ncomp) ib = static_cast<const float*>(a.in[2 * pr + 1]) + row * N;
+    }
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) {
+      const int x = N2 * n1 + j;
+      v[n1] = make_float2(ia ? __ldg(ia + x) * sc : 0.f, ib ? __ldg(ib + x) * sc : 0.f);
+    }
+    DFT<N1, false, float2>::run(v);
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], __ldg(&tw[j * k1]));
+    float2* yp = yb + p * N1 * N2P;
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) yp[k1 * N2P + j] = v[k1];
+  }
+  __syncthreads();
+  for (int it = threadIdx.x; it < TP * N1; it += NT) {
+    const int p = it / N1, i = it - p * N1;
+    float2 w[N2];
+    const float2* yp = yb + p * N1 * N2P + i * N2P;
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
+    DFT<N2, false, float2>::run(w);
+    float2* zp = zb + p * 2 * KMAX;
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) {
+      const int k = i + N1 * k2;
+      if (k <= ko) zp[k] = w[k2];
+      else if (k >= N - ko) zp[ko + (N - k)] = w[k2];
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TP * K1; idx += NT) {
+    const int p = idx / K1, kx = idx - p * K1;
+    const long long pen = pen0 + p;
+    if (pen >= npen) continue;
+    const long long row = pen / npair;
+    const int pr = int(pen % npair);
+    const float2* zp = zb + p * 2 * KMAX;
+    // X[k] = (Z[k] + conj Z[-k]) / 2, Y[k] = (Z[k] - conj Z[-k]) / 2i; Z[-0] = Z[0],
+    // and Z[-N/2] = Z[N/2] at the Nyquist mode of a full-layout row
+    const int kc = kx == 0 ? 0 : (2 * kx == N ? kx : ko + kx);
+    const float2 z = zp[kx], zc = zp[kc];
+    static_cast<float2*>(a.out[2 * pr])[row * K1 + kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+    if (2 * pr + 1 < a.ncomp)
+      static_cast<float2*>(a.out[2 * pr + 1])[row * K1 + kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // dispatch
 // ---------------------------------------------------------------------------
 template <typename F> static void set_smem2(F* f, size_t bytes) {
@@ -882,6 +1049,8 @@ template <int N, int V = 0> static void init_col2_variants() {
   }
 }
 
+template <int N> static void init_xplain();
+
 template <int N> static void init_fast_n() {
   constexpr int T = ColVariants<N>::T[0];
   set_smem2(k_col2<N, T, true, true, false>, Col2Cfg<N, T>::SMEM);
@@ -891,9 +1060,35 @@ template <int N> static void init_fast_n() {
   set_smem2(k_xsweep2<N, 3>, X2Cfg<N, 3>::SMEM);
   set_smem2(k_xsweep3<N>, X3Cfg<N>::SMEM);
   if (N == 810) set_smem2(k_xsweep4<true>, X4Cfg::SMEM), set_smem2(k_xsweep4<false>, X4Cfg::SMEM);
+  init_xplain<N>();
 }
 
 bool fast_supported(int N) { return N == 810 || N == 256 || N == 128 || N == 64; }
+
+template <int N> static void init_xplain() {
+  set_smem2(k_xc2r_fast<N>, XPFCfg<N>::SMEM);
+  set_smem2(k_xr2c_fast<N>, XPFCfg<N>::SMEM);
+}
+
+template <int N> static void xplain_n(bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st) {
+  using Cfg = XPFCfg<N>;
+  const long long npen = a.nrows * ((a.ncomp + 1) / 2);
+  const unsigned nb = unsigned((npen + Cfg::TP - 1) / Cfg::TP);
+  const float2* t2 = static_cast<const float2*>(tw);
+  if (inv) k_xc2r_fast<N><<<nb, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+  else k_xr2c_fast<N><<<nb, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
+}
+
+bool launch_xplain_fast(int N, bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st) {
+  if (a.K1 > N / 2 + 1 || a.K1 < 1) return false;
+  switch (N) {
+    case 810: xplain_n<810>(inv, a, tw, st); return true;
+    case 256: xplain_n<256>(inv, a, tw, st); return true;
+    case 128: xplain_n<128>(inv, a, tw, st); return true;
+    case 64: xplain_n<64>(inv, a, tw, st); return true;
+    default: return false;
+  }
+}
 
 bool init_fast(int N) {
   switch (N) {

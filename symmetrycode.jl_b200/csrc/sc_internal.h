@@ -140,6 +140,8 @@ void launch_random_draws(void* const* w, int D, int K1, int kc, unsigned long lo
 template <typename R>
 void launch_random_finish(void* const* w, void* const* out, int D, int n, int K1, int kc, double* eshell,
                           const double* target, cudaStream_t st);
+// FP32 plain c2r (inv) / r2c along x for the fast sizes (sc_fast.cu); false when not applicable
+bool launch_xplain_fast(int N, bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st);
 // number of autotuner variants of the FP32 column sweeps / 3D x sweep of size N
 int col2_variants(int N);
 int xsweep_variants(int N, int D);

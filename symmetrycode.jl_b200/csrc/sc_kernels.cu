@@ -856,6 +856,7 @@ template <typename R> bool launch_xsweep_ns(int N, const XArgs& a, const void* t
   }
 }
 template <typename R> bool launch_x_c2r(int N, const XPlainArgs& a, const void* tw, cudaStream_t st) {
+  if (use_fast<R>(N) && launch_xplain_fast(N, true, a, tw, st)) return true;
   switch (N) {
 #define SC_CASE(NN) case NN: return xc2r_n<R, NN>(a, tw, st);
     SC_SIZES(SC_CASE)
@@ -864,6 +865,7 @@ template <typename R> bool launch_x_c2r(int N, const XPlainArgs& a, const void* 
   }
 }
 template <typename R> bool launch_x_r2c(int N, const XPlainArgs& a, const void* tw, cudaStream_t st) {
+  if (use_fast<R>(N) && launch_xplain_fast(N, false, a, tw, st)) return true;
   switch (N) {
 #define SC_CASE(NN) case NN: return xr2c_n<R, NN>(a, tw, st);
     SC_SIZES(SC_CASE)

@@ -72,12 +72,28 @@ __global__ void k_rf_hermitian(double2* u0, double2* u1, double2* u2, int D, int
 }
 
 // project! (k = 0 untouched) then twothirds!'s k = 0, and the shell energies
-// with the RFFT double count of kx > 0 (FP64 atomics)
-__global__ void k_rf_project(double2* u0, double2* u1, double2* u2, int D, int K1, int kc, double* eshell) {
+// with the RFFT double count of kx > 0: each block sums its shells in shared
+// memory, then one FP64 atomic per shell and block
+__device__ void rf_project_mode(double2* u0, double2* u1, double2* u2, int D, int K1, int kc, long long m,
+                                double* ssh);
+
+__global__ void k_rf_project(double2* u0, double2* u1, double2* u2, int D, int K1, int kc, int nshell,
+                             double* eshell) {
+  extern __shared__ double ssh[];
+  for (int i = threadIdx.x; i < nshell; i += blockDim.x) ssh[i] = 0.0;
+  __syncthreads();
   const int K2 = 2 * kc + 1;
   const long long nm = (long long)K1 * K2 * (D == 3 ? K2 : 1);
-  const long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nm) return;
+  for (long long m = (long long)blockIdx.x * blockDim.x + threadIdx.x; m < nm; m += (long long)gridDim.x * blockDim.x)
+    rf_project_mode(u0, u1, u2, D, K1, kc, m, ssh);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nshell; i += blockDim.x)
+    if (ssh[i] != 0.0) atomicAdd(&eshell[i], ssh[i]);
+}
+
+__device__ void rf_project_mode(double2* u0, double2* u1, double2* u2, int D, int K1, int kc, long long m,
+                                double* ssh) {
+  const int K2 = 2 * kc + 1;
   const int ix = int(m % K1);
   const long long r = m / K1;
   const int iy = kwave(int(r % K2), kc), iz = D == 3 ? kwave(int(r / K2), kc) : 0;
@@ -101,7 +117,7 @@ __global__ void k_rf_project(double2* u0, double2* u1, double2* u2, int D, int K
   int s = int(sqrt(double(k2)));
   while ((long long)(s + 1) * (s + 1) <= k2) ++s;
   while ((long long)s * s > k2) --s;
-  atomicAdd(&eshell[s], (ix > 0 ? 2.0 : 1.0) * 0.5 * e);
+  atomicAdd(&ssh[s], (ix > 0 ? 2.0 : 1.0) * 0.5 * e);
 }
 
 // rescale shell s by sqrt(target_s / E_s) and write the plan's precision
@@ -151,7 +167,13 @@ void launch_random_finish(void* const* w, void* const* out, int D, int n, int K1
                    static_cast<double2*>(D == 3 ? w[2] : w[1])};
   R* o[3] = {static_cast<R*>(out[0]), static_cast<R*>(out[1]), static_cast<R*>(D == 3 ? out[2] : out[1])};
   k_rf_hermitian<<<nb(D == 3 ? (long long)K2 * K2 : K2), 256, 0, st>>>(u[0], u[1], u[2], D, n, K1, kc);
-  k_rf_project<<<nb(nm), 256, 0, st>>>(u[0], u[1], u[2], D, K1, kc, eshell);
+  // shells 0 .. floor(sqrt(D) kc) hold the cube's modes
+  const int smax = int(floor(sqrt(double(D)) * (n / 2)));  // the caller's eshell has smax + 1 entries
+  int nshell = int(sqrt(double(D)) * kc) + 2;
+  if (nshell > smax + 1) nshell = smax + 1;
+  long long nbp = nb(nm);
+  if (nbp > 148 * 8) nbp = 148 * 8;
+  k_rf_project<<<unsigned(nbp), 256, nshell * sizeof(double), st>>>(u[0], u[1], u[2], D, K1, kc, nshell, eshell);
   k_rf_scale<R><<<nb(nm), 256, 0, st>>>(u[0], u[1], u[2], o[0], o[1], o[2], D, K1, kc, eshell, target);
 }
 
