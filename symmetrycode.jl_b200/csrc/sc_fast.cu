@@ -880,18 +880,20 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xc2r_fast(const XPlainArgs a,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* rin = reinterpret_cast<float2*>(smem_raw);              // [TP][2][KMAX]
   float2* yb = reinterpret_cast<float2*>(smem_raw + Cfg::RIN);    // [TP][N1][N2P]
+  // pencil, row and element indices stay 32-bit (at most 810^2 rows x 406
+  // modes per component); one warp stages one row, so no per-element division
   const int npair = (a.ncomp + 1) / 2, K1 = a.K1;
-  const long long npen = a.nrows * npair, pen0 = (long long)blockIdx.x * TP;
-  for (int idx = threadIdx.x; idx < TP * 2 * K1; idx += NT) {
-    const int p = idx / (2 * K1), rem = idx - p * 2 * K1, h = rem / K1, kx = rem - h * K1;
-    const long long pen = pen0 + p;
-    float2 v = make_float2(0.f, 0.f);
+  const int npen = int(a.nrows) * npair, pen0 = blockIdx.x * TP;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int s = warp; s < 2 * TP; s += NT / 32) {
+    const int pen = pen0 + (s >> 1);
+    const float2* src = nullptr;
     if (pen < npen) {
-      const long long row = pen / npair;
-      const int q = 2 * int(pen % npair) + h;
-      if (q < a.ncomp) v = __ldg(static_cast<const float2*>(a.in[q]) + row * K1 + kx);
+      const int row = pen / npair, q = 2 * (pen - row * npair) + (s & 1);
+      if (q < a.ncomp) src = static_cast<const float2*>(a.in[q]) + row * K1;
     }
-    rin[(p * 2 + h) * KMAX + kx] = v;
+    float2* dst = rin + s * KMAX;
+    for (int kx = lane; kx < K1; kx += 32) dst[kx] = src ? __ldg(src + kx) : make_float2(0.f, 0.f);
   }
   __syncthreads();
   for (int it = threadIdx.x; it < TP * N2; it += NT) {
@@ -919,15 +921,15 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xc2r_fast(const XPlainArgs a,
   const float sc = float(a.scale);
   for (int it = threadIdx.x; it < TP * N1; it += NT) {
     const int p = it / N1, i = it - p * N1;
-    const long long pen = pen0 + p;
+    const int pen = pen0 + p;
     if (pen >= npen) continue;
     float2 w[N2];
     const float2* yp = yb + p * N1 * N2P + i * N2P;
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) w[n2] = yp[n2];
     DFT<N2, true, float2>::run(w);
-    const long long row = pen / npair;
-    const int pr = int(pen % npair);
+    const int row = pen / npair;
+    const int pr = pen - row * npair;
     float* oa = static_cast<float*>(a.out[2 * pr]) + row * N + i;
     float* ob = 2 * pr + 1 < a.ncomp ? static_cast<float*>(a.out[2 * pr + 1]) + row * N + i : nullptr;
 #pragma unroll
@@ -946,17 +948,17 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xr2c_fast(const XPlainArgs a,
   float2* zb = reinterpret_cast<float2*>(smem_raw);               // [TP][2 KMAX]: kept outputs
   float2* yb = reinterpret_cast<float2*>(smem_raw + Cfg::RIN);    // [TP][N1][N2P]
   const int npair = (a.ncomp + 1) / 2, K1 = a.K1, ko = K1 - 1;
-  const long long npen = a.nrows * npair, pen0 = (long long)blockIdx.x * TP;
+  const int npen = int(a.nrows) * npair, pen0 = blockIdx.x * TP;  // 32-bit, as in k_xc2r_fast
   const float sc = float(a.scale);
   for (int it = threadIdx.x; it < TP * N2; it += NT) {
     const int p = it / N2, j = it - p * N2;
-    const long long pen = pen0 + p;
+    const int pen = pen0 + p;
     float2 v[N1];
     const float* ia = nullptr;
     const float* ib = nullptr;
     if (pen < npen) {
-      const long long row = pen / npair;
-      const int pr = int(pen % npair);
+      const int row = pen / npair;
+      const int pr = pen - row * npair;
       ia = static_cast<const float*>(a.in[2 * pr]) + row * N;
       if (2 * pr + 1 < a.ncomp) ib = static_cast<const float*>(a.in[2 * pr + 1]) + row * N;
     }
@@ -989,20 +991,23 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xr2c_fast(const XPlainArgs a,
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < TP * K1; idx += NT) {
-    const int p = idx / K1, kx = idx - p * K1;
-    const long long pen = pen0 + p;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int p = warp; p < TP; p += NT / 32) {
+    const int pen = pen0 + p;
     if (pen >= npen) continue;
-    const long long row = pen / npair;
-    const int pr = int(pen % npair);
+    const int row = pen / npair;
+    const int pr = pen - row * npair;
     const float2* zp = zb + p * 2 * KMAX;
-    // X[k] = (Z[k] + conj Z[-k]) / 2, Y[k] = (Z[k] - conj Z[-k]) / 2i; Z[-0] = Z[0],
-    // and Z[-N/2] = Z[N/2] at the Nyquist mode of a full-layout row
-    const int kc = kx == 0 ? 0 : (2 * kx == N ? kx : ko + kx);
-    const float2 z = zp[kx], zc = zp[kc];
-    static_cast<float2*>(a.out[2 * pr])[row * K1 + kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-    if (2 * pr + 1 < a.ncomp)
-      static_cast<float2*>(a.out[2 * pr + 1])[row * K1 + kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+    float2* oa = static_cast<float2*>(a.out[2 * pr]) + row * K1;
+    float2* ob = 2 * pr + 1 < a.ncomp ? static_cast<float2*>(a.out[2 * pr + 1]) + row * K1 : nullptr;
+    for (int kx = lane; kx < K1; kx += 32) {
+      // X[k] = (Z[k] + conj Z[-k]) / 2, Y[k] = (Z[k] - conj Z[-k]) / 2i; Z[-0] = Z[0],
+      // and Z[-N/2] = Z[N/2] at the Nyquist mode of a full-layout row
+      const int kc = kx == 0 ? 0 : (2 * kx == N ? kx : ko + kx);
+      const float2 z = zp[kx], zc = zp[kc];
+      oa[kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+      if (ob) ob[kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+    }
   }
 }
 
@@ -1081,6 +1086,7 @@ template <int N> static void xplain_n(bool inv, const XPlainArgs& a, const void*
 
 bool launch_xplain_fast(int N, bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st) {
   if (a.K1 > N / 2 + 1 || a.K1 < 1) return false;
+  if (a.nrows * N >= (1ll << 31)) return false;  // the kernels index rows and elements in 32 bits
   switch (N) {
     case 810: xplain_n<810>(inv, a, tw, st); return true;
     case 256: xplain_n<256>(inv, a, tw, st); return true;
