@@ -292,21 +292,25 @@ SC_API int sc_les_batch_snapshots(sc_les_batch* batch, int* nsnap, double* out, 
 
 /* ---- plan options ---------------------------------------------------------------- */
 #define SC_OPT_USE_GRAPH 1 /* 1 (default): steppers replay a captured CUDA graph; 0: launch eagerly */
-/* Bound of the device-side waits of the plan's tensor-core CNN closures (polls
- * of an mbarrier before a wait gives up, sets the closure's error flag --
+/* Bound of the device-side waits of the plan's tensor-core CNN closures and
+ * of its TMA-fed column sweeps (polls of an mbarrier before a wait gives up).
+ * A CNN kernel whose wait runs out sets the closure's error flag --
  * sc_closure_status then reports SC_ERR_TIMEOUT -- frees its tensor memory and
- * returns).  A negative value restores the default (2^26 polls); 0 makes
+ * returns; a column sweep sets the plan's error word (sc_plan_status) and
+ * returns.  A negative value restores the default (2^26 polls); 0 makes
  * every such wait give up at once, which lets a test exercise the timeout path
  * without hanging or faulting anything; the kernels' last wait for work still
- * in flight before they free tensor memory always keeps the default bound.
- * Takes effect at the next evaluation (not in step graphs captured before the
- * change). */
+ * in flight (tensor-core MMAs, bulk copies into shared memory) always keeps
+ * the default bound.  Takes effect at the next evaluation (not in step graphs
+ * captured before the change). */
 #define SC_OPT_WAIT_LIMIT 2
 /* Kernel variant of one sweep of the 3D product pipeline of an FP32 plan
  * (value 0 .. sc_plan_num_variants - 1; 0 is the default): the candidates of
  * the autotuner (symcode.autotune), which times every variant of every sweep
  * on the plan's own buffers and keeps the fastest.  The variants are the same
- * transforms by other tile widths, splits N = N1 N2 or x-sweep kernels; the
+ * transforms by other tile widths, splits N = N1 N2 or x-sweep kernels, and at
+ * n = 810 persistent column sweeps fed by tensor-memory-access bulk copies
+ * (variants 4-6 of the y-inverse, y-forward and z-forward sweeps); the
  * steppers' cached graphs are rebuilt after a change.  No reference
  * counterpart (the reference's plan choice is cuFFT/FFTW planning,
  * src/solver.jl:432). */
@@ -320,6 +324,10 @@ SC_API int sc_plan_set_option(sc_plan* plan, int option, long long value);
  * z-forward) for this plan (1 where there is no choice: FP64 plans, 2D, sizes
  * without the FP32 two-level engine). */
 SC_API int sc_plan_num_variants(const sc_plan* plan, int sweep, int* count);
+/* Synchronous: SC_ERR_TIMEOUT in *status if a bounded wait of the plan's
+ * TMA-fed column sweeps ran out since the last call (their outputs are then
+ * invalid), else SC_OK; reading clears the record. */
+SC_API int sc_plan_status(sc_plan* plan, int* status);
 
 /* ---- a-posteriori training: rollout, loss and hand-written adjoint ----------
  * New (the reference trains a-priori only, src/training.jl:3-109).  A rollout

@@ -70,6 +70,7 @@ struct sc_plan {
   void* cc[3] = {};
   void* dd[6] = {};
   double* dscal = nullptr;  // [0] forcing A, [1] reduction accumulator
+  int* err = nullptr;       // device word set when a bounded wait of a TMA-fed sweep ran out
   void* fa = nullptr, *fb = nullptr;  // full-spectrum scratch (lazy)
   std::vector<void*> allocs;
   cudaStream_t cap = nullptr;
@@ -215,39 +216,47 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 // intermediate, each z sweep has one such page-spread side instead of two and
 // each y sweep gets one: at 810^3 the four sweeps of one right-hand side take
 // about 8.1 ms instead of 9.0 ms with a [z][ky][kx] intermediate.
+// `ld` (default K1): row length of the intermediates' x axis.  The product
+// pipeline pads it to an even count (272 at 810^3) so that every row of the
+// intermediates it feeds to the TMA-fed sweeps starts on a 16-byte boundary.
 // Inverse z: compact cube (K1 x K2 x K2) -> intermediate, k = 0 masked.
-sc::ColArgs z_inverse_args(int K1, int K2, int n, int kc) {
+sc::ColArgs z_inverse_args(int K1, int K2, int n, int kc, int ldo = 0) {
   sc::ColArgs a{};
+  const long long lo = ldo > 0 ? ldo : K1;
   a.K1 = K1; a.ncols = K2;
-  a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = (long long)K1 * n; a.out_es = K1;
+  a.in_cs = K1; a.in_es = (long long)K1 * K2; a.out_cs = lo * n; a.out_es = lo;
   a.kpos = kc + 1; a.kneg = kc; a.zero_origin = 1;
   return a;
 }
-// Inverse y: intermediate -> physical-(y, z) rows [z][y][kx].
-sc::ColArgs y_inverse_args(int K1, int n, int kc) {
+// Inverse y: intermediate -> physical-(y, z) rows [z][y][kx] (row length K1).
+sc::ColArgs y_inverse_args(int K1, int n, int kc, int ldi = 0) {
   sc::ColArgs b{};
+  const long long li = ldi > 0 ? ldi : K1;
   b.K1 = K1; b.ncols = n;
-  b.in_cs = K1; b.in_es = (long long)K1 * n; b.out_cs = (long long)K1 * n; b.out_es = K1;
+  b.in_cs = li; b.in_es = li * n; b.out_cs = (long long)K1 * n; b.out_es = K1;
   b.kpos = kc + 1; b.kneg = kc;
   return b;
 }
 // Forward y: rows [z][y][kx] (x extent K1) -> intermediate (ky pruned to 2 kout + 1).
-sc::ColArgs y_forward_args(int K1, int n, int kout) {
+sc::ColArgs y_forward_args(int K1, int n, int kout, int ld = 0) {
   sc::ColArgs f{};
+  const long long l = ld > 0 ? ld : K1;
   f.K1 = K1; f.ncols = n;
-  f.in_cs = (long long)K1 * n; f.in_es = K1; f.out_cs = K1; f.out_es = (long long)K1 * n;
+  f.in_cs = l * n; f.in_es = l; f.out_cs = l; f.out_es = l * n;
   f.kpos = kout + 1; f.kneg = kout;
   return f;
 }
 // Forward z: intermediate -> compact cube of half-width kout (x extent K1 = kout + 1).
-sc::ColArgs z_forward_args(int K1, int n, int kout) {
+sc::ColArgs z_forward_args(int K1, int n, int kout, int ldi = 0) {
   sc::ColArgs g{};
   const int K2 = 2 * kout + 1;
+  const long long li = ldi > 0 ? ldi : K1;
   g.K1 = K1; g.ncols = K2;
-  g.in_cs = (long long)K1 * n; g.in_es = K1; g.out_cs = K1; g.out_es = (long long)K1 * K2;
+  g.in_cs = li * n; g.in_es = li; g.out_cs = K1; g.out_es = (long long)K1 * K2;
   g.kpos = kout + 1; g.kneg = kout;
   return g;
 }
+int even_up(int k) { return k + (k & 1); }
 
 // ---------------------------------------------------------------------------
 // the five-sweep product pipeline: compact u -> compact F[u_i u_j]/n^D in p->sig
@@ -267,35 +276,40 @@ int products(sc_plan* p, void* const* u, cudaStream_t st, cudaEvent_t* ev = null
   mark();
   sc::ColArgs a{};
   if (p->D == 3) {
-    a = z_inverse_args(K1, K2, n, kc);
+    // intermediates B = z-inverse output, D = x-sweep output, E = y-forward
+    // output have even row lengths (the buffers are allocated for K1 + 1)
+    const int ld = even_up(K1), ldo = even_up(K1o);
+    auto bounded = [&](sc::ColArgs& c, int v) { c.variant = v; c.wait_limit = p->wait_limit; c.err = p->err; };
+    a = z_inverse_args(K1, K2, n, kc, ld);
     for (int c = 0; c < 3; ++c) { a.in[c] = u[c]; a.out[c] = p->be[c]; }
     a.ncomp = 3;
-    a.variant = p->variant[0];
+    bounded(a, p->variant[0]);
     if (!sc::launch_col_inv<R>(n, a, p->tw, st)) return fail(SC_ERR_SIZE, "unsupported n=%d", n);
     mark();
-    sc::ColArgs b = y_inverse_args(K1, n, kc);
+    sc::ColArgs b = y_inverse_args(K1, n, kc, ld);
     for (int c = 0; c < 3; ++c) { b.in[c] = p->be[c]; b.out[c] = p->cc[c]; }
     b.ncomp = 3;
-    b.variant = p->variant[1];
+    bounded(b, p->variant[1]);
     sc::launch_col_inv<R>(n, b, p->tw, st);
     mark();
     sc::XArgs x{};
     for (int c = 0; c < 3; ++c) x.in[c] = p->cc[c];
     for (int c = 0; c < 6; ++c) x.out[c] = p->dd[c];
     x.D = 3; x.K1in = K1; x.K1out = K1o; x.nrows = (long long)n * n; x.scale = 1.0 / ((double)n * n * n);
+    x.ldo = ldo;
     x.variant = p->variant[2];
     sc::launch_xsweep_ns<R>(n, x, p->tw, st);
     mark();
-    sc::ColArgs f = y_forward_args(K1o, n, kout);
+    sc::ColArgs f = y_forward_args(K1o, n, kout, ldo);
     for (int c = 0; c < 6; ++c) { f.in[c] = p->dd[c]; f.out[c] = p->be[c]; }
     f.ncomp = 6;
-    f.variant = p->variant[3];
+    bounded(f, p->variant[3]);
     sc::launch_col_fwd<R>(n, f, p->tw, st);
     mark();
-    sc::ColArgs g = z_forward_args(K1o, n, kout);
+    sc::ColArgs g = z_forward_args(K1o, n, kout, ldo);
     for (int c = 0; c < 6; ++c) { g.in[c] = p->be[c]; g.out[c] = sig[c]; }
     g.ncomp = 6;
-    g.variant = p->variant[4];
+    bounded(g, p->variant[4]);
     sc::launch_col_fwd<R>(n, g, p->tw, st);
     mark();
   } else {
@@ -1017,8 +1031,11 @@ int sc_plan_create(sc_plan** out, int D, int n, double l, int dtype, size_t* wor
   p->esz = dtype == SC_FLOAT64 ? 16 : 8;
   p->csz = (size_t)p->K1 * p->K2 * (D == 3 ? p->K2 : 1);
   p->fsz = (size_t)(n / 2 + 1) * n * (D == 3 ? n : 1);
-  const size_t plane = (size_t)p->K1 * n * (D == 3 ? n : 1);  // (kx, y[, z])
-  const size_t mid = (size_t)p->K1 * p->K2 * n;                // (kx, ky, z)
+  // (kx, y[, z]) and (kx, ky, z) scratch; in 3D the x extent is padded to an
+  // even count for the product pipeline's intermediates
+  const size_t K1x = D == 3 ? (size_t)even_up(p->K1) : (size_t)p->K1;
+  const size_t plane = K1x * n * (D == 3 ? n : 1);
+  const size_t mid = K1x * p->K2 * n;
   int rc = SC_OK;
   bool ok = (dtype == SC_FLOAT64) ? sc::init_kernels<double>(n) : sc::init_kernels<float>(n);
   if (!ok) { rc = fail(SC_ERR_CUDA, "kernel attribute setup failed for n=%d", n); goto bad; }
@@ -1036,13 +1053,18 @@ int sc_plan_create(sc_plan** out, int D, int n, double l, int dtype, size_t* wor
   for (int c = 0; c < D; ++c)
     if ((rc = plan_alloc(p, &p->cc[c], plane * p->esz))) goto bad;
   if ((rc = plan_alloc(p, (void**)&p->dscal, 16 * sizeof(double)))) goto bad;
+  if ((rc = plan_alloc(p, (void**)&p->err, sizeof(int)))) goto bad;
   if (cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking) != cudaSuccess) {
     rc = fail(SC_ERR_CUDA, "stream creation failed");
     goto bad;
   }
   rc = dtype == SC_FLOAT64 ? upload_twiddles<double>(p) : upload_twiddles<float>(p);
   if (rc) goto bad;
-  if (cudaMemset(p->dscal, 0, 16 * sizeof(double)) != cudaSuccess) { rc = fail(SC_ERR_CUDA, "memset"); goto bad; }
+  if (cudaMemset(p->dscal, 0, 16 * sizeof(double)) != cudaSuccess ||
+      cudaMemset(p->err, 0, sizeof(int)) != cudaSuccess) {
+    rc = fail(SC_ERR_CUDA, "memset");
+    goto bad;
+  }
   if (workspace_bytes) *workspace_bytes = p->ws;
   *out = p;
   return SC_OK;
@@ -1216,24 +1238,27 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
   sc::ColArgs ca{};
   sc::XArgs xa{};
   double b = 0;
+  const int ld = even_up(K1);
+  int* err = static_cast<int*>(alloc(1));
   const int nin = kernel == 1 ? 6 : 3, nout = kernel == 0 ? 3 : 6;
   if (kernel == 0 || kernel == 1) {
     // y-inverse (3 comps) / y-forward (6 comps) of the solver over `count` z
     // planes: the (kx, ky, z) side is a full-size intermediate, so its lines
     // keep the solver's strides
+    // (the product pipeline's padded row length on the intermediate side)
     if (count > n) { cleanup(); return fail(SC_ERR_INVALID, "count exceeds the %d z planes", n); }
-    const size_t mid = (size_t)K1 * n * K2, rows = (size_t)K1 * n * count;
-    ca = kernel == 0 ? y_inverse_args(K1, n, kc) : y_forward_args(K1, n, kc);
-    for (int c = 0; c < nin; ++c) ca.in[c] = alloc(kernel == 0 ? mid : rows);
-    for (int c = 0; c < nout; ++c) ca.out[c] = alloc(kernel == 0 ? rows : mid);
+    const size_t mid = (size_t)ld * n * K2;
+    ca = kernel == 0 ? y_inverse_args(K1, n, kc, ld) : y_forward_args(K1, n, kc, ld);
+    for (int c = 0; c < nin; ++c) ca.in[c] = alloc(kernel == 0 ? mid : (size_t)ld * n * count);
+    for (int c = 0; c < nout; ++c) ca.out[c] = alloc(kernel == 0 ? (size_t)K1 * n * count : mid);
     ca.ncomp = nout; ca.ncols = (int)count;
     b = (double)(nin + nout) / 2 * esz * K1 * count * (K2 + n);
   } else if (kernel == 3 || kernel == 4) {
     // z-inverse / z-forward of the solver, one component, over the first
     // `count` ky columns of a full-size cube and intermediate
     if (count > K2) { cleanup(); return fail(SC_ERR_INVALID, "count exceeds the %d ky columns", K2); }
-    const size_t cube = (size_t)K1 * K2 * K2, mid = (size_t)K1 * n * K2;
-    ca = kernel == 3 ? z_inverse_args(K1, K2, n, kc) : z_forward_args(K1, n, kc);
+    const size_t cube = (size_t)K1 * K2 * K2, mid = (size_t)ld * n * K2;
+    ca = kernel == 3 ? z_inverse_args(K1, K2, n, kc, ld) : z_forward_args(K1, n, kc, ld);
     ca.in[0] = alloc(kernel == 3 ? cube : mid);
     ca.out[0] = alloc(kernel == 3 ? mid : cube);
     ca.ncomp = 1; ca.ncols = (int)count;
@@ -1249,6 +1274,9 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
     return fail(SC_ERR_INVALID, "unknown microbench kernel %d", kernel);
   }
   for (void* q : bufs) if (!q) { cleanup(); return fail(SC_ERR_OOM, "microbench allocation failed"); }
+  ca.variant = variant;
+  ca.wait_limit = sc::kDefaultWaitLimit;
+  ca.err = err;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   auto launch = [&]() {
@@ -1265,6 +1293,9 @@ int microbench_impl(int kernel, int n, long long count, int reps, double* ms, do
   cudaEventElapsedTime(&t, e0, e1);
   cudaEventDestroy(e0); cudaEventDestroy(e1);
   int rc = check_launch("microbench");
+  int h = 0;
+  if (!rc && err) cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (!rc && h) rc = fail(SC_ERR_TIMEOUT, "a bounded wait of the TMA-fed sweep ran out");
   cleanup();
   if (rc) return rc;
   *ms = t / reps;
@@ -1659,6 +1690,16 @@ int sc_closure_set_params(sc_closure* cl, const double* theta) {
     }
   }
   // cached step graphs captured the old weights by pointer, which stay valid
+  return SC_OK;
+}
+
+int sc_plan_status(sc_plan* p, int* status) {
+  if (!p || !status) return fail(SC_ERR_INVALID, "null argument");
+  ensure_device(p);
+  int h = 0;
+  SC_CU(cudaMemcpy(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) SC_CU(cudaMemset(p->err, 0, sizeof(int)));
+  *status = h ? SC_ERR_TIMEOUT : SC_OK;
   return SC_OK;
 }
 
@@ -2303,6 +2344,9 @@ int sc_plan_num_variants(const sc_plan* p, int sweep, int* count) {
   if (p->dtype != SC_FLOAT32 || !sc::fast_supported(p->n)) return SC_OK;
   if (p->D != 3) return SC_OK;
   *count = sweep == 2 ? sc::xsweep_variants(p->n, p->D) : sc::col2_variants(p->n);
+  // the z inverse reads the compact cube, whose rows (271 complex at 810^3)
+  // are not 16-byte strided: no TMA-fed variants
+  if (sweep == 0 && p->n == 810) *count -= sc::kColTmaConfigs;
   return SC_OK;
 }
 
@@ -2311,6 +2355,9 @@ int sc_plan_set_option(sc_plan* p, int option, long long value) {
   if (option == SC_OPT_USE_GRAPH) { p->use_graph = value ? 1 : 0; return SC_OK; }
   if (option == SC_OPT_WAIT_LIMIT) {
     p->wait_limit = value < 0 ? sc::kDefaultWaitLimit : value;
+    // the plan's own step graphs carry the bound of their column sweeps
+    if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
+    if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
     return SC_OK;
   }
   if (option >= SC_OPT_VARIANT_ZINV && option <= SC_OPT_VARIANT_ZFWD) {

@@ -31,10 +31,6 @@ template <> struct Split<128, 1> { static constexpr int N1 = 8, N2 = 16; };
 template <> struct Split<64, 0> { static constexpr int N1 = 8, N2 = 8; };
 template <> struct Split<64, 1> { static constexpr int N1 = 8, N2 = 8; };
 
-__device__ __forceinline__ int cpos(int f, int N, int kpos, int kneg) {
-  return f < kpos ? f : (f >= N - kneg ? f - N + kpos + kneg : -1);
-}
-
 // ---------------------------------------------------------------------------
 // column sweeps: tile of T consecutive kx, one column c, all N elements
 // ---------------------------------------------------------------------------
@@ -47,14 +43,6 @@ template <int N, int T, int S = 0> struct Col2Cfg {
   // at 810 the tile of 8 columns keeps 80 registers and three CTAs per SM
   static constexpr int MINB = N == 810 ? (T == 4 ? 6 : (T == 8 ? 3 : 1)) : 1;
 };
-
-// Where a block of B consecutive transform indices e0 .. e0 + B - 1 falls in
-// the compact layout (kpos modes e < kpos kept in place, kneg modes
-// e >= N - kneg moved down by N - kpos - kneg): 0 every index kept in place,
-// 1 every index moved, 2 none kept, 3 the block straddles a boundary.
-constexpr int crange(int e0, int B, int N, int kpos, int kneg) {
-  return e0 + B - 1 < kpos ? 0 : (e0 >= N - kneg ? 1 : (e0 >= kpos && e0 + B - 1 < N - kneg ? 2 : 3));
-}
 
 // DRV: the launch carries derivative outputs (ColArgs::ndrv > 0).  Without it
 // the wavenumber scaling is compiled out; otherwise the compiler hoists the
@@ -342,6 +330,7 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
   // S: split the paired spectra and store the product rows
   constexpr int NBF = NPF / TR;
   const int K1o = a.K1out;
+  const long long ldo = a.ldo > 0 ? a.ldo : K1o;
   for (int it = threadIdx.x; it < TR * K1o; it += NT) {
     const int r = it / K1o, kx = it % K1o;
     const long long row = row0 + r;
@@ -352,8 +341,8 @@ k_xsweep2(const XArgs a, const float2* __restrict__ tw) {
       const C z = zp[kx], zc = zp[kx == 0 ? 0 : ko + kx];
       const C xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
       const C xbv = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
-      static_cast<C*>(a.out[2 * b])[row * K1o + kx] = xa;
-      if (2 * b + 1 < (D == 3 ? 6 : 3)) static_cast<C*>(a.out[2 * b + 1])[row * K1o + kx] = xbv;
+      static_cast<C*>(a.out[2 * b])[row * ldo + kx] = xa;
+      if (2 * b + 1 < (D == 3 ? 6 : 3)) static_cast<C*>(a.out[2 * b + 1])[row * ldo + kx] = xbv;
     }
   }
 }
@@ -467,6 +456,7 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
   __syncthreads();
   const float sc = float(a.scale);
   const int K1o = a.K1out;
+  const long long ldo = a.ldo > 0 ? a.ldo : K1o;
 #pragma unroll 1
   for (int half = 0; half < 2; ++half) {
     // F1: products of the half's rows, forward step 1 (pencil p: row half*TH + p % TH, kind p / TH)
@@ -519,8 +509,8 @@ k_xsweep3(const XArgs a, const float2* __restrict__ tw) {
       for (int b = 0; b < 3; ++b) {
         const C* zp = zb + (b * TH + rr) * ZS;
         const C z = zp[kx], zc = zp[kx == 0 ? 0 : ko + kx];
-        static_cast<C*>(a.out[2 * b])[row * K1o + kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
-        static_cast<C*>(a.out[2 * b + 1])[row * K1o + kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
+        static_cast<C*>(a.out[2 * b])[row * ldo + kx] = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
+        static_cast<C*>(a.out[2 * b + 1])[row * ldo + kx] = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
       }
     }
     __syncthreads();
@@ -628,6 +618,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
   const bool has1 = r0 + 1 < a.nrows;
   const int K1 = FULL ? 271 : a.K1in, kmax = K1 - 1;
   const int K1o = FULL ? 271 : a.K1out, ko = K1o - 1;
+  const int ldo = a.ldo > 0 ? a.ldo : K1o;
 
   // L: stage the six input rows (u1, u2, u3 of rows r, r') in region 1 with one
   // round of asynchronous copies; region 1 is not written before Ib.
@@ -825,7 +816,7 @@ k_xsweep4(const XArgs a, const float2* __restrict__ tw) {
   for (int it = t; it < 2 * K1o; it += X4Cfg::NT) {
     const int rr = it >= K1o, kx = it - rr * K1o;
     if (rr == 1 && !has1) continue;
-    const int o = int(r0 + rr) * K1o + kx;  // < 810^2 rows x 406: 32-bit
+    const int o = int(r0 + rr) * ldo + kx;  // < 810^2 rows x 407: 32-bit
     const C* zs = rr ? reg1 : reg0;
     const int kc = kx == 0 ? 0 : ko + kx;
 #pragma unroll
@@ -1026,6 +1017,7 @@ template <> struct ColVariants<810> {
   static constexpr int count = 4;
   static constexpr int T[4] = {8, 8, 4, 16}, S[4] = {0, 1, 0, 0};
 };
+static_assert(ColVariants<810>::count == kColTmaVariant, "the TMA-fed sweep follows the k_col2 variants");
 template <> struct ColVariants<256> {
   static constexpr int count = 2;
   static constexpr int T[2] = {16, 8}, S[2] = {0, 0};
@@ -1098,7 +1090,7 @@ bool launch_xplain_fast(int N, bool inv, const XPlainArgs& a, const void* tw, cu
 
 bool init_fast(int N) {
   switch (N) {
-    case 810: init_fast_n<810>(); init_xpair810(); break;
+    case 810: init_fast_n<810>(); init_xpair810(); colt_init(); break;
     case 256: init_fast_n<256>(); break;
     case 128: init_fast_n<128>(); break;
     case 64: init_fast_n<64>(); break;
@@ -1141,6 +1133,9 @@ template <int N, bool INV> static void col2_n(const ColArgs& a, const void* tw, 
       return;
     }
   }
+  if (N == 810 && a.variant >= kColTmaVariant && a.variant < kColTmaVariant + kColTmaConfigs &&
+      launch_colt(N, INV, a, tw, a.variant - kColTmaVariant, st))
+    return;
   const int v = a.variant >= 0 && a.variant < ColVariants<N>::count ? a.variant : 0;
   col2_variant<N, INV>(v, a, t2, st);
 }
@@ -1157,7 +1152,7 @@ bool launch_col2(int N, bool inv, const ColArgs& a, const void* tw, cudaStream_t
 
 int col2_variants(int N) {
   switch (N) {
-    case 810: return ColVariants<810>::count;
+    case 810: return ColVariants<810>::count + kColTmaConfigs;  // + the TMA-fed sweeps
     case 256: return ColVariants<256>::count;
     case 128: return ColVariants<128>::count;
     case 64: return ColVariants<64>::count;

@@ -22,6 +22,23 @@
 namespace sc {
 
 // ---------------------------------------------------------------------------
+// compact (2/3-rule) layout of a transform axis: kpos modes e < kpos kept in
+// place, kneg modes e >= N - kneg moved down by N - kpos - kneg
+// ---------------------------------------------------------------------------
+// compact position of transform index f, -1 when f is not retained
+__device__ __forceinline__ int cpos(int f, int N, int kpos, int kneg) {
+  return f < kpos ? f : (f >= N - kneg ? f - N + kpos + kneg : -1);
+}
+
+// Where a block of B consecutive transform indices e0 .. e0 + B - 1 falls in
+// the compact layout (kpos modes e < kpos kept in place, kneg modes
+// e >= N - kneg moved down by N - kpos - kneg): 0 every index kept in place,
+// 1 every index moved, 2 none kept, 3 the block straddles a boundary.
+constexpr int crange(int e0, int B, int N, int kpos, int kneg) {
+  return e0 + B - 1 < kpos ? 0 : (e0 >= N - kneg ? 1 : (e0 >= kpos && e0 + B - 1 < N - kneg ? 2 : 3));
+}
+
+// ---------------------------------------------------------------------------
 // complex helpers
 // ---------------------------------------------------------------------------
 template <typename R> struct V2;

@@ -30,6 +30,10 @@ struct ColArgs {
   int drv_src[kMaxComp];
   double kfac;
   int variant;  // FP32 fast sizes: kernel variant chosen by the autotuner (0 = default)
+  // bounded device waits of the TMA-fed sweeps: polls before a wait gives up
+  // and the plan's device error word it then sets (nullptr: no TMA sweep)
+  long long wait_limit;
+  int* err;
 };
 
 // The x sweep of the Navier-Stokes right-hand side: per row (y[, z]) read the
@@ -44,6 +48,7 @@ struct XArgs {
   long long nrows;
   double scale;
   int variant;  // FP32 fast sizes: kernel variant chosen by the autotuner (0 = default)
+  int ldo;      // row stride of the outputs (elements; 0: K1out)
 };
 
 // Plain batched c2r / r2c along x for `ncomp` rows-of-fields (FFT API).
@@ -144,6 +149,12 @@ void launch_random_finish(void* const* w, void* const* out, int D, int n, int K1
 bool launch_xplain_fast(int N, bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st);
 // number of autotuner variants of the FP32 column sweeps / 3D x sweep of size N
 int col2_variants(int N);
+// TMA-fed persistent column sweeps for N = 810 (sc_coltma.cu): column-sweep
+// variants kColTmaVariant + which, which < kColTmaConfigs; false when the
+// geometry does not allow them (the caller then launches k_col2)
+constexpr int kColTmaVariant = 4, kColTmaConfigs = 3;
+bool colt_init();
+bool launch_colt(int N, bool inv, const ColArgs& a, const void* tw, int which, cudaStream_t st);
 int xsweep_variants(int N, int D);
 // FP32 n = 810 x sweep on paired rows (sc_xpair.cu).  Its twiddles are the
 // plain table's exp(-2 pi i j / 810) as register-pair entries

@@ -238,6 +238,7 @@ k_xsweep_ns(const XArgs a, const typename V2<R>::T* __restrict__ tw) {
   // split the paired spectra: X_a = (Z_k + conj Z_{N-k})/2, X_b = -i/2 (Z_k - conj Z_{N-k})
   constexpr int NB = D == 3 ? 3 : 2;
   const int nout = D == 3 ? 6 : 3;
+  const long long ldo = a.ldo > 0 ? a.ldo : a.K1out;
   for (int idx = threadIdx.x; idx < TR * a.K1out; idx += NT) {
     const int t = idx / a.K1out, kx = idx % a.K1out;
     const long long row = row0 + t;
@@ -249,8 +250,8 @@ k_xsweep_ns(const XArgs a, const typename V2<R>::T* __restrict__ tw) {
       const C z = sb[kx], zc = sb[kn];
       const C xa = mk<C>(R(0.5) * (z.x + zc.x), R(0.5) * (z.y - zc.y));
       const C xb = mk<C>(R(0.5) * (z.y + zc.y), R(0.5) * (zc.x - z.x));
-      static_cast<C*>(a.out[2 * b])[row * a.K1out + kx] = xa;
-      if (2 * b + 1 < nout) static_cast<C*>(a.out[2 * b + 1])[row * a.K1out + kx] = xb;
+      static_cast<C*>(a.out[2 * b])[row * ldo + kx] = xa;
+      if (2 * b + 1 < nout) static_cast<C*>(a.out[2 * b + 1])[row * ldo + kx] = xb;
     }
   }
 }

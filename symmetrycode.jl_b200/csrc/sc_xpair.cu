@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
   const bool has1 = r0 + 1 < a.nrows;
   const int K1 = FULL ? 271 : a.K1in, kmax = K1 - 1;
   const int K1o = FULL ? 271 : a.K1out, ko = K1o - 1;
+  const long long ldo = a.ldo > 0 ? a.ldo : K1o;
 
   // L: stage the six rows (u1, u2, u3 of r and r') into slot 2, [c][row][K1]
   float2* rin = reinterpret_cast<float2*>(s2);
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(kXT, MINB) k_xpair810(const XArgs a, const flo
   for (int c = 0; c < 6; ++c) o[c] = static_cast<float2*>(a.out[c]);
   for (int kx = t; kx < K1o; kx += kXT) {
     const int kc = kx == 0 ? 0 : ko + kx;
-    const long long oa = r0 * K1o + kx, ob = oa + K1o;
+    const long long oa = r0 * ldo + kx, ob = oa + ldo;
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
       const P2* zs = b == 0 ? s0 : b == 1 ? s1 : s2;

@@ -597,9 +597,19 @@ def random_field(g: Grid, seed=0, kpeak=4.0, totalenergy=1.0, draws=None, out=No
 def set_option(g: Grid, option, value):
     """``sc_plan_set_option``: ``SC_OPT_USE_GRAPH`` (1) replays captured CUDA
     graphs in the steppers (default) or launches eagerly (0);
-    ``SC_OPT_WAIT_LIMIT`` (2) bounds the tensor-core CNN's device waits (polls;
-    negative: the default)."""
+    ``SC_OPT_WAIT_LIMIT`` (2) bounds the device waits of the tensor-core CNN
+    and of the TMA-fed column sweeps (polls; negative: the default);
+    ``SC_OPT_VARIANT_*`` (3..7) pick a sweep's kernel variant (``autotune``)."""
     check(lib().sc_plan_set_option(g.plan, int(option), int(value)))
+
+
+def plan_status(g: Grid):
+    """``sc_plan_status``: SC_ERR_TIMEOUT (7) if a bounded wait of the plan's
+    TMA-fed column sweeps ran out since the last call, else 0 (synchronous;
+    reading clears the record)."""
+    st = ct.c_int()
+    check(lib().sc_plan_status(g.plan, ct.byref(st)))
+    return st.value
 
 
 def propose_timestep(u, g: Grid, visc, stream=None):

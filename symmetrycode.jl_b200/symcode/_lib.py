@@ -97,6 +97,7 @@ _SIGS = {
     "sc_les_batch_destroy": ([_vp], ct.c_int),
     "sc_plan_set_option": ([_vp, ct.c_int, ct.c_longlong], ct.c_int),
     "sc_plan_num_variants": ([_vp, ct.c_int, ct.POINTER(ct.c_int)], ct.c_int),
+    "sc_plan_status": ([_vp, ct.POINTER(ct.c_int)], ct.c_int),
     "sc_propose_timestep": ([_vp, _pp, ct.c_double, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_shell_energies": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),
     "sc_maintain_shell_energy": ([_vp, _pp, ct.POINTER(ct.c_double), _vp], ct.c_int),

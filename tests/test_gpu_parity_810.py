@@ -185,8 +185,9 @@ def test_sfs_810_fp32_matches_oracle(bench_field, oracle810):
 
 def test_every_810_sweep_variant_matches_triad_oracle():
     """Every kernel variant the autotuner may pick at 810 (column tiles 8 / 4 /
-    16, the 30 x 27 split, the three x-sweep kernels) computes the same FP32
-    right-hand side, pinned to the exact triad oracle."""
+    16, the 30 x 27 split, the three TMA-fed column sweeps, the four x-sweep
+    kernels) computes the same FP32 right-hand side, pinned to the exact triad
+    oracle."""
     from symcode import autotune as A
     k, u = T.random_sparse_field(N, 200, 23, extra=EDGES)
     kout, du_ref = T.convectiondiffusion(k, u, N, NU)
@@ -202,7 +203,7 @@ def test_every_810_sweep_variant_matches_triad_oracle():
     oz, oy, ox = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kout, N))
     ref = [torch.from_numpy(du_ref[:, c]).to(DEV) for c in range(3)]
     counts = A.num_variants(g)
-    assert counts == [4, 4, 4, 4, 4]
+    assert counts == [4, 7, 4, 7, 7]
     du = S.vectorfield(g)
     for s, name in enumerate(A.SWEEPS):
         for v in range(counts[s]):
@@ -211,6 +212,56 @@ def test_every_810_sweep_variant_matches_triad_oracle():
             err = _triad_err(du, ref, (oz, oy, ox))
             print(f"{name} variant {v}: {err:.3e}")
             assert err < 1e-5, (name, v, err)
+    # the three sweeps with TMA-fed variants on one configuration at once, with
+    # no bounded wait run out
+    for v in (4, 5, 6):
+        A.set_variants(g, {"z_inverse": 0, "y_inverse": v, "x_sweep": 0, "y_forward": v, "z_forward": v})
+        S.convectiondiffusion_(du, uin, g, NU)
+        err = _triad_err(du, ref, (oz, oy, ox))
+        print(f"TMA-fed column sweeps, variant {v}: {err:.3e}")
+        assert err < 1e-5
+    assert S.plan_status(g) == 0
+    g.close()
+
+
+def test_tma_sweep_wait_limit_reports_timeout_and_recovers():
+    """SC_OPT_WAIT_LIMIT = 0 makes the first mbarrier wait of every CTA of the
+    TMA-fed column sweeps give up at once: the CTA records the timeout, waits
+    (with the default bound) for its copies in flight and returns, nothing
+    hangs or faults, sc_plan_status reports SC_ERR_TIMEOUT once, and the next
+    evaluation with the default bound is exact again."""
+    from symcode import autotune as A
+    from symcode._lib import SC_ERR_TIMEOUT, SC_OPT_WAIT_LIMIT
+    k, u = T.random_sparse_field(N, 60, 29, extra=EDGES)
+    kout, du_ref = T.convectiondiffusion(k, u, N, NU)
+    g = S.Grid(3, N, dtype=torch.float32, device=DEV)
+    kf, uf = T.full_modes(k, u)
+    m = kf[:, 0] >= 0
+    iz, iy, ix = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kf[m], N))
+    uin = []
+    for c in range(3):
+        t = torch.zeros(g.spec_shape, dtype=g.cdtype, device=DEV)
+        t[iz, iy, ix] = torch.from_numpy(uf[m][:, c]).to(g.cdtype).to(DEV)
+        uin.append(t)
+    oz, oy, ox = (torch.from_numpy(a).to(DEV) for a in T.to_rfft_index(kout, N))
+    ref = [torch.from_numpy(du_ref[:, c]).to(DEV) for c in range(3)]
+    A.set_variants(g, {"y_inverse": 4, "y_forward": 4, "z_forward": 4})
+    good = S.vectorfield(g)
+    S.convectiondiffusion_(good, uin, g, NU)
+    # the FP32 floor at 810 (about 1e-5, growing like n; the bench field's bar)
+    assert _triad_err(good, ref, (oz, oy, ox)) < 1.2e-5
+    assert S.plan_status(g) == 0
+    du = S.vectorfield(g)
+    S.set_option(g, SC_OPT_WAIT_LIMIT, 0)
+    S.convectiondiffusion_(du, uin, g, NU)
+    torch.cuda.synchronize()
+    assert S.plan_status(g) == SC_ERR_TIMEOUT
+    assert S.plan_status(g) == 0  # reading cleared the record
+    S.set_option(g, SC_OPT_WAIT_LIMIT, -1)
+    S.convectiondiffusion_(du, uin, g, NU)
+    assert S.plan_status(g) == 0
+    for a, b in zip(du, good):  # the same deterministic launches as before the timeout
+        assert torch.equal(a, b)
     g.close()
 
 
