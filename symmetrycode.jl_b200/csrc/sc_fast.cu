@@ -875,8 +875,14 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xc2r_fast(const XPlainArgs a,
   // modes per component); one warp stages one row, so no per-element division
   const int npair = (a.ncomp + 1) / 2, K1 = a.K1;
   const int npen = int(a.nrows) * npair, pen0 = blockIdx.x * TP;
+  // both loops have compile-time trip counts and are unrolled, so each thread
+  // issues all of its loads before the first store (a rolled loop waited out
+  // one global-load latency per element)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int s = warp; s < 2 * TP; s += NT / 32) {
+  static_assert((2 * TP) % (NT / 32) == 0, "whole rows per warp");
+#pragma unroll
+  for (int i = 0; i < 2 * TP / (NT / 32); ++i) {
+    const int s = warp + i * (NT / 32);
     const int pen = pen0 + (s >> 1);
     const float2* src = nullptr;
     if (pen < npen) {
@@ -884,7 +890,11 @@ __global__ void __launch_bounds__(XPFCfg<N>::NT) k_xc2r_fast(const XPlainArgs a,
       if (q < a.ncomp) src = static_cast<const float2*>(a.in[q]) + row * K1;
     }
     float2* dst = rin + s * KMAX;
-    for (int kx = lane; kx < K1; kx += 32) dst[kx] = src ? __ldg(src + kx) : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < (KMAX + 31) / 32; ++u) {
+      const int kx = lane + 32 * u;
+      if (kx < K1) dst[kx] = src ? __ldg(src + kx) : make_float2(0.f, 0.f);
+    }
   }
   __syncthreads();
   for (int it = threadIdx.x; it < TP * N2; it += NT) {
