@@ -101,6 +101,16 @@ __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// zero 32 lanes x 16 columns of tensor memory (this warp's lane quadrant)
+__device__ __forceinline__ void tmem_zero16(uint32_t taddr) {
+  const uint32_t z = 0;
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+      "r"(z)
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
 // GELU in the tanh form of NNlib's gelu (the activation of the reference's nets):
 // 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).  The hardware tanh.approx
 // (relative error about 2^-11) is below the BF16 rounding of the activations.
@@ -142,15 +152,35 @@ struct ConvOut {
 
 // One convolution layer.  act_in: BF16 channels-last [n^3][CP]; weights:
 // BF16 [27][CP/8][COP][8] (UMMA K-major planes per tap); output per MODE.
-// Each CTA walks a contiguous run of x-rows (y fastest), software-pipelined
-// with one CTA barrier per row and three warp roles:
-//  - warp 0, one thread: issues the 27 x CP/16 MMAs of row y into one of two
-//    tensor-memory accumulators;
-//  - warps 1-3: once the MMAs of row y-1 are done, fetch row y+3 with cp.async
-//    into the ring slot that row y-2 left (kSlots y-slots per z-offset; row
-//    y+2 is already resident, so each fetch has two rows of time to land);
-//  - warps 4-11 (two per tensor-memory lane quadrant): the epilogue of row
-//    y-1 from the other accumulator, while row y computes.
+//
+// Input-stationary MMAs: an output row (y, z) sums the 27 taps over the input
+// rows (y + dy, z + dz), so one staged input row (y', z + dz) shifted by dx
+// feeds the three output rows y' - 1, y', y' + 1 (dy = +1, 0, -1) at once: one
+// MMA of N = 3 C_out per (dz, dx, 16 input channels) against the weights
+// stacked in shared memory as [dz][dx][k-chunk][dy = +1, 0, -1][C_out][8],
+// instead of three MMAs of N = C_out -- the same FLOPs with a third of the
+// A-operand reads, so the tensor pipe rather than the shared-memory operand
+// bandwidth sets the pace.  Output row y accumulates in tensor-memory block
+// y mod 6 (C_out columns each) and the MMAs of step y' write blocks
+// m, m + 1, m + 2 with m = (y' - 1) mod 6, where blocks 6 and 7 stand in for
+// blocks 0 and 1: the three rows always form one contiguous range, every MMA
+// has the same shape and accumulates (MMAs of mixed shapes or split column
+// ranges measured up to 5x slower), and a row of block 0 or 1 is the sum of
+// that block and its stand-in.  Row y completes with step y + 1; its blocks are
+// read out and zeroed one step later, well before row y + 6 takes them.  A step
+// is 9 x CP/16 MMAs; the steps of a run of output rows y0..y1 of one plane go
+// from y0 - 1 to y1 + 1.
+//
+// Each CTA walks a contiguous run of x-rows (y fastest), one CTA barrier per
+// step, three warp roles:
+//  - warp 0, one thread: issues the MMAs of step y' and commits them to one of
+//    two mbarriers;
+//  - warps 1-3: once step y' - 1 is done, fetch input row y' + 4 with cp.async
+//    into the ring slot that input row y' - 1 left (kSlots y-slots per
+//    z-offset, four steps ahead);
+//  - warps 4-11 (two per tensor-memory lane quadrant): once step y' - 1 is
+//    done, read out and zero row y' - 2 and run its bias + activation + store,
+//    while step y' computes.
 // A change of z-plane drains the pipeline and restages the new plane.
 constexpr int kSlots = 5;
 constexpr int kConvThreads = 384;
@@ -163,9 +193,10 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   constexpr int CPC = CP / 8;              // 16-byte channel chunks
   constexpr int PLANE_ROW = CPC * kRowPlane;
   constexpr int SIN = 3 * kSlots * PLANE_ROW;  // [zr][slot] staged rows
-  constexpr int SW = 27 * CPC * COP * 16;
-  constexpr uint32_t IDESC = make_idesc<COP>();
-  constexpr uint32_t kTmemCols = 64;       // two accumulators of COP <= 32 columns
+  constexpr int NS = 3 * COP;              // stacked rows per k-chunk plane: the three dy taps
+  constexpr int SW = 9 * CPC * NS * 16;
+  constexpr uint32_t IDESC = make_idesc<3 * COP>();
+  constexpr uint32_t kTmemCols = 8 * COP;  // eight accumulator blocks
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char* s_in = sm;
   unsigned char* s_w = sm + SIN;
@@ -178,8 +209,15 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   const int ecol0 = warp >= 8 ? COP / 2 : 0;
   const bool is_epi = warp >= 4 && (COP / 2 == 16 || warp < 8) && lane_base < KN;
 
-  for (int i = tid; i < SW / 16; i += blockDim.x)
-    reinterpret_cast<uint4*>(s_w)[i] = __ldg(reinterpret_cast<const uint4*>(wgt) + i);
+  // stacked weights: chunk ((dz 3 + dx) CPC + kc) NS + j COP + co holds tap
+  // (dz, dy index 2 - j, dx) of the [27][CPC][COP] layout (dy index 0, 1, 2
+  // for dy = -1, 0, +1), j = 0, 1, 2 for the output rows y' - 1, y', y' + 1
+  for (int d = tid; d < SW / 16; d += blockDim.x) {
+    const int co = d % COP, j = (d % NS) / COP, kc = (d / NS) % CPC, g = d / (NS * CPC);
+    const int dyi = 2 - j;
+    const int src = (((g / 3) * 9 + dyi * 3 + g % 3) * CPC + kc) * COP + co;
+    reinterpret_cast<uint4*>(s_w)[d] = __ldg(reinterpret_cast<const uint4*>(wgt) + src);
+  }
   float bia[16];
 #pragma unroll
   for (int c = 0; c < 16; ++c)
@@ -244,10 +282,28 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
     return r;
   };
   // epilogue of row prow from accumulator buffer b (epilogue warps)
-  auto epilogue = [&](int prow, int b) {
+  // tensor-memory block of output row y (y >= -2); blocks 0 and 1 also
+  // accumulate in their stand-ins 6 and 7
+  auto acc_blk = [](int y) -> int { return ((y % 6) + 6) % 6; };
+  // read out row y's 16 columns of this warp and zero them (epilogue warps)
+  auto readout = [&](int y, float* v) {
     if (!is_epi) return;
-    float v[16];
-    tmem_ld<16>(tmem + (uint32_t(lane_base) << 16) + uint32_t(b * 32 + ecol0), v);
+    const int blk = acc_blk(y);
+    const uint32_t ta = tmem + (uint32_t(lane_base) << 16) + uint32_t(blk * COP + ecol0);
+    tmem_ld<16>(ta, v);
+    tmem_zero16(ta);
+    if (blk < 2) {
+      float w[16];
+      const uint32_t tb = ta + uint32_t(6 * COP);
+      tmem_ld<16>(tb, w);
+      tmem_zero16(tb);
+#pragma unroll
+      for (int c = 0; c < 16; ++c) v[c] += w[c];
+    }
+  };
+  // bias + activation + store of row prow (z KN + y) from the read-out values
+  auto epilogue = [&](int prow, const float* v) {
+    if (!is_epi) return;
     const long long vox = (long long)prow * KN + lane_base + tid % 32;
     if (MODE == kGelu || MODE == kGeluSave) {
       __align__(16) __nv_bfloat16 o[16];
@@ -274,80 +330,75 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
       for (int j = 0; j < 4; ++j) pl[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
   };
-  // wait for buffer b everywhere, run its epilogue, barrier; false on a timeout
-  auto drain = [&](int prow) -> bool {
-    const int b = prow & 1;
-    const bool mine = wait_buf(b);
-    if (mine) epilogue(prow, b);
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    const bool all = __syncthreads_and(mine) != 0;
-    if (all) { phase ^= 1u << b; inflight &= ~(1u << b); }
-    return all;
-  };
-
   const int nrows = KN * KN;
   const int per = (nrows + gridDim.x - 1) / gridDim.x;
   const int rbeg = blockIdx.x * per;
   const int rend = min(rbeg + per, nrows);
-  int cur_z = -1;
-  int pending = -1;  // row whose accumulator still needs its epilogue
-  for (int row = rbeg; row < rend; ++row) {
-    const int y = row % KN, z = row / KN;
-    if (z != cur_z) {
-      // new plane: drain, then stage rows y-1 .. y+2 as one group (all threads)
-      if (pending >= 0) {
-        ok = drain(pending);
-        pending = -1;
-        if (!ok) break;
-      }
-      stage(z, y - 1, min(y + 2, KN), tid, kConvThreads);
-      commit();
-      cur_z = z;
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 1;" ::: "memory");  // row y+1 has landed; row y+2 may be in flight
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    const int b = row & 1;
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      // descriptors are a base plus a compile-time offset (start-address field
-      // in 16-byte units); only the three ring slots of this row are run-time
-      const uint64_t DA0 = make_desc(smem_u32(s_in), kRowPlane, 128);
-      const uint64_t DB0 = make_desc(smem_u32(s_w), COP * 16, 128);
-      const uint32_t dcol = tmem + uint32_t(b * 32);
-      uint32_t sl[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) sl[d] = uint32_t((y + d - 1 + KN) % kSlots) * (PLANE_ROW >> 4);
-#pragma unroll
-      for (int t = 0; t < 27; ++t) {
-        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-        const uint64_t arow = DA0 + sl[dy] + uint32_t(dz * kSlots * (PLANE_ROW >> 4) + dx);
-#pragma unroll
-        for (int h = 0; h < CPC / 2; ++h) {
-          const uint64_t da = arow + uint32_t(2 * h * (kRowPlane >> 4));
-          const uint64_t db = DB0 + uint32_t((t * CPC + 2 * h) * COP);
-          mma_bf16(dcol, da, db, IDESC, (t | h) ? 1u : 0u);
-        }
-      }
-      mma_commit(bar + b);
-    }
-    inflight |= 1u << b;
-    bool mine = true;
-    if (pending >= 0 && warp != 0) mine = wait_buf(pending & 1);  // the last readers of row y-2's slot
-    // prefetch row y+3 (read first by the MMAs of row y+2, when this CTA runs
-    // that row in this plane); every thread commits a group, empty or not
-    if (is_stage && mine && y + 2 < KN && row + 2 < rend) stage_row(z, y + 3, tid - 32);
+  int k = 0;  // MMA step counter: step k commits to mbarrier k & 1
+  float v[16];  // read-out accumulator values (epilogue warps)
+  for (int r0 = rbeg; r0 < rend && ok;) {
+    // one run of output rows y0..y1 of plane z
+    const int z = r0 / KN, y0 = r0 % KN;
+    const int y1 = min(KN - 1, y0 + (rend - r0) - 1);
+    const int zrow = z * KN;
+    r0 += y1 - y0 + 1;
+    // stage input rows y0 - 1 .. y0 + 2 (all threads, one group) and zero the
+    // accumulator blocks
+    stage(z, y0 - 1, min(y0 + 2, y1 + 1), tid, kConvThreads);
     commit();
-    if (pending >= 0 && mine) epilogue(pending, pending & 1);
+    if (is_epi)
+      for (int q = 0; q < 8; ++q) tmem_zero16(tmem + (uint32_t(lane_base) << 16) + uint32_t(q * COP + ecol0));
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    for (int yv = y0 - 1; yv <= y1 + 1; ++yv, ++k) {
+      const int b = k & 1;
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint64_t DA0 = make_desc(smem_u32(s_in), kRowPlane, 128);
+        const uint64_t DB0 = make_desc(smem_u32(s_w), NS * 16, 128);
+        const uint32_t sa = uint32_t((yv + KN) % kSlots) * (PLANE_ROW >> 4);  // the staging's ring slot
+        const uint32_t dcol = tmem + uint32_t(acc_blk(yv - 1) * COP);         // rows yv - 1, yv, yv + 1
+#pragma unroll
+        for (int g = 0; g < 9 * (CPC / 2); ++g) {
+          const int dz = g / (3 * (CPC / 2)), dx = (g / (CPC / 2)) % 3, h = g % (CPC / 2);
+          const uint64_t da = DA0 + sa + uint32_t(dz * kSlots * (PLANE_ROW >> 4) + dx + 2 * h * (kRowPlane >> 4));
+          const uint64_t db = DB0 + uint32_t(((dz * 3 + dx) * CPC + 2 * h) * NS);
+          mma_bf16(dcol, da, db, IDESC, 1u);
+        }
+        mma_commit(bar + b);
+      }
+      inflight |= 1u << b;
+      bool mine = true;
+      const bool first = yv == y0 - 1;
+      // step yv - 1: the last reader of input row yv - 1's ring slot and the
+      // last writer of row yv - 2 (the outcome is made warp-uniform: the
+      // tensor-memory loads and stores below are warp-collective)
+      if (!first && warp != 0) mine = __all_sync(0xffffffffu, wait_buf(b ^ 1));
+      if (is_stage && mine && yv + 4 <= y1 + 1) stage_row(z, yv + 4, tid - 32);
+      commit();
+      const bool out_row = yv - 2 >= y0;
+      if (mine && !first) readout(yv - 2, v);  // also zeroes its blocks for row yv + 4
+      if (mine && out_row) epilogue(zrow + yv - 2, v);
+      // input row yv + 1 (fetched three groups ago) has landed for step yv + 1
+      asm volatile("cp.async.wait_group 3;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      ok = __syncthreads_and(mine) != 0;
+      if (!ok) break;
+      if (!first) { phase ^= 1u << (b ^ 1); inflight &= ~(1u << (b ^ 1)); }
+    }
+    if (!ok) break;
+    // the run's last step completes row y1
+    const int b = (k - 1) & 1;
+    const bool mine = __all_sync(0xffffffffu, wait_buf(b));
+    if (mine) readout(y1, v);
+    if (mine) epilogue(zrow + y1, v);
     asm volatile("tcgen05.fence::before_thread_sync;");
     ok = __syncthreads_and(mine) != 0;
-    if (!ok) break;
-    if (pending >= 0) { phase ^= 1u << (pending & 1); inflight &= ~(1u << (pending & 1)); }
-    pending = row;
+    if (ok) { phase ^= 1u << b; inflight &= ~(1u << b); }
   }
-  if (ok && pending >= 0) ok = drain(pending);
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
