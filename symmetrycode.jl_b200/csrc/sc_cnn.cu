@@ -133,11 +133,9 @@ __device__ __forceinline__ float gelu_grad(float x) {
 
 }  // namespace
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-
-template <int KN> constexpr int row_plane() { return (KN + 2) * 16; }  // bytes of one k-chunk plane of a staged row
+// bytes of one k-chunk plane of a staged row: KN + 2 voxels of 16 bytes,
+// rounded up to 128 bytes so that every plane is a bulk-copy destination
+template <int KN> constexpr int row_plane() { return ((KN + 2) * 16 + 127) / 128 * 128; }
 
 // Epilogue modes: BF16 GELU activations; the same plus the FP32
 // pre-activations (kept for the adjoint); FP32 planar tau (last layer);
@@ -171,23 +169,28 @@ struct ConvOut {
 // is 9 x CP/16 MMAs; the steps of a run of output rows y0..y1 of one plane go
 // from y0 - 1 to y1 + 1.
 //
-// Each CTA walks a contiguous run of x-rows (y fastest), one CTA barrier per
-// step, three warp roles:
-//  - warp 0, one thread: issues the MMAs of step y' and commits them to one of
-//    two mbarriers;
-//  - warps 1-3: once step y' - 1 is done, fetch input row y' + 4 with cp.async
-//    into the ring slot that input row y' - 1 left (kSlots y-slots per
-//    z-offset, four steps ahead);
-//  - warps 4-11 (two per tensor-memory lane quadrant): once step y' - 1 is
-//    done, read out and zero row y' - 2 and run its bias + activation + store,
-//    while step y' computes.
-// A change of z-plane drains the pipeline and restages the new plane.
+// Each CTA walks a contiguous run of x-rows (y fastest) of one plane at a
+// time.  Three warp roles run decoupled within a run, handing off through
+// mbarriers (every wait bounded; a wait that runs out raises a shared abort
+// flag that ends the other roles' waits too):
+//  - warp 0, one thread: for each step y', waits until input row y' is staged
+//    and (from the sixth step on) until the block of row y' + 1 was read out
+//    and zeroed, issues the MMAs and commits them to step barrier k mod 4;
+//  - warp 1: waits for the copies of input row y' + 1, writes its halo and
+//    marks it staged, then, once step y' - 1 is done, issues the bulk copies
+//    of input row y' + 4 into the ring slot row y' - 1 left;
+//  - warps 4-11 (two per tensor-memory lane quadrant): for each row, once the
+//    step that completes it is done, read it out, zero its blocks and mark
+//    them free, then bias + activation + store.
+// The epilogue may lag the MMAs by up to four steps (the accumulator ring and
+// the four step barriers), so its latency overlaps the tensor pipe's work.  A
+// change of z-plane ends the run with a CTA barrier and restages.
 constexpr int kSlots = 5;
 constexpr int kConvThreads = 384;
 
 template <int KN, int CP, int COP, int MODE>
 __global__ void __launch_bounds__(kConvThreads, 1)
-k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restrict__ wgt,
+k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__ wgt,
         const float* __restrict__ bias, const ConvOut out, int* __restrict__ err, long long wait_limit) {
   constexpr int kRowPlane = row_plane<KN>();
   constexpr int CPC = CP / 8;              // 16-byte channel chunks
@@ -200,14 +203,19 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char* s_in = sm;
   unsigned char* s_w = sm + SIN;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + SIN + SW);       // [2]
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SIN + SW + 16);
-  const int tid = threadIdx.x, warp = tid / 32;
-  const bool is_stage = warp >= 1 && warp < 4;
+  uint64_t* cbar = reinterpret_cast<uint64_t*>(sm + SIN + SW);       // [4] MMA steps
+  uint64_t* staged = cbar + 4;                                        // [kSlots] row copies landed
+  uint64_t* ready = staged + kSlots;                                  // [kSlots] rows staged (halo written)
+  uint64_t* zeroed = ready + kSlots;                                  // [6] accumulator blocks free
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(zeroed + 6);
+  int* abort_flag = reinterpret_cast<int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   // epilogue warps: lane quadrant warp % 4 (rows 32 (warp % 4) ..), columns ecol0 .. ecol0 + 15
   const int lane_base = 32 * (warp % 4);
   const int ecol0 = warp >= 8 ? COP / 2 : 0;
   const bool is_epi = warp >= 4 && (COP / 2 == 16 || warp < 8) && lane_base < KN;
+  // number of epilogue warps (the arrival count of the zeroed barriers)
+  constexpr int NEPI = ((COP / 2 == 16) ? 2 : 1) * (KN >= 128 ? 4 : (KN + 31) / 32);
 
   // stacked weights: chunk ((dz 3 + dx) CPC + kc) NS + j COP + co holds tap
   // (dz, dy index 2 - j, dx) of the [27][CPC][COP] layout (dy index 0, 1, 2
@@ -223,9 +231,15 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   for (int c = 0; c < 16; ++c)
     bia[c] = (is_epi && MODE != kLinear && (MODE != kTau || c < 6)) ? __ldg(bias + ecol0 + c) : 0.f;
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + 1)));
+    for (int q = 0; q < 4; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(cbar + q)));
+    for (int q = 0; q < kSlots; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(staged + q)));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(ready + q)));
+    }
+    for (int q = 0; q < 6; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(zeroed + q)), "r"(NEPI));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *abort_flag = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -236,58 +250,41 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tslot;
-  uint32_t phase = 0;     // bit b: parity of the next wait on buffer b (same in every thread)
-  uint32_t inflight = 0;  // bit b: a committed MMA group of buffer b not yet waited for
   bool ok = true;
 
-  // copy x-rows ylo..yhi of the three z-offsets of plane z into their ring slots
-  auto stage = [&](int z, int ylo, int yhi, int t0, int tstride) {
-    const int nyr = yhi - ylo + 1;
-    const int chunks = 3 * nyr * (KN + 2) * CPC;
-    for (int i = t0; i < chunks; i += tstride) {
-      const int kc = i % CPC;
-      const int xi = (i / CPC) % (KN + 2);
-      const int q = i / (CPC * (KN + 2));
-      const int zr = q / nyr, yv = ylo + q % nyr;
-      const int zz = (z + zr - 1 + KN) % KN, yy = (yv + KN) % KN;
-      const int x = (xi - 1 + KN) % KN;
-      const long long vox = ((long long)zz * KN + yy) * KN + x;
-      unsigned char* dst = s_in + (zr * kSlots + (yv + KN) % kSlots) * PLANE_ROW + kc * kRowPlane + xi * 16;
-      cp_async16(dst, reinterpret_cast<const uint4*>(act_in + vox * CP) + kc);
+  // bounded wait that also gives up once another role raised the abort flag;
+  // it spins on the non-suspending test_wait (the roles hand off every step,
+  // and a suspended try_wait resumed measurably later than the phase completed)
+  auto wait = [&](uint64_t* bar, uint32_t parity) -> bool {
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < wait_limit; ++it) {
+      uint32_t done;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}\n"
+          : "=r"(done)
+          : "r"(a), "r"(parity)
+          : "memory");
+      if (done) return true;
+      if ((it & 63) == 63 && *reinterpret_cast<volatile int*>(abort_flag)) return false;
     }
+    return false;
   };
-  // one row yv of plane z by the 96 staging threads: 96 is a multiple of CPC, so
-  // each thread keeps its channel chunk and walks (z-offset, x) with adds only
-  auto stage_row = [&](int z, int yv, int pt) {
-    const int kc = pt % CPC, step = 96 / CPC;
-    const int yy = (yv + KN) % KN, sl = (yv + KN) % kSlots;
-    const long long zb0 = ((long long)((z - 1 + KN) % KN) * KN + yy) * KN;
-    const long long zb1 = ((long long)z * KN + yy) * KN;
-    const long long zb2 = ((long long)((z + 1) % KN) * KN + yy) * KN;
-    for (int xz = pt / CPC; xz < 3 * (KN + 2); xz += step) {
-      const int zr = xz >= 2 * (KN + 2) ? 2 : (xz >= KN + 2 ? 1 : 0);
-      const int xi = xz - zr * (KN + 2);
-      int x = xi - 1;
-      x = x < 0 ? x + KN : (x >= KN ? x - KN : x);
-      unsigned char* dst = s_in + (zr * kSlots + sl) * PLANE_ROW + kc * kRowPlane + xi * 16;
-      const long long zb = zr == 0 ? zb0 : (zr == 1 ? zb1 : zb2);
-      cp_async16(dst, reinterpret_cast<const uint4*>(act_in + (zb + x) * CP) + kc);
-    }
+  auto fail = [&] { *reinterpret_cast<volatile int*>(abort_flag) = 1; };
+  auto arrive = [](uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
   };
-  auto commit = [] { asm volatile("cp.async.commit_group;" ::: "memory"); };
-  // bounded wait of this thread for the MMAs of buffer b
-  auto wait_buf = [&](int b) -> bool {
-    const bool r = mbar_wait(bar + b, (phase >> b) & 1u, wait_limit);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    return r;
+  // number of r in [lo, hi) with (r + off) mod m == j
+  auto count_mod = [](int lo, int hi, int j, int m, int off) -> int {
+    const int r0 = lo + (((j - (lo + off)) % m) + m) % m;
+    return r0 < hi ? (hi - 1 - r0) / m + 1 : 0;
   };
-  // epilogue of row prow from accumulator buffer b (epilogue warps)
   // tensor-memory block of output row y (y >= -2); blocks 0 and 1 also
   // accumulate in their stand-ins 6 and 7
   auto acc_blk = [](int y) -> int { return ((y % 6) + 6) % 6; };
   // read out row y's 16 columns of this warp and zero them (epilogue warps)
   auto readout = [&](int y, float* v) {
-    if (!is_epi) return;
     const int blk = acc_blk(y);
     const uint32_t ta = tmem + (uint32_t(lane_base) << 16) + uint32_t(blk * COP + ecol0);
     tmem_ld<16>(ta, v);
@@ -330,36 +327,88 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
       for (int j = 0; j < 4; ++j) pl[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
     }
   };
+  // Input rows reach the ring by bulk tensor copies: row yv of the three
+  // z-offsets of plane z, CP/8 boxes of 8 channels x (KN + 2) voxels each (x
+  // from -1; the copy engine fills x = -1 and x = KN with zeros), completing on
+  // the slot's mbarrier.  Thread 32 issues them; warp 1 then waits for them and
+  // writes the periodic halo voxels x = -1 and x = KN from x = KN - 1 and 0.
+  uint32_t spar = 0;  // bit s: parity of the next wait on staged[s] (same in every thread)
+  uint32_t tin = 0;   // thread 32: bit s set while a copy into slot s is in flight
+  auto slot_of = [](int yv) { return (yv + KN) % kSlots; };
+  auto tma_row = [&](int z, int yv) {
+    const int sl = slot_of(yv), yy = (yv + KN) % KN;
+    // bytes delivered: 3 rows x CP/8 boxes of (KN + 2) 16-byte voxels (the
+    // planes' padding to 128 bytes is not written)
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(staged + sl)),
+                 "r"(3 * CPC * (KN + 2) * 16)
+                 : "memory");
+    for (int zr = 0; zr < 3; ++zr) {
+      const int zz = (z + zr - 1 + KN) % KN;
+      for (int c = 0; c < CPC; ++c) {
+        unsigned char* dst = s_in + (zr * kSlots + sl) * PLANE_ROW + c * kRowPlane;
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+            "[%6];" ::"r"(smem_u32(dst)),
+            "l"(reinterpret_cast<uint64_t>(&maps.m[c])), "r"(0), "r"(-1), "r"(yy), "r"(zz), "r"(smem_u32(staged + sl))
+            : "memory");
+      }
+    }
+    tin |= 1u << sl;
+  };
+  // warp 1: wait for row yv's copies (bounded) and write its halo; warp-uniform result
+  auto patch_row = [&](int yv) -> bool {
+    const int sl = slot_of(yv);
+    const bool w = __all_sync(0xffffffffu, wait(staged + sl, (spar >> sl) & 1u));
+    if (w && lane < 3 * CPC * 2) {
+      const int zr = lane / (2 * CPC), c = (lane / 2) % CPC, side = lane & 1;
+      unsigned char* plane = s_in + (zr * kSlots + sl) * PLANE_ROW + c * kRowPlane;
+      const uint4 v = reinterpret_cast<const uint4*>(plane)[side ? 1 : KN];
+      reinterpret_cast<uint4*>(plane)[side ? KN + 1 : 0] = v;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    return w;
+  };
   const int nrows = KN * KN;
   const int per = (nrows + gridDim.x - 1) / gridDim.x;
   const int rbeg = blockIdx.x * per;
   const int rend = min(rbeg + per, nrows);
-  int k = 0;  // MMA step counter: step k commits to mbarrier k & 1
-  float v[16];  // read-out accumulator values (epilogue warps)
+  int k0 = 0;                    // global index of the run's first step (step k on cbar[k % 4])
+  int rbase[kSlots] = {};        // thread 0: earlier stagings of each ring slot
+  int zbase[6] = {};             // thread 0: earlier read-outs of each accumulator block
+  int last_k = -1;               // thread 0: last committed step
+  float v[16];
   for (int r0 = rbeg; r0 < rend && ok;) {
-    // one run of output rows y0..y1 of plane z
+    // one run of output rows y0..y1 of plane z: steps y0 - 1 .. y1 + 1
     const int z = r0 / KN, y0 = r0 % KN;
     const int y1 = min(KN - 1, y0 + (rend - r0) - 1);
     const int zrow = z * KN;
+    const int nsteps = y1 - y0 + 3;
     r0 += y1 - y0 + 1;
-    // stage input rows y0 - 1 .. y0 + 2 (all threads, one group) and zero the
-    // accumulator blocks
-    stage(z, y0 - 1, min(y0 + 2, y1 + 1), tid, kConvThreads);
-    commit();
+    // copy input rows y0 - 1 .. y0 + 2 and zero the accumulator blocks
+    if (tid == 32)
+      for (int yv = y0 - 1; yv <= min(y0 + 2, y1 + 1); ++yv) tma_row(z, yv);
     if (is_epi)
       for (int q = 0; q < 8; ++q) tmem_zero16(tmem + (uint32_t(lane_base) << 16) + uint32_t(q * COP + ecol0));
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    for (int yv = y0 - 1; yv <= y1 + 1; ++yv, ++k) {
-      const int b = k & 1;
-      if (tid == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    bool mine = true;
+    if (tid == 0) {
+      // MMA issue
+      for (int i = 0; i < nsteps && mine; ++i) {
+        const int yv = y0 - 1 + i, kk = k0 + i;
+        const int sl = slot_of(yv);
+        mine = wait(ready + sl, uint32_t(rbase[sl] + count_mod(y0 - 1, yv, sl, kSlots, KN)) & 1u);
+        if (mine && yv >= y0 + 3) {  // the block of row yv + 1 held row yv - 5 of this run
+          const int q = yv - 5, bq = acc_blk(q);
+          mine = wait(zeroed + bq, uint32_t(zbase[bq] + count_mod(y0 - 2, q, bq, 6, 0)) & 1u);
+        }
+        if (!mine) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint64_t DA0 = make_desc(smem_u32(s_in), kRowPlane, 128);
         const uint64_t DB0 = make_desc(smem_u32(s_w), NS * 16, 128);
-        const uint32_t sa = uint32_t((yv + KN) % kSlots) * (PLANE_ROW >> 4);  // the staging's ring slot
-        const uint32_t dcol = tmem + uint32_t(acc_blk(yv - 1) * COP);         // rows yv - 1, yv, yv + 1
+        const uint32_t sa = uint32_t(sl) * (PLANE_ROW >> 4);
+        const uint32_t dcol = tmem + uint32_t(acc_blk(yv - 1) * COP);  // rows yv - 1, yv, yv + 1
 #pragma unroll
         for (int g = 0; g < 9 * (CPC / 2); ++g) {
           const int dz = g / (3 * (CPC / 2)), dx = (g / (CPC / 2)) % 3, h = g % (CPC / 2);
@@ -367,51 +416,79 @@ k_conv3(const __nv_bfloat16* __restrict__ act_in, const __nv_bfloat16* __restric
           const uint64_t db = DB0 + uint32_t(((dz * 3 + dx) * CPC + 2 * h) * NS);
           mma_bf16(dcol, da, db, IDESC, 1u);
         }
-        mma_commit(bar + b);
+        mma_commit(cbar + (kk & 3));
+        last_k = kk;
       }
-      inflight |= 1u << b;
-      bool mine = true;
-      const bool first = yv == y0 - 1;
-      // step yv - 1: the last reader of input row yv - 1's ring slot and the
-      // last writer of row yv - 2 (the outcome is made warp-uniform: the
-      // tensor-memory loads and stores below are warp-collective)
-      if (!first && warp != 0) mine = __all_sync(0xffffffffu, wait_buf(b ^ 1));
-      if (is_stage && mine && yv + 4 <= y1 + 1) stage_row(z, yv + 4, tid - 32);
-      commit();
-      const bool out_row = yv - 2 >= y0;
-      if (mine && !first) readout(yv - 2, v);  // also zeroes its blocks for row yv + 4
-      if (mine && out_row) epilogue(zrow + yv - 2, v);
-      // input row yv + 1 (fetched three groups ago) has landed for step yv + 1
-      asm volatile("cp.async.wait_group 3;" ::: "memory");
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;");
-      ok = __syncthreads_and(mine) != 0;
-      if (!ok) break;
-      if (!first) { phase ^= 1u << (b ^ 1); inflight &= ~(1u << (b ^ 1)); }
+      if (!mine) fail();
+      for (int j = 0; j < kSlots; ++j) rbase[j] += count_mod(y0 - 1, y1 + 2, j, kSlots, KN);
+      for (int j = 0; j < 6; ++j) zbase[j] += count_mod(y0 - 2, y1 + 1, j, 6, 0);
+    } else if (warp == 1) {
+      // staging: complete row y0 - 1, then per step
+      // (a copy whose wait ran out stays recorded in flight for the exit path)
+      mine = patch_row(y0 - 1);
+      __syncwarp();
+      if (mine) {
+        if (lane == 0) arrive(ready + slot_of(y0 - 1));
+        spar ^= 1u << slot_of(y0 - 1);
+        if (lane == 0) tin &= ~(1u << slot_of(y0 - 1));
+      }
+      for (int i = 0; i < nsteps && mine; ++i) {
+        const int yv = y0 - 1 + i, kk = k0 + i;
+        // complete input row yv + 1 as soon as its copies (issued three steps
+        // ago) have landed: the MMA thread may run several steps ahead
+        if (yv + 1 <= y1 + 1) {
+          mine = patch_row(yv + 1);
+          __syncwarp();
+          if (mine) {
+            if (lane == 0) arrive(ready + slot_of(yv + 1));
+            spar ^= 1u << slot_of(yv + 1);
+            if (lane == 0) tin &= ~(1u << slot_of(yv + 1));
+          }
+        }
+        // copy input row yv + 4 into the slot input row yv - 1 left, once step
+        // yv - 1 (its last reader) is done
+        if (mine && yv + 4 <= y1 + 1) {
+          if (i > 0) mine = __all_sync(0xffffffffu, wait(cbar + ((kk - 1) & 3), uint32_t((kk - 1) >> 2) & 1u));
+          if (mine && lane == 0) tma_row(z, yv + 4);
+        }
+      }
+      if (!mine) fail();
+    } else if (is_epi) {
+      // read-out, zeroing and epilogue of rows y0 - 2 .. y1 (row r completes with step r + 1)
+      for (int r = y0 - 2; r <= y1 && mine; ++r) {
+        const int kk = k0 + (r + 1 - (y0 - 1));
+        mine = __all_sync(0xffffffffu, wait(cbar + (kk & 3), uint32_t(kk >> 2) & 1u));
+        if (!mine) break;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        readout(r, v);
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncwarp();
+        if (lane == 0) arrive(zeroed + acc_blk(r));
+        if (r >= y0) epilogue(zrow + r, v);
+      }
+      if (!mine) fail();
     }
-    if (!ok) break;
-    // the run's last step completes row y1
-    const int b = (k - 1) & 1;
-    const bool mine = __all_sync(0xffffffffu, wait_buf(b));
-    if (mine) readout(y1, v);
-    if (mine) epilogue(zrow + y1, v);
+    k0 += nsteps;
     asm volatile("tcgen05.fence::before_thread_sync;");
     ok = __syncthreads_and(mine) != 0;
-    if (ok) { phase ^= 1u << b; inflight &= ~(1u << b); }
   }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
     // a wait ran out: give the MMAs still in flight one more bounded wait before
-    // the tensor memory they write is released
-    for (int bb = 0; bb < 2; ++bb)
-      if ((inflight >> bb) & 1u) mbar_wait(bar + bb, (phase >> bb) & 1u, kDefaultWaitLimit);
+    // the tensor memory they write is released (steps complete in order), and
+    // the row copies still in flight one before the CTA's shared memory is
+    if (tid == 0 && last_k >= 0) mbar_wait(cbar + (last_k & 3), uint32_t(last_k >> 2) & 1u, kDefaultWaitLimit);
+    if (tid == 32)
+      for (int q = 0; q < kSlots; ++q)
+        if ((tin >> q) & 1u) mbar_wait(staged + q, (spar >> q) & 1u, kDefaultWaitLimit);
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
+
+__global__ void k_set_flag(int* f) { *f = 1; }
 
 // input channels: u (3 physical FP32 fields) and the constant channel *z -> BF16 [n^3][16]
 __global__ void k_cnn_input(const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
@@ -569,7 +646,8 @@ k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restric
 // host side
 // ---------------------------------------------------------------------------
 template <int KN, int CP, int COP, int MODE> static size_t conv_smem() {
-  return size_t(3 * kSlots) * (CP / 8) * row_plane<KN>() + size_t(27) * (CP / 8) * COP * 16 + 32;
+  // + the mbarriers (4 steps, 2 x kSlots rows, 6 blocks), the TMEM slot and the abort flag
+  return size_t(3 * kSlots) * (CP / 8) * row_plane<KN>() + size_t(27) * (CP / 8) * COP * 16 + 192;
 }
 
 template <int KN, int CP, int COP, int MODE> static void conv_attr() {
@@ -580,7 +658,19 @@ template <int KN, int CP, int COP, int MODE> static void conv_attr() {
 template <int KN, int CP, int COP, int MODE>
 static void conv_launch(int grid, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* b, const ConvOut& o,
                         int* err, long long wait_limit, cudaStream_t st) {
-  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(in, w, b, o, err,
+  // one map per 8-channel chunk of the BF16 channels-last input [z][y][x][CP]:
+  // dims (8 channels, x, y, z), boxes of 8 channels x (KN + 2) voxels of one row
+  ConvMaps maps{};
+  const unsigned long long dims[4] = {8, KN, KN, KN};
+  const unsigned long long str[3] = {CP * 2ull, KN * CP * 2ull, (unsigned long long)KN * KN * CP * 2ull};
+  const unsigned box[4] = {8, KN + 2, 1, 1};
+  bool enc = true;
+  for (int c = 0; c < CP / 8; ++c) enc = enc && tma_encode_bf16_4d(&maps.m[c], in + 8 * c, dims, str, box);
+  if (!enc) {  // no tensor-map encoder: report it through the closure's error flag
+    k_set_flag<<<1, 1, 0, st>>>(err);
+    return;
+  }
+  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(maps, w, b, o, err,
                                                                                          wait_limit);
 }
 

@@ -55,6 +55,20 @@ struct CnnBwdArgs {
   long long wait_limit;
 };
 
+// An encoded tensor map (CUtensorMap, 128 bytes) for the bulk tensor copies
+// that stage the convolutions' input rows; one per 8-channel chunk.
+struct alignas(64) TmaMap {
+  unsigned char b[128];
+};
+struct ConvMaps {
+  TmaMap m[4];
+};
+// Encodes a 4D BF16 tiled tensor map (dims innermost first, strides of dims
+// 1..3 in bytes); false when the driver entry point or the encoding fails.
+// Implemented beside the column sweeps' maps (sc_coltma.cu).
+bool tma_encode_bf16_4d(TmaMap* map, const void* base, const unsigned long long dims[4],
+                        const unsigned long long strides[3], const unsigned box[4]);
+
 bool cnn_supported(int n, int D);
 void cnn_init();
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st);

@@ -283,6 +283,20 @@ bool launch_cfg(bool inv, const ColArgs& a, const float2* tw, cudaStream_t st) {
 
 }  // namespace
 
+bool tma_encode_bf16_4d(TmaMap* map, const void* base, const unsigned long long dims[4],
+                        const unsigned long long strides[3], const unsigned box[4]) {
+  static_assert(sizeof(CUtensorMap) == sizeof(TmaMap), "tensor map size");
+  const EncodeTiled enc = encode_fn();
+  if (!enc || (reinterpret_cast<uintptr_t>(base) & 15)) return false;
+  const cuuint64_t gdim[4] = {dims[0], dims[1], dims[2], dims[3]};
+  const cuuint64_t gstr[3] = {strides[0], strides[1], strides[2]};
+  const cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(reinterpret_cast<CUtensorMap*>(map), CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), gdim,
+             gstr, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool colt_init() { return set_attr<8, 2>() && set_attr<16, 2>() && set_attr<8, 3>(); }
 
 // Launches TMA-fed sweep configuration `which` (0: T = 8 with two stages and two
