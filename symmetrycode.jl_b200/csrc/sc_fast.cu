@@ -1077,11 +1077,86 @@ template <int N> static void init_xplain() {
   set_smem2(k_xr2c_fast<N>, XPFCfg<N>::SMEM);
 }
 
+// ---------------------------------------------------------------------------
+// x c2r for N = 64 and 128 with one warp per packed row pair, in registers
+// ---------------------------------------------------------------------------
+// Z[f] = X_a[f] + i X_b[f] (the Hermitian extensions of two real rows' half
+// spectra); lane l holds Z[l + 32 q], q < Q = N / 32.  A radix-Q inverse DFT
+// over q and the twiddles exp(+2 pi i l k1 / N) in registers, then for each
+// k1 a 32-point inverse DFT across the lanes (five radix-2 decimation-in-
+// frequency stages on warp shuffles), which leaves X[k1 + Q k2] with k2 the
+// 5-bit reversal of the lane: x_a = Re, x_b = Im.  No shared memory and no
+// CTA barrier; each warp's loads of a row are one or two 128-byte lines.
+template <int N>
+__global__ void __launch_bounds__(256) k_xc2r_warp(const XPlainArgs a, const float2* __restrict__ tw) {
+  constexpr int Q = N / 32;
+  const int lane = threadIdx.x & 31;
+  const int pen = int(blockIdx.x) * 8 + (threadIdx.x >> 5);
+  const int npair = (a.ncomp + 1) / 2, K1 = a.K1, kmax = K1 - 1;
+  if (pen >= int(a.nrows) * npair) return;  // whole warps leave together
+  const int row = pen / npair, pr = pen - row * npair;
+  const float2* ra = static_cast<const float2*>(a.in[2 * pr]) + row * K1;
+  const float2* rb = 2 * pr + 1 < a.ncomp ? static_cast<const float2*>(a.in[2 * pr + 1]) + row * K1 : nullptr;
+  auto hext = [&](const float2* r, int f) -> float2 {
+    if (!r) return make_float2(0.f, 0.f);
+    if (f == 0) return make_float2(__ldg(&r[0].x), 0.f);
+    if (f <= kmax) {
+      float2 v = __ldg(&r[f]);
+      if (2 * f == N) v.y = 0.f;
+      return v;
+    }
+    if (f >= N - kmax) { const float2 v = __ldg(&r[N - f]); return make_float2(v.x, -v.y); }
+    return make_float2(0.f, 0.f);
+  };
+  float2 v[Q];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) {
+    const int f = lane + 32 * q;
+    const float2 x = hext(ra, f), y = hext(rb, f);
+    v[q] = make_float2(x.x - y.y, x.y + y.x);
+  }
+  DFT<Q, true, float2>::run(v);
+#pragma unroll
+  for (int k1 = 1; k1 < Q; ++k1) {
+    const float2 w = __ldg(&tw[lane * k1]);  // exp(-2 pi i lane k1 / N), conjugated below
+    v[k1] = cmul(v[k1], make_float2(w.x, -w.y));
+  }
+#pragma unroll
+  for (int h = 16; h >= 1; h >>= 1) {
+    const bool hi = (lane & h) != 0;
+    // exp(+2 pi i (lane mod h) (16 / h) / 32) = conj(tw[(lane mod h) (16 / h) Q])
+    const float2 w = __ldg(&tw[(lane & (h - 1)) * (16 / h) * Q]);
+#pragma unroll
+    for (int k1 = 0; k1 < Q; ++k1) {
+      const float ux = __shfl_xor_sync(0xffffffffu, v[k1].x, h);
+      const float uy = __shfl_xor_sync(0xffffffffu, v[k1].y, h);
+      if (!hi) {
+        v[k1] = make_float2(v[k1].x + ux, v[k1].y + uy);
+      } else {
+        v[k1] = cmul(make_float2(ux - v[k1].x, uy - v[k1].y), make_float2(w.x, -w.y));
+      }
+    }
+  }
+  const int k2 = __brev(unsigned(lane)) >> 27;
+  const float sc = float(a.scale);
+  float* oa = static_cast<float*>(a.out[2 * pr]) + row * N;
+  float* ob = 2 * pr + 1 < a.ncomp ? static_cast<float*>(a.out[2 * pr + 1]) + row * N : nullptr;
+#pragma unroll
+  for (int k1 = 0; k1 < Q; ++k1) {
+    oa[k1 + Q * k2] = v[k1].x * sc;
+    if (ob) ob[k1 + Q * k2] = v[k1].y * sc;
+  }
+}
+
 template <int N> static void xplain_n(bool inv, const XPlainArgs& a, const void* tw, cudaStream_t st) {
   using Cfg = XPFCfg<N>;
   const long long npen = a.nrows * ((a.ncomp + 1) / 2);
   const unsigned nb = unsigned((npen + Cfg::TP - 1) / Cfg::TP);
   const float2* t2 = static_cast<const float2*>(tw);
+  if (inv && (N == 64 || N == 128)) {
+    k_xc2r_warp<N == 64 ? 64 : 128><<<unsigned((npen + 7) / 8), 256, 0, st>>>(a, t2);
+    return;
+  }
   if (inv) k_xc2r_fast<N><<<nb, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
   else k_xr2c_fast<N><<<nb, Cfg::NT, Cfg::SMEM, st>>>(a, t2);
 }
