@@ -22,7 +22,7 @@
 // rows high, so a tile is 3 (compact inverse input, 541 rows) or 4 (810 rows)
 // boxes.  Rows past the end of the axis and the kx past K1 are filled with
 // zeros by the copy engine.  Only plain per-CTA loads of this GPU's own
-// memory are issued (no cluster multicast).
+// memory are issued, each into the issuing CTA's shared memory.
 //
 // Every mbarrier wait is bounded (SC_OPT_WAIT_LIMIT polls): when thread 0's
 // wait runs out, the CTA sets the plan's error word, waits with the default
