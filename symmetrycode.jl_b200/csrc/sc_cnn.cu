@@ -275,11 +275,6 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
   auto arrive = [](uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
   };
-  // number of r in [lo, hi) with (r + off) mod m == j
-  auto count_mod = [](int lo, int hi, int j, int m, int off) -> int {
-    const int r0 = lo + (((j - (lo + off)) % m) + m) % m;
-    return r0 < hi ? (hi - 1 - r0) / m + 1 : 0;
-  };
   // tensor-memory block of output row y (y >= -2); blocks 0 and 1 also
   // accumulate in their stand-ins 6 and 7
   auto acc_blk = [](int y) -> int { return ((y % 6) + 6) % 6; };
@@ -373,8 +368,8 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
   const int rbeg = blockIdx.x * per;
   const int rend = min(rbeg + per, nrows);
   int k0 = 0;                    // global index of the run's first step (step k on cbar[k % 4])
-  int rbase[kSlots] = {};        // thread 0: earlier stagings of each ring slot
-  int zbase[6] = {};             // thread 0: earlier read-outs of each accumulator block
+  uint32_t rpar = 0;             // thread 0: bit s, parity of the next wait on ready[s]
+  uint32_t zpar = 0;             // thread 0: bit b, parity of the next wait on zeroed[b]
   int last_k = -1;               // thread 0: last committed step
   float v[16];
   for (int r0 = rbeg; r0 < rend && ok;) {
@@ -398,10 +393,13 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
       for (int i = 0; i < nsteps && mine; ++i) {
         const int yv = y0 - 1 + i, kk = k0 + i;
         const int sl = slot_of(yv);
-        mine = wait(ready + sl, uint32_t(rbase[sl] + count_mod(y0 - 1, yv, sl, kSlots, KN)) & 1u);
+        // every staged row is waited for once, in order
+        mine = wait(ready + sl, (rpar >> sl) & 1u);
+        rpar ^= 1u << sl;
         if (mine && yv >= y0 + 3) {  // the block of row yv + 1 held row yv - 5 of this run
-          const int q = yv - 5, bq = acc_blk(q);
-          mine = wait(zeroed + bq, uint32_t(zbase[bq] + count_mod(y0 - 2, q, bq, 6, 0)) & 1u);
+          const int bq = acc_blk(yv - 5);
+          mine = wait(zeroed + bq, (zpar >> bq) & 1u);
+          zpar ^= 1u << bq;
         }
         if (!mine) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -420,8 +418,10 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
         last_k = kk;
       }
       if (!mine) fail();
-      for (int j = 0; j < kSlots; ++j) rbase[j] += count_mod(y0 - 1, y1 + 2, j, kSlots, KN);
-      for (int j = 0; j < 6; ++j) zbase[j] += count_mod(y0 - 2, y1 + 1, j, 6, 0);
+      // read-outs of this run no step waited for (rows y1 - 3 .. y1, or the
+      // whole run if it is short): their phases complete before the run-end
+      // barrier, so they are counted here without a wait
+      for (int r = max(y0 - 2, y1 - 3); r <= y1; ++r) zpar ^= 1u << acc_blk(r);
     } else if (warp == 1) {
       // staging: complete row y0 - 1, then per step
       // (a copy whose wait ran out stays recorded in flight for the exit path)
