@@ -52,14 +52,14 @@ __host__ __device__ constexpr uint32_t make_idesc() {
   return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(NOUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
-  uint32_t mask[4] = {0, 0, 0, 0};
+// D += A B (the accumulators are zeroed in tensor memory beforehand), no lanes masked
+__device__ __forceinline__ void mma_bf16_acc(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
       :
-      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(mask[0]), "r"(mask[1]), "r"(mask[2]), "r"(mask[3]));
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(1u));
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -390,6 +390,8 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
     bool mine = true;
     if (tid == 0) {
       // MMA issue
+      const uint64_t DA0 = make_desc(smem_u32(s_in), kRowPlane, 128);
+      const uint64_t DB0 = make_desc(smem_u32(s_w), NS * 16, 128);
       for (int i = 0; i < nsteps && mine; ++i) {
         const int yv = y0 - 1 + i, kk = k0 + i;
         const int sl = slot_of(yv);
@@ -403,8 +405,6 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
         }
         if (!mine) break;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint64_t DA0 = make_desc(smem_u32(s_in), kRowPlane, 128);
-        const uint64_t DB0 = make_desc(smem_u32(s_w), NS * 16, 128);
         const uint32_t sa = uint32_t(sl) * (PLANE_ROW >> 4);
         const uint32_t dcol = tmem + uint32_t(acc_blk(yv - 1) * COP);  // rows yv - 1, yv, yv + 1
 #pragma unroll
@@ -412,7 +412,7 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
           const int dz = g / (3 * (CPC / 2)), dx = (g / (CPC / 2)) % 3, h = g % (CPC / 2);
           const uint64_t da = DA0 + sa + uint32_t(dz * kSlots * (PLANE_ROW >> 4) + dx + 2 * h * (kRowPlane >> 4));
           const uint64_t db = DB0 + uint32_t(((dz * 3 + dx) * CPC + 2 * h) * NS);
-          mma_bf16(dcol, da, db, IDESC, 1u);
+          mma_bf16_acc(dcol, da, db, IDESC);
         }
         mma_commit(cbar + (kk & 3));
         last_k = kk;
