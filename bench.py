@@ -524,9 +524,11 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
     Delta/h = 4), CNN closure, nsteps-step RK4 rollout checkpointed every ck
     steps, trajectory-MSE loss against a target rollout of the perturbed closure
     (weights x (1 + 0.01 N(0,1))), gradient by the hand-written adjoint.
-    Batched: FP32 with the tensor-core CNN (BF16 convolutions, FP32 accumulate;
-    the adjoint takes the BF16 roundings as identities), the 8 jobs
-    concurrently (sc_rollout_adjoint_batch).  Plain: the per-instance FP64
+    Batched: FP32 with the tensor-core CNN in split precision (three passes
+    over hi/lo operand parts per convolution, FP32 accumulate), the 8 jobs
+    concurrently (sc_rollout_adjoint_batch); beside it the same with one BF16
+    pass per convolution (the adjoint takes the BF16 roundings as identities)
+    and with the CNN on CUDA cores in FP32.  Plain: the per-instance FP64
     path (the same network on CUDA cores in FP64), one instance after another
     (plain_instances of them timed, per-instance time reported)."""
     import numpy as np
@@ -547,14 +549,16 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
         gl.close()
     gd.close()
 
-    def make(dtype, idx, tensor_cores=True):
+    def make(dtype, idx, tensor_cores=True, split=False):
         jobs = []
         for i in idx:
             nu = ADJ_NU[i % 2]
             g = S.Grid(3, ADJ_N, dtype=dtype, device=dev)
             u0 = [c.to(g.cdtype).contiguous() for c in fields[i // 2]]
-            make = S.create_cnn_closure if (dtype == torch.float32 and tensor_cores) else S.create_cnn_fp_closure
-            cl = make(ADJ_DH * g.l / ADJ_N, nu, g, ws, bs, mu=5.0, sigma=2.0)
+            if dtype == torch.float32 and tensor_cores:
+                cl = S.create_cnn_closure(ADJ_DH * g.l / ADJ_N, nu, g, ws, bs, mu=5.0, sigma=2.0, split=split)
+            else:
+                cl = S.create_cnn_fp_closure(ADJ_DH * g.l / ADJ_N, nu, g, ws, bs, mu=5.0, sigma=2.0)
             rng = np.random.default_rng(ADJ_SEED * 100 + i)
             S.closure_set_params(cl, theta * (1 + 0.01 * rng.standard_normal(theta.size)))
             traj = S.rollout_record(g, cl, u0, ADJ_DT, nu, nsteps)
@@ -562,8 +566,8 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
             jobs.append(dict(grid=g, closure=cl, u0=u0, traj=traj, dt=ADJ_DT, visc=nu, nsteps=nsteps, ckpt_every=ck))
         return jobs
 
-    def run_batch(tensor_cores, njobs=8, warm=True):
-        jobs = make(torch.float32, range(njobs), tensor_cores)
+    def run_batch(tensor_cores, njobs=8, warm=True, split=False):
+        jobs = make(torch.float32, range(njobs), tensor_cores, split)
         if warm:
             S.rollout_adjoint_batch(jobs)  # warm-up
         torch.cuda.synchronize()
@@ -579,6 +583,8 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
         return res, t
 
     res32, t_batch = run_batch(True)
+    # the tensor-core CNN in split precision (three passes over hi/lo parts per convolution)
+    res_sp, t_batch_sp = run_batch(True, split=True)
     # the CUDA-core FP32 closure: 4 of the 8 jobs, one timed batch (about a minute)
     ncc = 4
     res32cc, t_batch_cc = run_batch(False, ncc, warm=False)
@@ -594,31 +600,44 @@ def les_adjoint_measure(dev, nsteps, ck, plain_instances=2):
             for i in range(plain_instances)]
     errs_cc = [float(np.linalg.norm(res32cc[i][1] - res64[i][1]) / np.linalg.norm(res64[i][1]))
                for i in range(plain_instances)]
+    errs_sp = [float(np.linalg.norm(res_sp[i][1] - res64[i][1]) / np.linalg.norm(res64[i][1]))
+               for i in range(plain_instances)]
     for j in jobs64:
         j["closure"].close()
         j["grid"].close()
     torch.cuda.empty_cache()
     return {
         "metric": "batched LES+adjoint steps/s (8 x 64^3 training rollouts: forward, loss and adjoint per step)",
-        "value": 8 * nsteps / t_batch, "unit": "steps/s", "s_per_training_step": t_batch,
+        "what": "the 8 jobs batched on the tensor cores in split precision (SC_CLOPT_CNN_SPLIT): each convolution "
+                "three tcgen05 passes A_hi W_hi + A_lo W_hi + A_hi W_lo over FP16 (forward) or BF16 (input "
+                "gradient) hi/lo operand parts, FP32 accumulation, GELU with tanhf; weight gradients on CUDA cores",
+        "value": 8 * nsteps / t_batch_sp, "unit": "steps/s", "s_per_training_step": t_batch_sp,
         "plain_fp64_steps_per_s": nsteps / t_plain, "plain_fp64_s_per_instance": t_plain,
-        "speedup_vs_plain": (8 * t_plain) / t_batch,
-        "grad_rel_err_fp32_vs_fp64": errs,
-        "losses": [r[0] for r in res32],
+        "speedup_vs_plain": (8 * t_plain) / t_batch_sp,
+        "grad_rel_err_fp32_vs_fp64": errs_sp,
+        "gradient_bar": 1e-4,
+        "losses": [r[0] for r in res_sp],
+        "bf16_one_pass": {
+            "what": "the same batched training step with one BF16 tcgen05 pass per convolution (the closure's "
+                    "default precision); its gradient error against FP64 is dominated by the BF16 rounding of "
+                    "weights and activations, which is comparable to the 1 % weight perturbation",
+            "value": 8 * nsteps / t_batch, "unit": "steps/s", "s_per_training_step": t_batch,
+            "speedup_vs_plain": (8 * t_plain) / t_batch,
+            "grad_rel_err_fp32_vs_fp64": errs,
+            "losses": [r[0] for r in res32]},
         "fp32_cuda_cores": {
-            "what": "the same batched training step with the CNN on CUDA cores in FP32 (no BF16 rounding): the "
-                    "path whose gradient matches FP64",
+            "what": "the same batched training step with the CNN on CUDA cores in FP32",
             "jobs": ncc, "value": ncc * nsteps / t_batch_cc, "unit": "steps/s",
             "s_per_training_step_of_8": t_batch_cc * 8 / ncc,
             "speedup_vs_plain": (ncc * t_plain) / t_batch_cc,
             "grad_rel_err_fp32_vs_fp64": errs_cc},
         "config": f"64^3, nu in {list(ADJ_NU)}, Delta/h={ADJ_DH}, RK4 dt={ADJ_DT}, {nsteps} steps, checkpoint every "
                   f"{ck}; CNN closure (4 layers 3x3x3, 32 channels, GELU, seeded Kaiming weights): batched on "
-                  "tcgen05 BF16 (forward and input-gradient convolutions; weight gradients on CUDA cores in FP32), "
-                  "plain on CUDA cores in FP64; target rollout of the closure with weights x (1 + 0.01 N(0,1)); "
-                  "the gradient error against FP64 is dominated by the BF16 rounding of weights and activations, "
-                  "which is comparable to that 1 % perturbation; initial fields sfs! of seeded 128^3 fields; "
-                  "host wall clock around the synchronous calls",
+                  "tcgen05 (forward and input-gradient convolutions; weight gradients on CUDA cores in FP32), "
+                  "plain on CUDA cores in FP64 one instance after another; target rollout of the closure with "
+                  "weights x (1 + 0.01 N(0,1)); initial fields sfs! of seeded 128^3 fields; gradient errors of the "
+                  f"first {plain_instances} jobs against the plain FP64 path's; host wall clock around the "
+                  "synchronous calls",
     }
 
 

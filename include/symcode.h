@@ -230,6 +230,22 @@ SC_API int sc_closure_num_params(const sc_closure* closure, long long* nparams);
 SC_API int sc_closure_set_params(sc_closure* closure, const double* theta);
 /* Synchronous: SC_ERR_TIMEOUT if a bounded wait of the closure's kernels ran out. */
 SC_API int sc_closure_status(sc_closure* closure, int* status);
+/* Closure options (no reference counterpart; the reference's networks run in
+ * the precision of their weights).  SC_CLOPT_CNN_SPLIT (tensor-core CNN
+ * closure only): 1 evaluates every convolution as three tcgen05 passes over
+ * split operands, x = hi + lo with hi the nearest 16-bit number to x and lo the
+ * nearest to x - hi, A_hi W_hi + A_lo W_hi + A_hi W_lo accumulated in FP32 (FP16
+ * parts in the forward pass, weights stored x 64 so that their low parts stay
+ * normal FP16 numbers; BF16 parts for the adjoint's input-gradient
+ * convolutions, whose gradients need BF16's exponent range), with GELU from
+ * tanhf and the weight gradients from the hi + lo sums: about FP32 accuracy at
+ * three times the convolutions' tensor-core work.  0 (default): BF16 operands,
+ * one pass.  SC_ERR_INVALID when a weight x 64 is beyond the FP16 range.
+ * Allocates the split activations on the first switch; cached step graphs of
+ * the closure's plan are rebuilt (LES batches and graphs captured by the caller
+ * keep the precision they were captured with). */
+#define SC_CLOPT_CNN_SPLIT 1
+SC_API int sc_closure_set_option(sc_closure* closure, int option, long long value);
 /* model(u, G): the packed physical stress tau (3|6 fields, pair order) from
  * the spectral velocity u_hat (full layout) and the physical velocity
  * gradient G (D*D fields, G[a + D b] = d u_a / d x_b; Clark, Smagorinsky and

@@ -113,6 +113,17 @@ struct sc_closure {
   void* tpre[3] = {};           // adjoint: FP32 pre-activations
   void* tgbf = nullptr;         // adjoint: BF16 gradient scratch
   void* tgf = nullptr;          // adjoint: FP32 gradient scratch
+  // split precision (SC_CLOPT_CNN_SPLIT): FP16 hi/lo forward weights (x kSplitScale),
+  // BF16 low parts of the transposed weights, FP16 hi/lo activations, FP32 accumulator
+  bool cnn_split = false;
+  bool split_fits = true;       // the uploaded weights x kSplitScale are FP16 numbers
+  void* cwh[4] = {};
+  void* cwl[4] = {};
+  void* cwtl[4] = {};
+  void* sacth[4] = {};
+  void* sactl[4] = {};
+  void* sacc = nullptr;
+  void* tgbfl = nullptr;        // adjoint: BF16 gradient scratch, low parts
   int* err = nullptr;
   double nu = 0, mu = 0, sigma = 1;
   // CUDA-core CNN (FP32/FP64): weights, activations a0 h1 a1 h2 a2 h3 a3, tau, gradients
@@ -510,6 +521,19 @@ sc::MlpArgs mlp_args(sc_closure* cl, const void* const* G, void* const* tau) {
   return a;
 }
 
+// The split-precision fields of a forward pass (pre[] as the caller set it).
+void tc_split_args(const sc_closure* cl, sc::CnnArgs& a) {
+  if (!cl->cnn_split) return;
+  a.split = true;
+  for (int l = 0; l < 4; ++l) {
+    a.wh[l] = static_cast<const __half*>(cl->cwh[l]);
+    a.wl[l] = static_cast<const __half*>(cl->cwl[l]);
+    a.acth[l] = static_cast<__half*>(cl->sacth[l]);
+    a.actl[l] = static_cast<__half*>(cl->sactl[l]);
+  }
+  a.acc = static_cast<float*>(cl->sacc);
+}
+
 // Tensor-core CNN for the adjoint: forward at u keeping every layer input and
 // the pre-activations (v in gp[0..2], tau in tp), and backward from dL/dtau
 // (planar FP32 in cctau) to dL/dv (ccg0[0..2]), dL/dz (dsum[1]) and the
@@ -539,6 +563,7 @@ int tc_forward(sc_closure* cl, void* const* u, cudaStream_t st) {
   a.err = cl->err;
   a.nsm = num_sms_api();
   a.wait_limit = p->wait_limit;
+  tc_split_args(cl, a);
   sc::launch_cnn_forward(a, st);
   return check_launch("cnn forward (tensor cores, adjoint)");
 }
@@ -563,6 +588,15 @@ int tc_backward(sc_closure* cl, cudaStream_t st) {
   b.err = cl->err;
   b.nsm = num_sms_api();
   b.wait_limit = p->wait_limit;
+  if (cl->cnn_split) {
+    b.split = true;
+    for (int l = 0; l < 4; ++l) {
+      b.wtl[l] = static_cast<const __nv_bfloat16*>(cl->cwtl[l]);
+      b.acth[l] = static_cast<const __half*>(cl->sacth[l]);
+      b.actl[l] = static_cast<const __half*>(cl->sactl[l]);
+    }
+    b.gbf_lo = static_cast<__nv_bfloat16*>(cl->tgbfl);
+  }
   sc::launch_cnn_backward(b, st);
   SC_CU(cudaMemsetAsync(cl->dsum + 1, 0, sizeof(double), st));
   sc::launch_sum<float>(static_cast<const float*>(cl->ccg0) + 3 * np, np, cl->dsum + 1, st);
@@ -684,6 +718,7 @@ int closure_tauhat(sc_closure* cl, void* const* u, cudaStream_t st, void* const*
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     a.nsm = nsm;
     a.wait_limit = p->wait_limit;
+    tc_split_args(cl, a);
     sc::launch_cnn_forward(a, st);
     if ((rc = check_launch("cnn closure"))) return rc;
   } else if (cl->kind == sc::kCnnFp) {
@@ -1437,6 +1472,13 @@ static uint16_t host_bf16(float f) {
   return uint16_t(x >> 16);
 }
 
+static float host_bf16_value(uint16_t b) {
+  const uint32_t x = uint32_t(b) << 16;
+  float f;
+  std::memcpy(&f, &x, 4);
+  return f;
+}
+
 }  // extern "C"
 
 namespace {
@@ -1448,16 +1490,30 @@ namespace {
 int tc_upload_params(sc_closure* cl, const double* theta) {
   static const int cin[4] = {4, 32, 32, 32}, cout[4] = {32, 32, 32, 6}, cp[4] = {16, 32, 32, 32},
                    cop[4] = {32, 32, 32, 16};
+  bool fits = true;  // every weight x kSplitScale is an FP16 number
   for (int l = 0; l < 4; ++l) {
     const long long o = cc_layer_offset(l), nw = (long long)cout[l] * cin[l] * 27;
     const int cpc = cp[l] / 8;
-    std::vector<uint16_t> wp((size_t)27 * cp[l] * cop[l], 0), wt((size_t)27 * cp[l] * cop[l], 0);
+    const size_t nwp = (size_t)27 * cp[l] * cop[l];
+    // BF16 forward and transposed weights; for the split precision also the
+    // FP16 high and low parts of theta x kSplitScale (forward) and the BF16
+    // low parts theta - bf16(theta) of the transposed weights
+    std::vector<uint16_t> wp(nwp, 0), wt(nwp, 0), wh(nwp, 0), wl(nwp, 0), wtl(nwp, 0);
     for (int t = 0; t < 27; ++t)
       for (int kc = 0; kc < cpc; ++kc)
         for (int nn = 0; nn < cout[l]; ++nn)
           for (int j = 0; j < 8; ++j) {
             const int ci = 8 * kc + j;
-            if (ci < cin[l]) wp[(((size_t)t * cpc + kc) * cop[l] + nn) * 8 + j] = host_bf16(float(theta[o + ((long long)nn * cin[l] + ci) * 27 + t]));
+            if (ci >= cin[l]) continue;
+            const double x = theta[o + ((long long)nn * cin[l] + ci) * 27 + t];
+            const size_t d = (((size_t)t * cpc + kc) * cop[l] + nn) * 8 + j;
+            wp[d] = host_bf16(float(x));
+            const double xs = x * double(sc::kSplitScale);
+            if (!(std::fabs(xs) < 6.5e4)) fits = false;
+            const __half hh = __float2half_rn(float(xs));
+            const __half hl = __float2half_rn(float(xs - double(__half2float(hh))));
+            std::memcpy(&wh[d], &hh, 2);
+            std::memcpy(&wl[d], &hl, 2);
           }
     const int cpc2 = cop[l] / 8;  // input-gradient convolution: CP' = cop, COP' = cp
     for (int t2 = 0; t2 < 27; ++t2)
@@ -1465,16 +1521,23 @@ int tc_upload_params(sc_closure* cl, const double* theta) {
         for (int nn = 0; nn < cin[l]; ++nn)
           for (int j = 0; j < 8; ++j) {
             const int k = 8 * kc + j;  // a forward output channel
-            if (k < cout[l])
-              wt[(((size_t)t2 * cpc2 + kc) * cp[l] + nn) * 8 + j] =
-                  host_bf16(float(theta[o + ((long long)k * cin[l] + nn) * 27 + (26 - t2)]));
+            if (k >= cout[l]) continue;
+            const double x = theta[o + ((long long)k * cin[l] + nn) * 27 + (26 - t2)];
+            const size_t d = (((size_t)t2 * cpc2 + kc) * cp[l] + nn) * 8 + j;
+            wt[d] = host_bf16(float(x));
+            wtl[d] = host_bf16(float(x - double(host_bf16_value(wt[d]))));
           }
     std::vector<float> bp(cop[l], 0.f);
     for (int nn = 0; nn < cout[l]; ++nn) bp[nn] = float(theta[o + nw + nn]);
     SC_CU(cudaMemcpy(cl->cw[l], wp.data(), wp.size() * 2, cudaMemcpyHostToDevice));
     SC_CU(cudaMemcpy(cl->cwt[l], wt.data(), wt.size() * 2, cudaMemcpyHostToDevice));
+    SC_CU(cudaMemcpy(cl->cwh[l], wh.data(), wh.size() * 2, cudaMemcpyHostToDevice));
+    SC_CU(cudaMemcpy(cl->cwl[l], wl.data(), wl.size() * 2, cudaMemcpyHostToDevice));
+    SC_CU(cudaMemcpy(cl->cwtl[l], wtl.data(), wtl.size() * 2, cudaMemcpyHostToDevice));
     SC_CU(cudaMemcpy(cl->cbias[l], bp.data(), bp.size() * 4, cudaMemcpyHostToDevice));
   }
+  cl->split_fits = fits;
+  if (cl->cnn_split && !fits) return fail(SC_ERR_INVALID, "a CNN weight is beyond the FP16 range of the split precision");
   return SC_OK;
 }
 
@@ -1493,7 +1556,28 @@ int tc_adjoint_buffers(sc_closure* cl) {
   if (!rc) rc = A(&cl->tgbf, np * 32 * 2);
   if (!rc) rc = A(&cl->cctau, np * 6 * 4);
   if (!rc) rc = A(&cl->ccg0, np * 4 * 4);
+  if (!rc) rc = A(&cl->tgbfl, np * 32 * 2);
   if (!rc) rc = A(&cl->tgf, np * 32 * 4);  // last: marks the set complete
+  return rc;
+}
+
+// the split precision's activation buffers, on first use
+int tc_split_buffers(sc_closure* cl) {
+  if (cl->sacc) return SC_OK;
+  const size_t np = (size_t)cl->p->n * cl->p->n * cl->p->n;
+  auto A = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(SC_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e)); }
+    cl->allocs.push_back(*ptr);
+    return SC_OK;
+  };
+  int rc = SC_OK;
+  for (int l = 0; l < 4 && !rc; ++l) {
+    const size_t ch = l == 0 ? 16 : 32;
+    rc = A(&cl->sacth[l], np * ch * 2);
+    if (!rc) rc = A(&cl->sactl[l], np * ch * 2);
+  }
+  if (!rc) rc = A(&cl->sacc, np * 32 * 4);  // last: marks the set complete
   return rc;
 }
 }  // namespace
@@ -1527,6 +1611,9 @@ int sc_cnn_closure_create(sc_closure** out, sc_plan* p, double delta, double vis
     const size_t nwp = (size_t)27 * cp[l] * cop[l];
     rc = A(&cl->cw[l], nwp * 2);
     if (!rc) rc = A(&cl->cwt[l], nwp * 2);
+    if (!rc) rc = A(&cl->cwh[l], nwp * 2);
+    if (!rc) rc = A(&cl->cwl[l], nwp * 2);
+    if (!rc) rc = A(&cl->cwtl[l], nwp * 2);
     if (!rc) rc = A(&cl->cbias[l], cop[l] * 4);
   }
   if (!rc) rc = A(&cl->act[0], npts * 16 * 2);
@@ -1690,6 +1777,27 @@ int sc_closure_set_params(sc_closure* cl, const double* theta) {
     }
   }
   // cached step graphs captured the old weights by pointer, which stay valid
+  return SC_OK;
+}
+
+int sc_closure_set_option(sc_closure* cl, int option, long long value) {
+  if (!cl) return fail(SC_ERR_INVALID, "null argument");
+  if (option != SC_CLOPT_CNN_SPLIT) return fail(SC_ERR_INVALID, "unknown closure option %d", option);
+  if (cl->kind != sc::kCnn)
+    return fail(SC_ERR_UNSUPPORTED, "the split precision is an option of the tensor-core CNN closure");
+  if (value != 0 && value != 1) return fail(SC_ERR_INVALID, "SC_CLOPT_CNN_SPLIT takes 0 or 1");
+  sc_plan* p = cl->p;
+  ensure_device(p);
+  if (value && !cl->split_fits)
+    return fail(SC_ERR_INVALID, "a CNN weight is beyond the FP16 range of the split precision");
+  if (value) {
+    const int rc = tc_split_buffers(cl);
+    if (rc) return rc;
+  }
+  cl->cnn_split = value != 0;
+  // cached step graphs hold the other precision's launches
+  if (p->g_rk4) { cudaGraphExecDestroy(p->g_rk4); p->g_rk4 = nullptr; }
+  if (p->g_wray) { cudaGraphExecDestroy(p->g_wray); p->g_wray = nullptr; }
   return SC_OK;
 }
 

@@ -45,11 +45,13 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
-template <int NOUT>
+template <int NOUT, bool F16 = false>
 __host__ __device__ constexpr uint32_t make_idesc() {
-  // kind::f16: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16 (10-12 = 1),
-  // both K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 128)
-  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(NOUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+  // kind::f16: D f32 (bits 4-5 = 1); A and B of one type, both bf16 (bits 7-9
+  // and 10-12 = 1) or both f16 (0); both K-major, N >> 3 at bit 17, M >> 4 at
+  // bit 24 (M = 128)
+  constexpr uint32_t ab = F16 ? 0u : 1u;
+  return (1u << 4) | (ab << 7) | (ab << 10) | (uint32_t(NOUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
 }
 
 // D += A B (the accumulators are zeroed in tensor memory beforehand), no lanes masked
@@ -123,6 +125,11 @@ __device__ __forceinline__ float gelu(float x) {
   const float u = 0.7978845608028654f * x * (1.f + 0.044715f * x * x);
   return 0.5f * x * (1.f + tanh_hw(u));
 }
+// the same with the library tanhf (a few ulp): the split precision's activation
+__device__ __forceinline__ float gelu_exact(float x) {
+  const float u = 0.7978845608028654f * x * (1.f + 0.044715f * x * x);
+  return 0.5f * x * (1.f + tanhf(u));
+}
 
 
 __device__ __forceinline__ float gelu_grad(float x) {
@@ -139,13 +146,22 @@ template <int KN> constexpr int row_plane() { return ((KN + 2) * 16 + 127) / 128
 
 // Epilogue modes: BF16 GELU activations; the same plus the FP32
 // pre-activations (kept for the adjoint); FP32 planar tau (last layer);
-// FP32 channels-last without bias or activation (the input-gradient convolution).
-enum { kGelu = 0, kGeluSave = 1, kTau = 2, kLinear = 3 };
+// FP32 channels-last without bias or activation (the input-gradient
+// convolution).  The split precision's passes: kLinear (first pass), kAccum
+// (the FP32 channels-last output += this pass), and the last pass kGeluSplit
+// (h = (this pass + the accumulated output) scale + bias, written back in
+// place as the pre-activation; GELU with tanhf; FP16 hi/lo activations) or
+// kTauSplit (tau = (this pass + accumulated) scale + bias, planar).
+enum { kGelu = 0, kGeluSave = 1, kTau = 2, kLinear = 3, kAccum = 4, kGeluSplit = 5, kTauSplit = 6 };
 
 struct ConvOut {
   __nv_bfloat16* act;  // kGelu, kGeluSave: BF16 channels-last [n^3][COP]
-  float* pre;          // kGeluSave: FP32 channels-last pre-activations; kLinear: FP32 channels-last output
-  TauPtrs tau;         // kTau
+  float* pre;          // kGeluSave: FP32 channels-last pre-activations; kLinear, kAccum: FP32 channels-last
+                       // output; kGeluSplit, kTauSplit: the accumulated passes (kGeluSplit writes h there)
+  TauPtrs tau;         // kTau, kTauSplit
+  __half* acth;        // kGeluSplit: FP16 channels-last activations, high parts
+  __half* actl;        // kGeluSplit: low parts (activation - high part, rounded to FP16)
+  float scale;         // kGeluSplit, kTauSplit: factor of the accumulated sum before the bias
 };
 
 // One convolution layer.  act_in: BF16 channels-last [n^3][CP]; weights:
@@ -188,7 +204,7 @@ struct ConvOut {
 constexpr int kSlots = 5;
 constexpr int kConvThreads = 384;
 
-template <int KN, int CP, int COP, int MODE>
+template <int KN, int CP, int COP, int MODE, bool F16>
 __global__ void __launch_bounds__(kConvThreads, 1)
 k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__ wgt,
         const float* __restrict__ bias, const ConvOut out, int* __restrict__ err, long long wait_limit) {
@@ -198,7 +214,7 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
   constexpr int SIN = 3 * kSlots * PLANE_ROW;  // [zr][slot] staged rows
   constexpr int NS = 3 * COP;              // stacked rows per k-chunk plane: the three dy taps
   constexpr int SW = 9 * CPC * NS * 16;
-  constexpr uint32_t IDESC = make_idesc<3 * COP>();
+  constexpr uint32_t IDESC = make_idesc<3 * COP, F16>();
   constexpr uint32_t kTmemCols = 8 * COP;  // eight accumulator blocks
   extern __shared__ __align__(128) unsigned char sm[];
   unsigned char* s_in = sm;
@@ -226,10 +242,11 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
     const int src = (((g / 3) * 9 + dyi * 3 + g % 3) * CPC + kc) * COP + co;
     reinterpret_cast<uint4*>(s_w)[d] = __ldg(reinterpret_cast<const uint4*>(wgt) + src);
   }
+  constexpr bool kBias = MODE == kGelu || MODE == kGeluSave || MODE == kTau || MODE == kGeluSplit || MODE == kTauSplit;
+  constexpr bool kTauOut = MODE == kTau || MODE == kTauSplit;
   float bia[16];
 #pragma unroll
-  for (int c = 0; c < 16; ++c)
-    bia[c] = (is_epi && MODE != kLinear && (MODE != kTau || c < 6)) ? __ldg(bias + ecol0 + c) : 0.f;
+  for (int c = 0; c < 16; ++c) bia[c] = (kBias && is_epi && (!kTauOut || c < 6)) ? __ldg(bias + ecol0 + c) : 0.f;
   if (tid == 0) {
     for (int q = 0; q < 4; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(cbar + q)));
     for (int q = 0; q < kSlots; ++q) {
@@ -316,6 +333,44 @@ k_conv3(const __grid_constant__ ConvMaps maps, const __nv_bfloat16* __restrict__
     } else if (MODE == kTau) {
 #pragma unroll
       for (int c = 0; c < 6; ++c) out.tau.p[c][vox] = v[c] + bia[c];
+    } else if (MODE == kTauSplit) {
+      const float4* pl = reinterpret_cast<const float4*>(out.pre + vox * COP);
+      const float4 p0 = pl[0], p1 = pl[1];
+      const float pv[6] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y};
+#pragma unroll
+      for (int c = 0; c < 6; ++c) out.tau.p[c][vox] = (v[c] + pv[c]) * out.scale + bia[c];
+    } else if (MODE == kGeluSplit) {
+      float4* pl = reinterpret_cast<float4*>(out.pre + vox * COP + ecol0);
+      __align__(16) __half hi[16];
+      __align__(16) __half lo[16];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float4 p = pl[j];
+        const float h[4] = {(v[4 * j] + p.x) * out.scale + bia[4 * j], (v[4 * j + 1] + p.y) * out.scale + bia[4 * j + 1],
+                            (v[4 * j + 2] + p.z) * out.scale + bia[4 * j + 2],
+                            (v[4 * j + 3] + p.w) * out.scale + bia[4 * j + 3]};
+        pl[j] = make_float4(h[0], h[1], h[2], h[3]);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float y = gelu_exact(h[e]);
+          const __half hh = __float2half_rn(y);
+          hi[4 * j + e] = hh;
+          lo[4 * j + e] = __float2half_rn(y - __half2float(hh));
+        }
+      }
+      uint4* dh = reinterpret_cast<uint4*>(out.acth + vox * COP + ecol0);
+      uint4* dl = reinterpret_cast<uint4*>(out.actl + vox * COP + ecol0);
+      dh[0] = reinterpret_cast<uint4*>(hi)[0];
+      dh[1] = reinterpret_cast<uint4*>(hi)[1];
+      dl[0] = reinterpret_cast<uint4*>(lo)[0];
+      dl[1] = reinterpret_cast<uint4*>(lo)[1];
+    } else if (MODE == kAccum) {
+      float4* pl = reinterpret_cast<float4*>(out.pre + vox * COP + ecol0);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float4 p = pl[j];
+        pl[j] = make_float4(p.x + v[4 * j], p.y + v[4 * j + 1], p.z + v[4 * j + 2], p.w + v[4 * j + 3]);
+      }
     } else {
       float4* pl = reinterpret_cast<float4*>(out.pre + vox * COP + ecol0);
 #pragma unroll
@@ -507,6 +562,32 @@ __global__ void k_cnn_input(const float* __restrict__ ux, const float* __restric
   dst[1] = reinterpret_cast<uint4*>(o)[1];
 }
 
+// the same input channels as FP16 high and low parts (split precision): hi = fp16(x), lo = fp16(x - hi)
+__device__ __forceinline__ void split_f16(float x, __half& hi, __half& lo) {
+  hi = __float2half_rn(x);
+  lo = __float2half_rn(x - __half2float(hi));
+}
+__global__ void k_cnn_input_split(const float* __restrict__ ux, const float* __restrict__ uy,
+                                  const float* __restrict__ uz, const double* __restrict__ z, __half* __restrict__ oh,
+                                  __half* __restrict__ ol, long long npts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  __align__(16) __half h[16];
+  __align__(16) __half l[16];
+  split_f16(ux[i], h[0], l[0]);
+  split_f16(uy[i], h[1], l[1]);
+  split_f16(uz[i], h[2], l[2]);
+  split_f16(float(*z), h[3], l[3]);
+#pragma unroll
+  for (int c = 4; c < 16; ++c) h[c] = l[c] = __float2half_rn(0.f);
+  uint4* dh = reinterpret_cast<uint4*>(oh + i * 16);
+  uint4* dl = reinterpret_cast<uint4*>(ol + i * 16);
+  dh[0] = reinterpret_cast<uint4*>(h)[0];
+  dh[1] = reinterpret_cast<uint4*>(h)[1];
+  dl[0] = reinterpret_cast<uint4*>(l)[0];
+  dl[1] = reinterpret_cast<uint4*>(l)[1];
+}
+
 // z = (log(Delta^2 sqrt(a2) / nu) - mu) / sigma   (Re_Delta channel, src/nets.jl:311-331 convention)
 __global__ void k_cnn_redelta(const double* a2, double* z, double delta, double nu, double mu, double sigma) {
   const double re = delta * delta * sqrt(*a2) / nu;
@@ -536,6 +617,33 @@ __global__ void k_gelu_bwd_cl(const float* __restrict__ gpost, const float* __re
   out[i] = __float2bfloat16_rn(gpost[i] * gelu_grad(h[i]));
 }
 
+// split precision: BF16 high and low parts, hi = bf16(x), lo = bf16(x - hi)
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+__global__ void k_gtau_cl_split(TauPtrs g, __nv_bfloat16* __restrict__ oh, __nv_bfloat16* __restrict__ ol,
+                                long long npts) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  __align__(16) __nv_bfloat16 h[16];
+  __align__(16) __nv_bfloat16 l[16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) split_bf16(c < 6 ? g.p[c][i] : 0.f, h[c], l[c]);
+  uint4* dh = reinterpret_cast<uint4*>(oh + i * 16);
+  uint4* dl = reinterpret_cast<uint4*>(ol + i * 16);
+  dh[0] = reinterpret_cast<uint4*>(h)[0];
+  dh[1] = reinterpret_cast<uint4*>(h)[1];
+  dl[0] = reinterpret_cast<uint4*>(l)[0];
+  dl[1] = reinterpret_cast<uint4*>(l)[1];
+}
+__global__ void k_gelu_bwd_cl_split(const float* __restrict__ gpost, const float* __restrict__ h,
+                                    __nv_bfloat16* __restrict__ oh, __nv_bfloat16* __restrict__ ol, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  split_bf16(gpost[i] * gelu_grad(h[i]), oh[i], ol[i]);
+}
+
 // FP32 channels-last [n^3][16] -> planar channels 0..3 (dL/dv and the z channel)
 __global__ void k_gin_planar(const float* __restrict__ gin, const GinPtrs o, long long npts) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -550,10 +658,13 @@ __global__ void k_gin_planar(const float* __restrict__ gin, const GinPtrs o, lon
 // for co < cout, ci < cin.  Block (tap t, chunk of voxels); a group of
 // (COP/4)(CP/4) threads holds a 4 x 4 (co, ci) register tile; the chunk's g
 // rows and shifted a rows are staged in shared memory 64 voxels at a time.
-template <int KN, int CP, int COP>
+// SPLIT: g = g + glo (BF16 high and low parts) and a = FP16 high + low parts
+// (a and alo of type __half); otherwise a is BF16 and glo, alo are unused.
+template <int KN, int CP, int COP, bool SPLIT>
 __global__ void __launch_bounds__(256)
-k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ a, int cin, int cout,
-             int vchunk, double* __restrict__ gw, double* __restrict__ gb) {
+k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ glo, const void* __restrict__ a,
+             const void* __restrict__ alo, int cin, int cout, int vchunk, double* __restrict__ gw,
+             double* __restrict__ gb) {
   constexpr int TG = (COP / 4) * (CP / 4);  // threads per group
   constexpr int NG = 256 / TG;              // groups (split the voxels of a stage)
   constexpr int VS = 64;                    // voxels per stage
@@ -577,7 +688,13 @@ k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restric
         const int vv = i / (COP / 2), c = 2 * (i % (COP / 2));
         const long long v = vb + vv;
         float2 f = make_float2(0.f, 0.f);
-        if (v < v1) f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(g + v * COP + c));
+        if (v < v1) {
+          f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(g + v * COP + c));
+          if (SPLIT) {
+            const float2 l = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(glo + v * COP + c));
+            f.x += l.x; f.y += l.y;
+          }
+        }
         sg[vv][c] = f.x; sg[vv][c + 1] = f.y;
       } else {
         const int j = i - pairs_g;
@@ -587,7 +704,13 @@ k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restric
         if (v < v1) {
           const int x = int(v % KN), y = int((v / KN) % KN), z = int(v / ((long long)KN * KN));
           const long long q = ((long long)((z + dz + KN) % KN) * KN + (y + dy + KN) % KN) * KN + (x + dx + KN) % KN;
-          f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(a + q * CP + c));
+          if (SPLIT) {
+            f = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(a) + q * CP + c));
+            const float2 l = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(alo) + q * CP + c));
+            f.x += l.x; f.y += l.y;
+          } else {
+            f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(static_cast<const __nv_bfloat16*>(a) + q * CP + c));
+          }
         }
         sa[vv][c] = f.x; sa[vv][c + 1] = f.y;
       }
@@ -645,33 +768,49 @@ k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restric
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-template <int KN, int CP, int COP, int MODE> static size_t conv_smem() {
+template <int KN, int CP, int COP> static size_t conv_smem() {
   // + the mbarriers (4 steps, 2 x kSlots rows, 6 blocks), the TMEM slot and the abort flag
   return size_t(3 * kSlots) * (CP / 8) * row_plane<KN>() + size_t(27) * (CP / 8) * COP * 16 + 192;
 }
 
-template <int KN, int CP, int COP, int MODE> static void conv_attr() {
-  cudaFuncSetAttribute(k_conv3<KN, CP, COP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       int(conv_smem<KN, CP, COP, MODE>()));
+template <int KN, int CP, int COP, int MODE, bool F16 = false> static void conv_attr() {
+  cudaFuncSetAttribute(k_conv3<KN, CP, COP, MODE, F16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       int(conv_smem<KN, CP, COP>()));
 }
 
-template <int KN, int CP, int COP, int MODE>
-static void conv_launch(int grid, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* b, const ConvOut& o,
-                        int* err, long long wait_limit, cudaStream_t st) {
-  // one map per 8-channel chunk of the BF16 channels-last input [z][y][x][CP]:
+// in: channels-last 16-bit input (BF16, or FP16 when F16); w: packed 16-bit
+// weights of the same type.  The tensor maps are encoded with the BF16 element
+// type for both: a bulk tensor copy moves 16-bit elements without converting
+// them, and its zero fill is the all-zero bit pattern, +0 in either type.
+template <int KN, int CP, int COP, int MODE, bool F16 = false>
+static void conv_launch(int grid, const void* in, const void* w, const float* b, const ConvOut& o, int* err,
+                        long long wait_limit, cudaStream_t st) {
+  // one map per 8-channel chunk of the channels-last input [z][y][x][CP]:
   // dims (8 channels, x, y, z), boxes of 8 channels x (KN + 2) voxels of one row
   ConvMaps maps{};
   const unsigned long long dims[4] = {8, KN, KN, KN};
   const unsigned long long str[3] = {CP * 2ull, KN * CP * 2ull, (unsigned long long)KN * KN * CP * 2ull};
   const unsigned box[4] = {8, KN + 2, 1, 1};
   bool enc = true;
-  for (int c = 0; c < CP / 8; ++c) enc = enc && tma_encode_bf16_4d(&maps.m[c], in + 8 * c, dims, str, box);
+  for (int c = 0; c < CP / 8; ++c)
+    enc = enc && tma_encode_bf16_4d(&maps.m[c], static_cast<const unsigned char*>(in) + 16 * c, dims, str, box);
   if (!enc) {  // no tensor-map encoder: report it through the closure's error flag
     k_set_flag<<<1, 1, 0, st>>>(err);
     return;
   }
-  k_conv3<KN, CP, COP, MODE><<<grid, kConvThreads, conv_smem<KN, CP, COP, MODE>(), st>>>(maps, w, b, o, err,
-                                                                                         wait_limit);
+  k_conv3<KN, CP, COP, MODE, F16><<<grid, kConvThreads, conv_smem<KN, CP, COP>(), st>>>(
+      maps, static_cast<const __nv_bfloat16*>(w), b, o, err, wait_limit);
+}
+
+// One layer in split precision: three passes A_hi W_hi (kLinear), A_lo W_hi
+// (kAccum) and A_hi W_lo (FIN), all accumulating in the FP32 buffer o.pre.  The
+// dropped A_lo W_lo term is below the representation error of the parts.
+template <int KN, int CP, int COP, int FIN, bool F16>
+static void conv_split(int grid, const void* in_h, const void* in_l, const void* w_h, const void* w_l, const float* b,
+                       const ConvOut& o, int* err, long long wait_limit, cudaStream_t st) {
+  conv_launch<KN, CP, COP, kLinear, F16>(grid, in_h, w_h, nullptr, o, err, wait_limit, st);
+  conv_launch<KN, CP, COP, kAccum, F16>(grid, in_l, w_h, nullptr, o, err, wait_limit, st);
+  conv_launch<KN, CP, COP, FIN, F16>(grid, in_h, w_l, b, o, err, wait_limit, st);
 }
 
 bool cnn_supported(int n, int D) { return (n == 64 || n == 128) && D == 3; }
@@ -689,6 +828,19 @@ template <int KN> static void cnn_init_n() {
   conv_attr<KN, 16, 32, kLinear>();
   conv_attr<KN, 32, 32, kLinear>();
   conv_attr<KN, 32, 16, kLinear>();
+  // split precision: FP16 forward passes, BF16 input-gradient passes
+  conv_attr<KN, 16, 32, kLinear, true>();
+  conv_attr<KN, 16, 32, kAccum, true>();
+  conv_attr<KN, 16, 32, kGeluSplit, true>();
+  conv_attr<KN, 32, 32, kLinear, true>();
+  conv_attr<KN, 32, 32, kAccum, true>();
+  conv_attr<KN, 32, 32, kGeluSplit, true>();
+  conv_attr<KN, 32, 16, kLinear, true>();
+  conv_attr<KN, 32, 16, kAccum, true>();
+  conv_attr<KN, 32, 16, kTauSplit, true>();
+  conv_attr<KN, 16, 32, kAccum>();
+  conv_attr<KN, 32, 32, kAccum>();
+  conv_attr<KN, 32, 16, kAccum>();
 }
 
 void cnn_init() {
@@ -722,18 +874,52 @@ template <int KN> static void cnn_forward_n(const CnnArgs& a, cudaStream_t st) {
   conv_launch<KN, 32, 16, kTau>(grid, a3, a.w[3], a.b[3], o4, a.err, a.wait_limit, st);
 }
 
+// split precision: FP16 hi/lo inputs and weights, three passes per layer,
+// exact GELU; layer l accumulates in pre[l] when given (the adjoint keeps h
+// there), else in acc; layer 4 always in acc
+template <int KN> static void cnn_forward_split_n(const CnnArgs& a, cudaStream_t st) {
+  const long long npts = (long long)KN * KN * KN;
+  k_cnn_redelta<<<1, 1, 0, st>>>(a.a2, a.z, a.delta, a.nu, a.mu, a.sigma);
+  k_cnn_input_split<<<nblk(npts), 256, 0, st>>>(static_cast<const float*>(a.u[0]), static_cast<const float*>(a.u[1]),
+                                                static_cast<const float*>(a.u[2]), a.z, a.acth[0], a.actl[0], npts);
+  const int grid = a.nsm > 0 ? a.nsm : 148;
+  ConvOut o[4] = {};
+  for (int l = 0; l < 3; ++l) {
+    o[l].pre = a.pre[l] ? a.pre[l] : a.acc;
+    o[l].acth = a.acth[l + 1];
+    o[l].actl = a.actl[l + 1];
+    o[l].scale = 1.f / kSplitScale;
+  }
+  o[3].pre = a.acc;
+  o[3].tau = a.tau;
+  o[3].scale = 1.f / kSplitScale;
+  conv_split<KN, 16, 32, kGeluSplit, true>(grid, a.acth[0], a.actl[0], a.wh[0], a.wl[0], a.b[0], o[0], a.err,
+                                           a.wait_limit, st);
+  conv_split<KN, 32, 32, kGeluSplit, true>(grid, a.acth[1], a.actl[1], a.wh[1], a.wl[1], a.b[1], o[1], a.err,
+                                           a.wait_limit, st);
+  conv_split<KN, 32, 32, kGeluSplit, true>(grid, a.acth[2], a.actl[2], a.wh[2], a.wl[2], a.b[2], o[2], a.err,
+                                           a.wait_limit, st);
+  conv_split<KN, 32, 16, kTauSplit, true>(grid, a.acth[3], a.actl[3], a.wh[3], a.wl[3], a.b[3], o[3], a.err,
+                                          a.wait_limit, st);
+}
+
 void launch_cnn_forward(const CnnArgs& a, cudaStream_t st) {
+  if (a.split) {
+    if (a.n == 64) cnn_forward_split_n<64>(a, st);
+    else cnn_forward_split_n<128>(a, st);
+    return;
+  }
   if (a.n == 64) cnn_forward_n<64>(a, st);
   else cnn_forward_n<128>(a, st);
 }
 
-template <int KN, int CP, int COP>
-static void wgrad_launch(const __nv_bfloat16* g, const __nv_bfloat16* act, int cin, int cout, double* gw, double* gb,
-                         cudaStream_t st) {
+template <int KN, int CP, int COP, bool SPLIT = false>
+static void wgrad_launch(const __nv_bfloat16* g, const void* act, int cin, int cout, double* gw, double* gb,
+                         cudaStream_t st, const __nv_bfloat16* glo = nullptr, const void* alo = nullptr) {
   constexpr long long npts = (long long)KN * KN * KN;
   const int vchunk = 4096;
   dim3 grid(27, unsigned((npts + vchunk - 1) / vchunk));
-  k_conv_wgrad<KN, CP, COP><<<grid, 256, 0, st>>>(g, act, cin, cout, vchunk, gw, gb);
+  k_conv_wgrad<KN, CP, COP, SPLIT><<<grid, 256, 0, st>>>(g, glo, act, alo, cin, cout, vchunk, gw, gb);
 }
 
 template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t st) {
@@ -758,7 +944,37 @@ template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t s
   k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);
 }
 
+// split precision: BF16 hi/lo gradients and transposed weights (three passes
+// per input-gradient convolution), weight gradients from the hi + lo sums
+template <int KN> static void cnn_backward_split_n(const CnnBwdArgs& a, cudaStream_t st) {
+  const long long npts = (long long)KN * KN * KN;
+  const int grid = a.nsm > 0 ? a.nsm : 148;
+  ConvOut o{};
+  o.pre = a.gf;
+  k_gtau_cl_split<<<nblk(npts), 256, 0, st>>>(a.gtau, a.gbf, a.gbf_lo, npts);
+  wgrad_launch<KN, 32, 16, true>(a.gbf, a.acth[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st,
+                                 a.gbf_lo, a.actl[3]);
+  conv_split<KN, 16, 32, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[3], a.wtl[3], nullptr, o, a.err, a.wait_limit, st);
+  for (int l = 2; l >= 1; --l) {
+    k_gelu_bwd_cl_split<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[l], a.gbf, a.gbf_lo, npts * 32);
+    wgrad_launch<KN, 32, 32, true>(a.gbf, a.acth[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st,
+                                   a.gbf_lo, a.actl[l]);
+    conv_split<KN, 32, 32, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[l], a.wtl[l], nullptr, o, a.err, a.wait_limit,
+                                          st);
+  }
+  k_gelu_bwd_cl_split<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[0], a.gbf, a.gbf_lo, npts * 32);
+  wgrad_launch<KN, 16, 32, true>(a.gbf, a.acth[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st,
+                                 a.gbf_lo, a.actl[0]);
+  conv_split<KN, 32, 16, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[0], a.wtl[0], nullptr, o, a.err, a.wait_limit, st);
+  k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);
+}
+
 void launch_cnn_backward(const CnnBwdArgs& a, cudaStream_t st) {
+  if (a.split) {
+    if (a.n == 64) cnn_backward_split_n<64>(a, st);
+    else cnn_backward_split_n<128>(a, st);
+    return;
+  }
   if (a.n == 64) cnn_backward_n<64>(a, st);
   else cnn_backward_n<128>(a, st);
 }

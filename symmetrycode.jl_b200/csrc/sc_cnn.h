@@ -1,6 +1,7 @@
 // Internal interface of the tensor-core CNN closure (sc_cnn.cu).
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace sc {
@@ -30,7 +31,20 @@ struct CnnArgs {
   int* err;                    // set to 1 when a bounded wait times out
   int nsm;
   long long wait_limit;        // polls of each mbarrier wait before it gives up (kDefaultWaitLimit)
+  // split precision (split = true): every layer is three MMA passes over FP16
+  // hi/lo operands, A_hi W_hi + A_lo W_hi + A_hi W_lo, accumulated in FP32
+  bool split;
+  const __half* wh[4];         // FP16 high parts of the forward weights (x kSplitScale), same layout as w
+  const __half* wl[4];         // FP16 low parts
+  __half* acth[4];             // FP16 high parts of the layer inputs act0..act3 ([n^3][16], [n^3][32] x 3)
+  __half* actl[4];             // FP16 low parts
+  float* acc;                  // FP32 [n^3][32] accumulator of the layers whose pre[l] is null (and of layer 4)
 };
+
+// The FP16 forward weights of the split precision are stored x kSplitScale (a
+// power of two, so exactly) so that their low parts stay normal FP16 numbers;
+// the accumulator is scaled back in the last pass's epilogue.
+constexpr float kSplitScale = 64.f;
 
 // Default bound of the CNN kernels' mbarrier waits (polls of try_wait).
 constexpr long long kDefaultWaitLimit = 1ll << 26;
@@ -53,6 +67,12 @@ struct CnnBwdArgs {
   int* err;
   int nsm;
   long long wait_limit;
+  // split precision: BF16 hi/lo gradients and transposed weights, FP16 hi/lo layer inputs
+  bool split;
+  const __nv_bfloat16* wtl[4];        // BF16 low parts of wt
+  const __half* acth[4];              // FP16 layer inputs (high parts)
+  const __half* actl[4];              // FP16 layer inputs (low parts)
+  __nv_bfloat16* gbf_lo;              // scratch BF16 [n^3][32], low parts of gbf
 };
 
 // An encoded tensor map (CUtensorMap, 128 bytes) for the bulk tensor copies

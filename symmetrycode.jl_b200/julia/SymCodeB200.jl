@@ -217,10 +217,12 @@ end
 """
 CNN closure (new): `ws[l]`, `bs[l]` in PyTorch conv3d order (Cout, Cin, 3, 3, 3),
 flattened column-major as Julia stores `permutedims(w, (5, 4, 3, 2, 1))`.
-`tensorcores = true` selects the tcgen05 BF16 network (FP32 plans, n = 64 or 128).
+`tensorcores = true` selects the tcgen05 BF16 network (FP32 plans, n = 64 or 128);
+`split = true` (tensor cores only) evaluates every convolution as three passes
+over hi/lo operand parts (`SC_CLOPT_CNN_SPLIT`), about FP32 accuracy.
 """
 function create_cnn(Δ, visc, p::Plan, ws::Vector{Vector{Float32}}, bs::Vector{Vector{Float32}};
-                    mu = 0.0, sigma = 1.0, tensorcores = true)
+                    mu = 0.0, sigma = 1.0, tensorcores = true, split = false)
     ref = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve ws bs begin
         wp = [pointer(w) for w in ws]
@@ -232,8 +234,15 @@ function create_cnn(Δ, visc, p::Plan, ws::Vector{Vector{Float32}}, bs::Vector{V
     end
     c = Closure(ref[], p)
     finalizer(c -> ccall((:sc_closure_destroy, LIB), Cint, (Ptr{Cvoid},), c.ptr), c)
+    split && set_option(c, SC_CLOPT_CNN_SPLIT, 1)
     return c
 end
+
+const SC_CLOPT_CNN_SPLIT = Cint(1)
+
+"Closure options (`sc_closure_set_option`): `SC_CLOPT_CNN_SPLIT` => 0 | 1."
+set_option(c::Closure, option::Integer, value::Integer) =
+    check(ccall((:sc_closure_set_option, LIB), Cint, (Ptr{Cvoid}, Cint, Clonglong), c.ptr, option, value))
 
 """
 Pointwise learned closures: `fullchain(setup, mlp(...))` (`kind = :mlp`) and `tbnn`

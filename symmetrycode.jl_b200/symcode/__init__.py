@@ -19,7 +19,7 @@ import math
 import torch
 
 from . import autotune, fields  # noqa: F401
-from ._lib import (SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
+from ._lib import (SC_CLOPT_CNN_SPLIT, SC_FLOAT32, SC_FLOAT64, SymcodeError, check, header_functions, lib,
                    ptr_array, sc_forcing, sc_les_instance)
 
 __all__ = [
@@ -29,7 +29,8 @@ __all__ = [
     "State", "LesBatch", "propose_timestep", "energy_shells", "maintain_shell_energy_", "spectrum",
     "turbulence_statistics", "set_option", "Closure", "create_clark", "create_smagorinsky", "create_verstappen",
     "create_dynamic_smagorinsky", "create_bardina", "create_cnn_closure", "kaiming_cnn_weights",
-    "create_cnn_fp_closure", "closure_num_params", "closure_set_params", "pack_cnn_params", "rollout_record",
+    "create_cnn_fp_closure", "closure_num_params", "closure_set_params", "closure_set_option", "SC_CLOPT_CNN_SPLIT",
+    "pack_cnn_params", "rollout_record",
     "rollout_loss", "rollout_adjoint", "les_", "les_wray3_", "les_rk4_", "fields",
 ]
 
@@ -338,8 +339,11 @@ def kaiming_cnn_weights(seed, layers=((4, 32), (32, 32), (32, 32), (32, 6))):
     return ws, bs
 
 
-def create_cnn_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0):
-    """The tensor-core CNN closure (``sc_cnn_closure_create``); FP32, 3D, n = 128."""
+def create_cnn_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0, split=False):
+    """The tensor-core CNN closure (``sc_cnn_closure_create``); FP32, 3D, n = 64 or 128.
+    ``split=True`` switches it to the split precision (``SC_CLOPT_CNN_SPLIT``):
+    three tensor-core passes over hi/lo operand parts per convolution, about
+    FP32 accuracy."""
     import numpy as np
     ws = [np.ascontiguousarray(w, dtype=np.float32) for w in weights]
     bs = [np.ascontiguousarray(b, dtype=np.float32) for b in biases]
@@ -353,7 +357,16 @@ def create_cnn_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0)
         check(lib().sc_cnn_closure_create(ct.byref(ptr), g.plan, float(delta), float(visc), wa, ba, float(mu),
                                           float(sigma)))
     cl._ptr = ptr
+    if split:
+        closure_set_option(cl, SC_CLOPT_CNN_SPLIT, 1)
     return cl
+
+
+def closure_set_option(cl, option, value):
+    """``sc_closure_set_option``: ``SC_CLOPT_CNN_SPLIT`` (1) = 1 evaluates the
+    tensor-core CNN in split precision, 0 in BF16."""
+    with torch.cuda.device(cl.g.device):
+        check(lib().sc_closure_set_option(cl.ptr, int(option), int(value)))
 
 
 def create_cnn_fp_closure(delta, visc, g: Grid, weights, biases, mu=0.0, sigma=1.0):

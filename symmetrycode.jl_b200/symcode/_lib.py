@@ -18,6 +18,7 @@ SC_OK, SC_ERR_INVALID, SC_ERR_SIZE, SC_ERR_CUDA, SC_ERR_OOM, SC_ERR_DIVERGED, SC
 SC_FLOAT32, SC_FLOAT64 = 0, 1
 SC_OPT_USE_GRAPH, SC_OPT_WAIT_LIMIT = 1, 2  # sc_plan_set_option
 SC_OPT_VARIANT_ZINV = 3  # ... SC_OPT_VARIANT_ZFWD = 7: sweep variants (z-inv, y-inv, x, y-fwd, z-fwd)
+SC_CLOPT_CNN_SPLIT = 1  # sc_closure_set_option: split-precision tensor-core CNN
 
 
 class SymcodeError(RuntimeError):
@@ -78,6 +79,7 @@ _SIGS = {
                                   ct.POINTER(ct.POINTER(ct.c_float)), ct.c_double, ct.c_double], ct.c_int),
     "sc_closure_num_params": ([_vp, ct.POINTER(ct.c_longlong)], ct.c_int),
     "sc_closure_set_params": ([_vp, ct.POINTER(ct.c_double)], ct.c_int),
+    "sc_closure_set_option": ([_vp, ct.c_int, ct.c_longlong], ct.c_int),
     "sc_rollout_traj_bytes": ([_vp, ct.c_int], ct.c_size_t),
     "sc_rollout_record": ([_vp, _vp, _pp, ct.c_double, ct.c_double, ct.c_int, _vp, _vp], ct.c_int),
     "sc_rollout_loss": ([_vp, _vp, _pp, _vp, ct.c_double, ct.c_double, ct.c_int, ct.POINTER(ct.c_double), _vp], ct.c_int),

@@ -88,6 +88,55 @@ def test_cnn_closure_64_matches_oracle():
     assert rel_l2(to_np(cl(ut, None)), tau) < 1e-7
 
 
+@pytest.mark.parametrize("n,seed", [(128, 40), (64, 41)])
+def test_cnn_closure_split_matches_unrounded_oracle(n, seed):
+    """Split precision (SC_CLOPT_CNN_SPLIT): three tensor-core passes over
+    FP16 hi/lo parts per convolution against the FP64 network without any
+    rounding.  The parts carry 22 significant bits, so the bar is the FP32
+    level, not the BF16 one (measured on a B200: 2.1e-6 at n = 128, 2.7e-6 at
+    n = 64)."""
+    g, go = S.Grid(3, n, dtype=torch.float32, device="cuda:0"), O.Grid(3, n)
+    u = O.random_field(go, seed=seed, kpeak=4)
+    delta, nu = 4 * go.l / n, 3e-4
+    ws, bs = S.kaiming_cnn_weights(7)
+    bs = [b + 0.05 * np.arange(b.size, dtype=np.float32) for b in bs]
+    cl = S.create_cnn_closure(delta, nu, g, ws, bs, mu=1.0, sigma=2.0, split=True)
+    ut = [to_dev(c, g) for c in u]
+    tau = to_np(cl(ut, None))
+    uphys = np.stack([to_np(S.to_phys_(S.spacescalarfield(g), c, g)) for c in ut], 0)
+    zval = O.cnn_redelta_channel(u, go, delta, nu, mu=1.0, sigma=2.0)
+    rows = [(0, 0), (17, 5), (n - 1, n - 1), (n // 2 + 3, n // 3)]
+    ref = O.cnn_rows(uphys, zval, ws, bs, rows, round_bf16=False)
+    got = np.stack([tau[:, z, y, :] for (y, z) in rows], 1)
+    err = rel_l2(got, ref)
+    print(f"split precision n={n}: tau relative L2 vs unrounded FP64 {err:.2e}")
+    assert np.isfinite(got).all()
+    assert err < 1e-5
+    # back to BF16: the one-pass result, BF16-level error again
+    S.closure_set_option(cl, S.SC_CLOPT_CNN_SPLIT, 0)
+    tau_bf = to_np(cl(ut, None))
+    S.closure_set_option(cl, S.SC_CLOPT_CNN_SPLIT, 1)
+    assert rel_l2(to_np(cl(ut, None)), tau) < 1e-7
+    ref_bf = O.cnn_rows(uphys, zval, ws, bs, rows)
+    assert rel_l2(np.stack([tau_bf[:, z, y, :] for (y, z) in rows], 1), ref_bf) < 5e-3
+    import ctypes as ct
+    status = ct.c_int()
+    S.lib().sc_closure_status(cl.ptr, ct.byref(status))
+    assert status.value == 0
+    cl.close()
+    g.close()
+
+
+def test_closure_option_rejects_other_closures():
+    g = S.Grid(3, 32, dtype=torch.float32, device="cuda:0")
+    ws, bs = S.kaiming_cnn_weights(3)
+    cl = S.create_cnn_fp_closure(4 * g.l / 32, 1e-3, g, ws, bs)
+    with pytest.raises(S.SymcodeError):
+        S.closure_set_option(cl, S.SC_CLOPT_CNN_SPLIT, 1)
+    cl.close()
+    g.close()
+
+
 @pytest.mark.parametrize("target_scale", [1.3])
 def test_tensor_core_adjoint_matches_fp64_gradient(target_scale):
     """The BF16 tensor-core adjoint (roundings taken as identities) against the
