@@ -655,113 +655,117 @@ __global__ void k_gin_planar(const float* __restrict__ gin, const GinPtrs o, lon
 // Weight and bias gradients of one layer (CUDA cores, FP32 accumulation,
 // FP64 atomics into the flat parameter gradient):
 //   gw[co][ci][t] += sum_v g[v][co] a[v + off(t)][ci],  gb[co] += sum_v g[v][co]
-// for co < cout, ci < cin.  Block (tap t, chunk of voxels); a group of
-// (COP/4)(CP/4) threads holds a 4 x 4 (co, ci) register tile; the chunk's g
-// rows and shifted a rows are staged in shared memory 64 voxels at a time.
+// for co < cout, ci < cin.  Block (tap t, chunk of voxels).  Only the first CI
+// (4 | 32) input and CO (8 | 32) output channels are formed, the layer's own
+// channels rounded up to the tile, not the padded CP, COP of the activations.
+// A group of (CO/8)(CI/4) threads holds 8 x 4 (co, ci) register tiles, so a
+// voxel costs three 16-byte shared loads per 32 FMAs; the groups split each
+// staged block of VS voxels.  The bias sums run only in the centre-tap blocks.
+// The groups' tiles are summed in shared memory by all threads, then one FP64
+// atomic per gradient entry and block.
 // SPLIT: g = g + glo (BF16 high and low parts) and a = FP16 high + low parts
 // (a and alo of type __half); otherwise a is BF16 and glo, alo are unused.
-template <int KN, int CP, int COP, bool SPLIT>
+template <int KN, int CP, int COP, int CI, int CO, bool SPLIT>
 __global__ void __launch_bounds__(256)
 k_conv_wgrad(const __nv_bfloat16* __restrict__ g, const __nv_bfloat16* __restrict__ glo, const void* __restrict__ a,
              const void* __restrict__ alo, int cin, int cout, int vchunk, double* __restrict__ gw,
              double* __restrict__ gb) {
-  constexpr int TG = (COP / 4) * (CP / 4);  // threads per group
-  constexpr int NG = 256 / TG;              // groups (split the voxels of a stage)
-  constexpr int VS = 64;                    // voxels per stage
+  static_assert(CI % 4 == 0 && CI <= CP && CO % 8 == 0 && CO <= COP, "tile shape");
+  constexpr int TCO = 8, TCI = 4, NE = TCO * TCI;
+  constexpr int TG = (CO / TCO) * (CI / TCI);  // threads per group
+  constexpr int NG = 256 / TG;                  // groups
+  constexpr int VS = 128;                       // voxels per stage
+  constexpr int LG = CO + 4, LA = CI + 4;       // padded shared rows (16-byte multiples)
+  constexpr int STAGE = VS * (LG + LA);         // floats of one staged block
+  constexpr int RED = 256 * NE;                 // floats of the groups' tiles
   constexpr long long NPTS = (long long)KN * KN * KN;
-  __shared__ __align__(16) float sg[VS][COP + 4];
-  __shared__ __align__(16) float sa[VS][CP + 4];
-  __shared__ float red[256][17];
-  const int t = blockIdx.x;  // tap
+  __shared__ __align__(16) float sbuf[STAGE > RED ? STAGE : RED];
+  float* sg = sbuf;            // [VS][LG]
+  float* sa = sbuf + VS * LG;  // [VS][LA]
+  const int t = blockIdx.x;    // tap
   const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+  const bool centre = t == 13;
   const int tid = threadIdx.x, grp = tid / TG, lt = tid % TG;
-  const int co0 = 4 * (lt / (CP / 4)), ci0 = 4 * (lt % (CP / 4));
-  float acc[4][4] = {};
-  float accb[4] = {};
+  const int co0 = TCO * (lt / (CI / TCI)), ci0 = TCI * (lt % (CI / TCI));
+  float acc[TCO][TCI] = {};
+  float accb[TCO] = {};
   const long long v0 = (long long)blockIdx.y * vchunk;
   const long long v1 = min(v0 + vchunk, NPTS);
   for (long long vb = v0; vb < v1; vb += VS) {
-    // stage g rows and shifted a rows (BF16 -> FP32)
-    for (int i = tid; i < VS * (COP + CP) / 2; i += 256) {
-      const int pairs_g = VS * COP / 2;
-      if (i < pairs_g) {
-        const int vv = i / (COP / 2), c = 2 * (i % (COP / 2));
-        const long long v = vb + vv;
-        float2 f = make_float2(0.f, 0.f);
-        if (v < v1) {
-          f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(g + v * COP + c));
-          if (SPLIT) {
-            const float2 l = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(glo + v * COP + c));
-            f.x += l.x; f.y += l.y;
-          }
+    // stage the g rows and the shifted a rows (16-bit pairs -> FP32)
+    for (int i = tid; i < VS * CO / 2; i += 256) {
+      const int vv = i / (CO / 2), c = 2 * (i % (CO / 2));
+      const long long v = vb + vv;
+      float2 f = make_float2(0.f, 0.f);
+      if (v < v1) {
+        f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(g + v * COP + c));
+        if (SPLIT) {
+          const float2 l = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(glo + v * COP + c));
+          f.x += l.x; f.y += l.y;
         }
-        sg[vv][c] = f.x; sg[vv][c + 1] = f.y;
-      } else {
-        const int j = i - pairs_g;
-        const int vv = j / (CP / 2), c = 2 * (j % (CP / 2));
-        const long long v = vb + vv;
-        float2 f = make_float2(0.f, 0.f);
-        if (v < v1) {
-          const int x = int(v % KN), y = int((v / KN) % KN), z = int(v / ((long long)KN * KN));
-          const long long q = ((long long)((z + dz + KN) % KN) * KN + (y + dy + KN) % KN) * KN + (x + dx + KN) % KN;
-          if (SPLIT) {
-            f = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(a) + q * CP + c));
-            const float2 l = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(alo) + q * CP + c));
-            f.x += l.x; f.y += l.y;
-          } else {
-            f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(static_cast<const __nv_bfloat16*>(a) + q * CP + c));
-          }
-        }
-        sa[vv][c] = f.x; sa[vv][c + 1] = f.y;
       }
+      *reinterpret_cast<float2*>(sg + vv * LG + c) = f;
+    }
+    for (int i = tid; i < VS * CI / 2; i += 256) {
+      const int vv = i / (CI / 2), c = 2 * (i % (CI / 2));
+      const long long v = vb + vv;
+      float2 f = make_float2(0.f, 0.f);
+      if (v < v1) {
+        const int x = int(v % KN), y = int((v / KN) % KN), z = int(v / ((long long)KN * KN));
+        const long long q = ((long long)((z + dz + KN) % KN) * KN + (y + dy + KN) % KN) * KN + (x + dx + KN) % KN;
+        if (SPLIT) {
+          f = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(a) + q * CP + c));
+          const float2 l = __half22float2(*reinterpret_cast<const __half2*>(static_cast<const __half*>(alo) + q * CP + c));
+          f.x += l.x; f.y += l.y;
+        } else {
+          f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(static_cast<const __nv_bfloat16*>(a) + q * CP + c));
+        }
+      }
+      *reinterpret_cast<float2*>(sa + vv * LA + c) = f;
     }
     __syncthreads();
     for (int vv = grp; vv < VS; vv += NG) {
-      const float4 gg = *reinterpret_cast<const float4*>(&sg[vv][co0]);
-      const float4 aa = *reinterpret_cast<const float4*>(&sa[vv][ci0]);
-      const float gv[4] = {gg.x, gg.y, gg.z, gg.w}, av[4] = {aa.x, aa.y, aa.z, aa.w};
+      const float4 g0 = *reinterpret_cast<const float4*>(sg + vv * LG + co0);
+      const float4 g1 = *reinterpret_cast<const float4*>(sg + vv * LG + co0 + 4);
+      const float4 aa = *reinterpret_cast<const float4*>(sa + vv * LA + ci0);
+      const float gv[TCO] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+      const float av[TCI] = {aa.x, aa.y, aa.z, aa.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
+      for (int i = 0; i < TCO; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += gv[i] * av[j];
-        accb[i] += gv[i];
+        for (int j = 0; j < TCI; ++j) acc[i][j] = fmaf(gv[i], av[j], acc[i][j]);
+      if (centre) {
+#pragma unroll
+        for (int i = 0; i < TCO; ++i) accb[i] += gv[i];
       }
     }
     __syncthreads();
   }
-  // reduce the groups, then one FP64 atomic per gradient entry
+  // the groups' tiles: red[grp][lt][e], e = i TCI + j; entry o = lt NE + e of
+  // a group is (co0(lt) + e / TCI, ci0(lt) + e % TCI)
+  float* red = sbuf;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int e = 0; e < NE; ++e) red[(grp * TG + lt) * NE + e] = acc[e / TCI][e % TCI];
+  __syncthreads();
+  for (int o = tid; o < TG * NE; o += 256) {
+    float sum = 0.f;
+    for (int k = 0; k < NG; ++k) sum += red[k * TG * NE + o];
+    const int l2 = o / NE, e = o % NE;
+    const int co = TCO * (l2 / (CI / TCI)) + e / TCI, ci = TCI * (l2 % (CI / TCI)) + e % TCI;
+    if (co < cout && ci < cin) atomicAdd(&gw[((long long)co * cin + ci) * 27 + t], double(sum));
+  }
+  if (!centre) return;  // uniform per block
+  __syncthreads();
+  // bias: the threads with ci0 = 0 hold every co once per group
+  if (ci0 == 0) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) red[tid][4 * i + j] = acc[i][j];
-    red[tid][16] = 0.f;
+    for (int i = 0; i < TCO; ++i) red[grp * CO + co0 + i] = accb[i];
   }
   __syncthreads();
-  if (grp == 0) {
-    for (int k = 1; k < NG; ++k)
-#pragma unroll
-      for (int e = 0; e < 16; ++e) acc[e / 4][e % 4] += red[k * TG + lt][e];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int co = co0 + i, ci = ci0 + j;
-        if (co < cout && ci < cin) atomicAdd(&gw[((long long)co * cin + ci) * 27 + t], double(acc[i][j]));
-      }
-  }
-  __syncthreads();
-  if (t == 13 && ci0 == 0) {  // bias gradient once (centre tap), from the same g rows
-#pragma unroll
-    for (int i = 0; i < 4; ++i) red[tid][i] = accb[i];
-  }
-  __syncthreads();
-  if (t == 13 && grp == 0 && ci0 == 0) {
-    for (int k = 1; k < NG; ++k)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) accb[i] += red[k * TG + lt][i];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (co0 + i < cout) atomicAdd(&gb[co0 + i], double(accb[i]));
+  if (tid < CO) {
+    float sum = 0.f;
+    for (int k = 0; k < NG; ++k) sum += red[k * CO + tid];
+    if (tid < cout) atomicAdd(&gb[tid], double(sum));
   }
 }
 
@@ -913,13 +917,14 @@ void launch_cnn_forward(const CnnArgs& a, cudaStream_t st) {
   else cnn_forward_n<128>(a, st);
 }
 
-template <int KN, int CP, int COP, bool SPLIT = false>
+// CI, CO: the layer's channels rounded up to the register tile (4 | 32 inputs, 8 | 32 outputs)
+template <int KN, int CP, int COP, int CI, int CO, bool SPLIT = false>
 static void wgrad_launch(const __nv_bfloat16* g, const void* act, int cin, int cout, double* gw, double* gb,
                          cudaStream_t st, const __nv_bfloat16* glo = nullptr, const void* alo = nullptr) {
   constexpr long long npts = (long long)KN * KN * KN;
-  const int vchunk = 4096;
+  const int vchunk = KN >= 128 ? 16384 : 4096;  // 27 x 128 | 27 x 64 blocks: about 6 and 3 full waves
   dim3 grid(27, unsigned((npts + vchunk - 1) / vchunk));
-  k_conv_wgrad<KN, CP, COP, SPLIT><<<grid, 256, 0, st>>>(g, glo, act, alo, cin, cout, vchunk, gw, gb);
+  k_conv_wgrad<KN, CP, COP, CI, CO, SPLIT><<<grid, 256, 0, st>>>(g, glo, act, alo, cin, cout, vchunk, gw, gb);
 }
 
 template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t st) {
@@ -927,19 +932,19 @@ template <int KN> static void cnn_backward_n(const CnnBwdArgs& a, cudaStream_t s
   const int grid = a.nsm > 0 ? a.nsm : 148;
   // layer 4: g4 = dL/dtau (BF16 [v][16]); input gradient through W4^T; weight gradient against act3
   k_gtau_cl<<<nblk(npts), 256, 0, st>>>(a.gtau, a.gbf, npts);
-  wgrad_launch<KN, 32, 16>(a.gbf, a.act[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st);
+  wgrad_launch<KN, 32, 16, 32, 8>(a.gbf, a.act[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st);
   ConvOut o{};
   o.pre = a.gf;
   conv_launch<KN, 16, 32, kLinear>(grid, a.gbf, a.wt[3], nullptr, o, a.err, a.wait_limit, st);
   // layers 3, 2: g_pre = g_post * gelu'(h); input and weight gradients
   for (int l = 2; l >= 1; --l) {
     k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[l], a.gbf, npts * 32);
-    wgrad_launch<KN, 32, 32>(a.gbf, a.act[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st);
+    wgrad_launch<KN, 32, 32, 32, 32>(a.gbf, a.act[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st);
     conv_launch<KN, 32, 32, kLinear>(grid, a.gbf, a.wt[l], nullptr, o, a.err, a.wait_limit, st);
   }
   // layer 1: input gradient into 16 channels (4 used), then planar
   k_gelu_bwd_cl<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[0], a.gbf, npts * 32);
-  wgrad_launch<KN, 16, 32>(a.gbf, a.act[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st);
+  wgrad_launch<KN, 16, 32, 4, 32>(a.gbf, a.act[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st);
   conv_launch<KN, 32, 16, kLinear>(grid, a.gbf, a.wt[0], nullptr, o, a.err, a.wait_limit, st);
   k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);
 }
@@ -952,18 +957,18 @@ template <int KN> static void cnn_backward_split_n(const CnnBwdArgs& a, cudaStre
   ConvOut o{};
   o.pre = a.gf;
   k_gtau_cl_split<<<nblk(npts), 256, 0, st>>>(a.gtau, a.gbf, a.gbf_lo, npts);
-  wgrad_launch<KN, 32, 16, true>(a.gbf, a.acth[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st,
+  wgrad_launch<KN, 32, 16, 32, 8, true>(a.gbf, a.acth[3], 32, 6, a.gw + a.woff[3], a.gw + a.woff[3] + 6 * 32 * 27, st,
                                  a.gbf_lo, a.actl[3]);
   conv_split<KN, 16, 32, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[3], a.wtl[3], nullptr, o, a.err, a.wait_limit, st);
   for (int l = 2; l >= 1; --l) {
     k_gelu_bwd_cl_split<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[l], a.gbf, a.gbf_lo, npts * 32);
-    wgrad_launch<KN, 32, 32, true>(a.gbf, a.acth[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st,
+    wgrad_launch<KN, 32, 32, 32, 32, true>(a.gbf, a.acth[l], 32, 32, a.gw + a.woff[l], a.gw + a.woff[l] + 32 * 32 * 27, st,
                                    a.gbf_lo, a.actl[l]);
     conv_split<KN, 32, 32, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[l], a.wtl[l], nullptr, o, a.err, a.wait_limit,
                                           st);
   }
   k_gelu_bwd_cl_split<<<nblk(npts * 32), 256, 0, st>>>(a.gf, a.pre[0], a.gbf, a.gbf_lo, npts * 32);
-  wgrad_launch<KN, 16, 32, true>(a.gbf, a.acth[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st,
+  wgrad_launch<KN, 16, 32, 4, 32, true>(a.gbf, a.acth[0], 4, 32, a.gw + a.woff[0], a.gw + a.woff[0] + 32 * 4 * 27, st,
                                  a.gbf_lo, a.actl[0]);
   conv_split<KN, 32, 16, kAccum, false>(grid, a.gbf, a.gbf_lo, a.wt[0], a.wtl[0], nullptr, o, a.err, a.wait_limit, st);
   k_gin_planar<<<nblk(npts), 256, 0, st>>>(a.gf, a.gin_planar, npts);

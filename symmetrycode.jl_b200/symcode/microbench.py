@@ -16,7 +16,15 @@ at n^3 (FP32).
 
 ``--kernel cnn`` evaluates the tensor-core CNN closure (n = 128, FP32) COUNT
 times on a seeded random field and reports ms per evaluation and the
-convolutions' TFLOP/s (2 x 27 x sum(C_in C_out) flops per grid point).
+convolutions' TFLOP/s (2 x 27 x sum(C_in C_out) flops per grid point);
+``--split`` in split precision (three passes per convolution; the TFLOP/s
+count one pass's flops).
+
+``--kernel adjoint`` runs one a-posteriori training rollout of the tensor-core
+CNN closure at n^3 (default n = 64 with ``--n 64``): record a target
+trajectory of COUNT RK4 steps, then loss and adjoint with checkpoints every 5
+steps, timed over REPS repetitions of the adjoint (``--split`` for the split
+precision).
 """
 
 import argparse
@@ -30,7 +38,7 @@ KERNELS = {"yinv": 0, "yfwd": 1, "x": 2, "zinv": 3, "zfwd": 4}
 CNN_LAYERS = ((4, 32), (32, 32), (32, 32), (32, 6))
 
 
-def run_cnn(n, count, reps=5):
+def run_cnn(n, count, reps=5, split=False):
     import torch
 
     from . import Grid, create_cnn_closure, kaiming_cnn_weights
@@ -39,7 +47,7 @@ def run_cnn(n, count, reps=5):
     gen = torch.Generator(device="cuda:0").manual_seed(3)
     u = [torch.randn(g.spec_shape, dtype=g.cdtype, device=g.device, generator=gen) * 1e-3 for _ in range(3)]
     ws, bs = kaiming_cnn_weights(7, CNN_LAYERS)
-    cl = create_cnn_closure(2 * g.l / n, 1e-3, g, ws, bs)
+    cl = create_cnn_closure(2 * g.l / n, 1e-3, g, ws, bs, split=split)
     cl(u)
     torch.cuda.synchronize()
     best = None
@@ -54,8 +62,40 @@ def run_cnn(n, count, reps=5):
         best = t if best is None else min(best, t)
     flops = 2.0 * 27 * n ** 3 * sum(ci * co for ci, co in CNN_LAYERS)
     cl.close()
-    return {"kernel": "cnn", "n": n, "count": count, "dtype": "bf16", "ms": best, "flops": flops,
-            "tflops": flops / (best / 1e3) / 1e12}
+    return {"kernel": "cnn", "n": n, "count": count, "dtype": "f16 split" if split else "bf16", "ms": best,
+            "flops": flops, "tflops": flops / (best / 1e3) / 1e12}
+
+
+def run_adjoint(n, nsteps, reps=1, split=False):
+    import time
+
+    import numpy as np
+    import torch
+
+    from . import (Grid, closure_set_params, create_cnn_closure, kaiming_cnn_weights, pack_cnn_params,
+                   rollout_adjoint, rollout_record)
+
+    g = Grid(3, n, dtype=torch.float32, device="cuda:0")
+    gen = torch.Generator(device="cuda:0").manual_seed(5)
+    u0 = [torch.randn(g.spec_shape, dtype=g.cdtype, device=g.device, generator=gen) * 1e-3 for _ in range(3)]
+    ws, bs = kaiming_cnn_weights(5, CNN_LAYERS)
+    theta = pack_cnn_params(ws, bs)
+    cl = create_cnn_closure(4 * g.l / n, 1e-3, g, ws, bs, mu=5.0, sigma=2.0, split=split)
+    closure_set_params(cl, theta * (1 + 0.01 * np.random.default_rng(6).standard_normal(theta.size)))
+    traj = rollout_record(g, cl, u0, 5e-3, 1e-3, nsteps)
+    closure_set_params(cl, theta)
+    rollout_adjoint(g, cl, u0, traj, 5e-3, 1e-3, nsteps, ckpt_every=5)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        loss, grad = rollout_adjoint(g, cl, u0, traj, 5e-3, 1e-3, nsteps, ckpt_every=5)
+    torch.cuda.synchronize()
+    t = (time.perf_counter() - t0) / reps
+    cl.close()
+    g.close()
+    return {"kernel": "adjoint", "n": n, "steps": nsteps, "precision": "split" if split else "bf16",
+            "s_per_rollout": t, "ms_per_step": 1e3 * t / nsteps, "loss": loss,
+            "grad_finite": bool(np.isfinite(grad).all())}
 
 
 def run_sfs(n, nl, count, reps=3):
@@ -126,16 +166,19 @@ def run(kernel, n, count, dtype="f32", reps=5, variant=0):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", choices=sorted(KERNELS) + ["cnn", "sfs", "clark", "dynsmag"], required=True)
+    ap.add_argument("--kernel", choices=sorted(KERNELS) + ["cnn", "sfs", "clark", "dynsmag", "adjoint"], required=True)
     ap.add_argument("--n-les", type=int, default=128)
     ap.add_argument("--n", type=int, default=810)
     ap.add_argument("--count", type=int, required=True)
     ap.add_argument("--dtype", choices=["f32", "f64"], default="f32")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--variant", type=int, default=0, help="autotuner variant of the sweep (sc_plan_num_variants)")
+    ap.add_argument("--split", action="store_true", help="cnn, adjoint: the CNN's split precision")
     a = ap.parse_args(argv)
     if a.kernel == "cnn":
-        print(json.dumps(run_cnn(a.n, a.count, a.reps)))
+        print(json.dumps(run_cnn(a.n, a.count, a.reps, a.split)))
+    elif a.kernel == "adjoint":
+        print(json.dumps(run_adjoint(a.n, a.count, a.reps, a.split)))
     elif a.kernel == "sfs":
         print(json.dumps(run_sfs(a.n, a.n_les, a.count, a.reps)))
     elif a.kernel in ("clark", "dynsmag"):
