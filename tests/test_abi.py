@@ -47,3 +47,10 @@ def test_plan_create_without_device_fails_loudly():
     import symcode
     with pytest.raises(RuntimeError):
         symcode.Grid(3, 8)
+
+
+def test_closure_set_option_rejects_a_null_closure():
+    # the null check runs before any CUDA call
+    L = _lib.lib()
+    assert L.sc_closure_set_option(None, _lib.SC_CLOPT_CNN_SPLIT, 1) == _lib.SC_ERR_INVALID
+    assert b"null" in L.sc_last_error_string()
