@@ -22,6 +22,14 @@
 // of the row pipeline's waits is a launch argument (a plan option, so that a
 // test can make a wait run out); the last wait for MMAs still in flight before
 // the tensor memory is freed always keeps the full default bound.
+//
+// Split precision (SC_CLOPT_CNN_SPLIT): each operand is stored as two 16-bit
+// parts x = hi + lo, and a convolution is three launches of the same kernel,
+// A_hi W_hi + A_lo W_hi + A_hi W_lo, accumulated in an FP32 channels-last
+// buffer by the epilogue modes kLinear, kAccum and a last mode that applies
+// bias and GELU (tanhf) and writes the hi/lo activations (or tau).  Forward
+// passes use FP16 parts (kind::f16 with both operands f16); the adjoint's
+// input-gradient passes use BF16 parts.  One MMA never mixes the two types.
 #include <cuda_bf16.h>
 #include <stdint.h>
 
