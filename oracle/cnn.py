@@ -18,7 +18,8 @@ import numpy as np
 
 from .spectral import Grid, getenergy, twothirds, vectorgradient
 
-__all__ = ["bf16", "gelu", "gelu_grad", "cnn_redelta_channel", "cnn_rows", "cnn_field"]
+__all__ = ["bf16", "f16", "split_parts", "gelu", "gelu_grad", "cnn_redelta_channel", "cnn_rows", "cnn_field",
+           "cnn_rows_split"]
 
 _GELU_C = math.sqrt(2.0 / math.pi)
 _GELU_A = 0.044715
@@ -44,6 +45,18 @@ def bf16(x):
     lsb = (b >> 16) & 1
     b = ((b + 0x7FFF + lsb) & 0xFFFF0000).astype(np.uint32)
     return b.view(np.float32).astype(np.float64)
+
+
+def f16(x):
+    """Round to the nearest FP16 value (ties to even, subnormals kept), returned as float64."""
+    return np.asarray(x, dtype=np.float64).astype(np.float16).astype(np.float64)
+
+
+def split_parts(x, rnd=f16):
+    """The split precision's two parts of x: hi = rnd(x), lo = rnd(x - hi)."""
+    x = np.asarray(x, dtype=np.float64)
+    hi = rnd(x)
+    return hi, rnd(x - hi)
 
 
 def cnn_redelta_channel(u, g: Grid, delta, nu, mu=0.0, sigma=1.0):
@@ -111,3 +124,31 @@ def cnn_field(uphys, zval, weights, biases, round_bf16=True):
         if li < 3:
             act = rnd(gelu(act))
     return act
+
+
+def cnn_rows_split(uphys, zval, weights, biases, rows, wscale=64.0):
+    """tau at ``rows`` as the split precision computes it: every operand x =
+    hi + lo in FP16 parts (weights scaled by ``wscale`` before the split and
+    the sum scaled back), each convolution the three products A_hi W_hi +
+    A_lo W_hi + A_hi W_lo accumulated exactly (FP64 here), GELU unrounded and
+    its output split again.  Emulates the rounding of the parts, not the FP32
+    accumulation order of the tensor cores."""
+    out = []
+    n = uphys.shape[-1]
+    wparts = [split_parts(np.asarray(w, dtype=np.float64) * wscale) for w in weights]
+    for (y0, z0) in rows:
+        idx_z = [(z0 + d) % n for d in range(-4, 5)]
+        idx_y = [(y0 + d) % n for d in range(-4, 5)]
+        win = uphys[:, idx_z][:, :, idx_y]
+        act = np.concatenate([np.asarray(win, dtype=np.float64), np.full((1,) + win.shape[1:], zval)], 0)
+        for li in range(4):
+            h = 4 - li
+            ah, al = split_parts(act)
+            wh, wl = wparts[li]
+            zero = np.zeros_like(np.asarray(biases[li], dtype=np.float64))
+            acc = sum(_conv(a_, w_, zero, 1, 2 * h - 1, 1, 2 * h - 1) for a_, w_ in ((ah, wh), (al, wh), (ah, wl)))
+            act = acc / wscale + np.asarray(biases[li], dtype=np.float64)[:, None, None, None]
+            if li < 3:
+                act = gelu(act)
+        out.append(act[:, 0, 0, :])
+    return np.stack(out, 1)

@@ -49,3 +49,37 @@ def test_cnn_field_equals_cnn_rows():
     rows = [(0, 0), (5, 7), (15, 3)]
     r = O.cnn_rows(uphys, 0.3, ws, bs, rows)
     assert np.array_equal(np.stack([f[:, z, y, :] for (y, z) in rows], 1), r)
+
+
+def test_split_parts_carry_22_bits():
+    """x = hi + lo with FP16 parts: |x - hi - lo| <= 2^-22 |x| while lo is a
+    normal FP16 number (|x| >= 2^-3), else at most half the subnormal spacing
+    2^-24.  The weights are stored x 64 to stay in the first range."""
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(10000) * 10.0 ** rng.uniform(-4, 3, 10000)
+    hi, lo = O.split_parts(x)
+    assert np.all(O.f16(hi) == hi) and np.all(O.f16(lo) == lo)
+    assert np.all(np.abs(x - hi - lo) <= np.maximum(2.0 ** -22 * np.abs(x), 2.0 ** -25))
+    big = np.abs(x) >= 2.0 ** -3
+    assert np.max(np.abs(x - hi - lo)[big] / np.abs(x[big])) <= 2.0 ** -22
+
+
+def test_split_network_sits_at_the_fp32_floor():
+    """The split precision's roundings alone move tau by 1.5e-7 here, against
+    4.6e-3 for one BF16 pass; the GPU's 2-3e-6 against FP64 is set by its FP32
+    accumulation, not by the parts."""
+    n = 16
+    rng = np.random.default_rng(11)
+    uphys = rng.standard_normal((3, n, n, n))
+    ws, bs = [], []
+    for cin, cout in ((4, 32), (32, 32), (32, 32), (32, 6)):
+        ws.append(rng.standard_normal((cout, cin, 3, 3, 3)) * (2.0 / (27 * cin)) ** 0.5)
+        bs.append(0.05 * np.arange(cout, dtype=np.float64))
+    rows = [(0, 0), (5, 9), (15, 15)]
+    ref = O.cnn_rows(uphys, 0.7, ws, bs, rows, round_bf16=False)
+    split = O.cnn_rows_split(uphys, 0.7, ws, bs, rows)
+    bf = O.cnn_rows(uphys, 0.7, ws, bs, rows)
+    e_split = np.linalg.norm(split - ref) / np.linalg.norm(ref)
+    e_bf = np.linalg.norm(bf - ref) / np.linalg.norm(ref)
+    assert e_split < 1e-6
+    assert e_bf > 1e-3 * 0.5 and e_split < 1e-3 * e_bf
