@@ -148,6 +148,32 @@ def test_make_tracefree():
         assert np.array_equal(t3[i], raw[i])
 
 
+# test/test_tensor_helpers.jl:47-58
+def test_strain_from_gradient_is_symmetric_part():
+    g = O.Grid(3, 4, 2 * math.pi)
+    names = ["xx", "yx", "zx", "xy", "yy", "zy", "xz", "yz", "zz"]
+    G = {k: _randn(g.phys_shape, 20 + i) for i, k in enumerate(names)}
+    S = O.strain_from_gradient(G, 3)  # pair order xx yy zz xy yz zx
+    assert np.array_equal(S[0], G["xx"]) and np.array_equal(S[1], G["yy"]) and np.array_equal(S[2], G["zz"])
+    np.testing.assert_allclose(S[3], (G["xy"] + G["yx"]) / 2, rtol=1e-15)
+    np.testing.assert_allclose(S[4], (G["yz"] + G["zy"]) / 2, rtol=1e-15)
+    np.testing.assert_allclose(S[5], (G["zx"] + G["xz"]) / 2, rtol=1e-15)
+
+
+# test/test_tensor_helpers.jl:60-77
+def test_contract_dissipation_matches_manual_sum():
+    g2 = O.Grid(2, 8, 2 * math.pi)
+    t2 = [_randn(g2.phys_shape, 30 + i) for i in range(3)]  # xx yy xy
+    s2 = [_randn(g2.phys_shape, 40 + i) for i in range(3)]
+    np.testing.assert_allclose(O.contract_dissipation(t2, s2, 2),
+                               t2[0] * s2[0] + t2[1] * s2[1] + 2 * t2[2] * s2[2], rtol=1e-14)
+    g3 = O.Grid(3, 4, 2 * math.pi)
+    t3 = [_randn(g3.phys_shape, 50 + i) for i in range(6)]  # xx yy zz xy yz zx
+    s3 = [_randn(g3.phys_shape, 60 + i) for i in range(6)]
+    ref = t3[0] * s3[0] + t3[1] * s3[1] + t3[2] * s3[2] + 2 * (t3[3] * s3[3] + t3[4] * s3[4] + t3[5] * s3[5])
+    np.testing.assert_allclose(O.contract_dissipation(t3, s3, 3), ref, rtol=1e-12, atol=1e-14)
+
+
 def test_symmetrize_gives_real_field():
     """``symmetrize!`` docstring (src/solver.jl:391-397): after it the c2r keeps all energy."""
     g = O.Grid(3, 8, 2 * math.pi)
