@@ -193,7 +193,9 @@ SC_API int sc_closure_destroy(sc_closure* closure);
  * src/nets.jl:187; hardware tanh.approx.f32 in this BF16 path); output tau in
  * pair order.  BF16 weights and activations, FP32 accumulation on tcgen05
  * tensor cores.  weights[l]: host FP32 (C_out, C_in, 3, 3, 3) (rounded to BF16
- * here), biases[l]: host FP32 (C_out).  FP32 3D plans with n = 128. */
+ * here), biases[l]: host FP32 (C_out).  FP32 3D plans with n = 64 or 128.
+ * sc_closure_set_option(SC_CLOPT_CNN_SPLIT) switches it to three passes over
+ * hi/lo operand parts per convolution (about FP32 accuracy). */
 SC_API int sc_cnn_closure_create(sc_closure** closure, sc_plan* plan, double delta, double visc,
                                  const float* const* weights, const float* const* biases, double mu, double sigma);
 /* The same CNN on CUDA cores in the plan's precision (FP32 or FP64, any 3D
